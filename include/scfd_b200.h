@@ -1,0 +1,222 @@
+/*
+ * scfd_b200.h -- C ABI of the B200 (sm_100a) implementation of shared_cfd's
+ * per-step residual-and-implicit-update path.
+ *
+ * The reference has no plugin or FFI layer.  Its "operator API" is the set of
+ * fixed subroutine names that the generated main.f90 calls every step
+ * (store/core/main.part_primitive.f90:2-3, store/core/main.part_main.f90:2-5,
+ * store/time_scheme/<scheme>/main.main*.f90) plus the module-global arrays of
+ * store/core/variable.f90:1-49.  A Fortran architecture variant binds the
+ * functions below with iso_c_binding and replaces that call sequence with one
+ * scfd_step() per physical step; everything between upload and download stays
+ * resident on the GPU.
+ *
+ * Conventions
+ *   - Every function returns an int status (SCFD_OK == 0).  Nothing aborts the
+ *     process; the reference's `stop` / `call exit(1)` sites become codes.
+ *   - Plane, cell and species indices in descriptors are 1-based, like the
+ *     reference's Fortran.
+ *   - Field arrays crossing the ABI use the reference's own layout, e.g.
+ *     q(1:dimq,-1:nimax+2,-1:njmax+2,1:Nplane) in Fortran column-major order,
+ *     so a Fortran caller passes its module arrays unchanged.
+ *   - A context owns all device memory and one CUDA stream.  It is not
+ *     thread-safe; use one context per host thread / GPU.
+ */
+#ifndef SCFD_B200_H
+#define SCFD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCFD_ABI_VERSION 1
+
+#define SCFD_MAX_PLANES    64
+#define SCFD_MAX_SPECIES   32
+#define SCFD_MAX_REACTIONS 256
+#define SCFD_MAX_TRANS_SEC 5
+/* w(1:dimw) followed by vhi(1:nY): dimw = nY+8 */
+#define SCFD_BC_MAXVAL     (2 * SCFD_MAX_SPECIES + 8)
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    SCFD_OK             = 0,
+    SCFD_E_ARG          = 1,  /* bad argument / descriptor                        */
+    SCFD_E_CUDA         = 2,  /* CUDA runtime error                               */
+    SCFD_E_TNEWTON      = 3,  /* T-from-e Newton exceeded max_T_loop (sub_chem.f90:1575-1579) */
+    SCFD_E_CHEM         = 4,  /* chemistry integrator did not converge (sub_chem.f90:1767,1812) */
+    SCFD_E_OMEGA        = 5,  /* NR relaxation omega < omega_min (NR/q2d/time_NR_viscous.f90:75-78) */
+    SCFD_E_RESRATE      = 6,  /* inner residual ratio > ResRateErr (NR/q2d/sch_NR.raw.f90:232-233) */
+    SCFD_E_NAN          = 7,  /* NaN in the RMS of rho*E (core/check_convergence.f90:29-32) */
+    SCFD_E_SPIN         = 8,  /* a bounded device wait gave up (wavefront flag)   */
+    SCFD_E_CONNECT      = 9,  /* bad connectivity record                          */
+    SCFD_E_IO           = 10, /* file input / output                              */
+    SCFD_E_STATE        = 11, /* call out of order (e.g. step before commit)      */
+    SCFD_E_UNSUPPORTED  = 12  /* option combination not provided                 */
+};
+
+/* ---- option enums (values follow checkout.inp where one exists) ------- */
+enum { SCFD_DIM_2D = 0, SCFD_DIM_Q2D = 1 };                   /* checkout_flow.py:105-118 */
+enum { SCFD_DT_GLOBAL = 0, SCFD_DT_LOCAL = 1, SCFD_DT_FIXED = 2 }; /* checkout_flow.py:120-132; FIXED: dt given */
+enum { SCFD_SCHEME_EULER = 0, SCFD_SCHEME_LUSGS = 2, SCFD_SCHEME_NR = 3 }; /* checkout_flow.py:134-181 */
+enum { SCFD_RECON_UPWIND = 0, SCFD_RECON_MUSCL = 1 };           /* checkout_flow.py:183-194 */
+enum { SCFD_THERMO_IDEAL = 0, SCFD_THERMO_CHEMKIN_COLD = 1, SCFD_THERMO_CHEMKIN_REACTIVE = 2 };
+enum { SCFD_MU_REFERENCE = 0, SCFD_MU_SUTHERLAND = 1 };        /* ideal gas viscosity law */
+enum { SCFD_PREC_FP64 = 0, SCFD_PREC_MIXED = 1 };
+
+/* Boundary kinds for the device boundary descriptors.  They cover the ghost
+ * fills written by hand in the sample condition.f90 files (e.g.
+ * sample/no27.chemkin_reaction/condition.f90:49-147); ghost layer 2 always
+ * copies ghost layer 1, as in those samples. */
+enum {
+    SCFD_BC_EXTRAP    = 0,  /* zero gradient: ghost = first interior cell            */
+    SCFD_BC_FIXED     = 1,  /* ghost w(1:dimw), vhi(1:nY) = value[]                   */
+    SCFD_BC_OUTFLOW_P = 2,  /* zero gradient, then w(4) = value[0]                    */
+    SCFD_BC_SLIP      = 3,  /* zero gradient, velocity mirrored about the face normal */
+    SCFD_BC_NOSLIP    = 4,  /* zero gradient, u,v -> 2*value[0..1] - u,v (adiabatic)   */
+    SCFD_BC_FIXED_PIN = 5   /* fixed state w(1:dimw), vhi(1:nY) = value[], except
+                               p = interior p and rho = (p*value[dimw+nY]) /
+                               value[dimw+nY+1], the inflow of
+                               sample/no27.chemkin_reaction/condition.f90:49-60   */
+};
+enum { SCFD_SIDE_ILO = 0, SCFD_SIDE_IHI = 1, SCFD_SIDE_JLO = 2, SCFD_SIDE_JHI = 3 };
+
+/* ---- descriptors ------------------------------------------------------- */
+typedef struct scfd_desc {
+    int32_t abi_version;           /* = SCFD_ABI_VERSION                          */
+    int32_t nplane;                /* Nplane (store/core/n_grid.raw.f90:4)        */
+    int32_t ni[SCFD_MAX_PLANES];   /* cells per plane in i                        */
+    int32_t nj[SCFD_MAX_PLANES];   /* cells per plane in j                        */
+    int32_t ny;                    /* nY: species count (1 for ideal gas)         */
+    int32_t dim;                   /* SCFD_DIM_*                                  */
+    int32_t dt_mode;               /* SCFD_DT_*                                   */
+    int32_t scheme;                /* SCFD_SCHEME_*                               */
+    int32_t recon;                 /* SCFD_RECON_*                                */
+    int32_t viscous;               /* 0 non-viscous, 1 viscous (no-nV variant)    */
+    int32_t thermo;                /* SCFD_THERMO_*                               */
+    int32_t mu_model;              /* SCFD_MU_* (ideal gas only)                  */
+    int32_t precision;             /* SCFD_PREC_*                                 */
+    int32_t quirk_q1;              /* 1: reproduce geometry.f90:95-103 whole-array
+                                      ghost extrapolation (reference behaviour)   */
+    int32_t num_internal_loop;     /* NR "InternalLoop Max Number" (N-1 inner its)*/
+    int32_t il_write;              /* NR "InternalLoop OutOmega" (diagnostic only)*/
+    double  phi_mus, k_mus;        /* MUSCL parameters (muscl.f90:87-106)         */
+    double  kappa, rgas, nu_gas;   /* ideal gas KAPPA, RGAS, NU (checkout_flow.py:216-221) */
+    double  suth_mu0, suth_t0, suth_s; /* Sutherland law (mu_model = SUTHERLAND)  */
+    double  prandtl, schmidt;      /* reference: Pr = Sc = 1 (sch_viscous.f90:98-99) */
+    double  cfl;                   /* control.inp "CFL Number"                    */
+    double  dt_fixed;              /* dt for SCFD_DT_FIXED                        */
+    double  omega_max, omega_min, dq_max, res_rate_warn, res_rate_err; /* NR control */
+    int32_t chem_max_substeps;     /* device cap on chemistry substeps per cell   */
+    int32_t reserved[15];
+} scfd_desc;
+
+typedef struct scfd_bc {
+    int32_t plane;                 /* 1-based                                     */
+    int32_t side;                  /* SCFD_SIDE_*                                 */
+    int32_t first, last;           /* inclusive cell range along the side         */
+    int32_t kind;                  /* SCFD_BC_*                                   */
+    int32_t pad;
+    double  value[SCFD_BC_MAXVAL + 2];
+} scfd_bc;
+
+/* Chemkin tables after parsing chem.inp / MW.inp / trans.inp and the
+ * fuel/oxidiser species reordering (store/therm_lib/chemkin/core/mod_chem.raw.f90:31-68,
+ * sub_chem.f90:191-502, 788-889, 968-979).  Species indices are 0-based here. */
+typedef struct scfd_chem {
+    int32_t ns, nr, nt;
+    int32_t pad0;
+    double  coeff[SCFD_MAX_SPECIES][2][7];   /* coeff(i,sec,k) -> [k][sec-1][i-1]  */
+    double  tthre[SCFD_MAX_SPECIES][3];
+    double  mws[SCFD_MAX_SPECIES];
+    int32_t rstate[SCFD_MAX_REACTIONS][2];
+    int32_t indnu[SCFD_MAX_REACTIONS][2][3];
+    int32_t numnu[SCFD_MAX_REACTIONS][2];
+    int32_t snu[SCFD_MAX_REACTIONS];
+    int32_t exist_m[SCFD_MAX_REACTIONS];
+    int32_t numm[SCFD_MAX_REACTIONS];
+    int32_t indm[SCFD_MAX_REACTIONS][SCFD_MAX_SPECIES];
+    double  men[SCFD_MAX_REACTIONS][SCFD_MAX_SPECIES];
+    double  abe[SCFD_MAX_REACTIONS][3];      /* (ln A, beta, Ea/Rc)                */
+    double  cabe[SCFD_MAX_REACTIONS][3];
+    double  troe[SCFD_MAX_REACTIONS][4];
+    int32_t tr2th[SCFD_MAX_SPECIES];         /* transport entry -> species (0-based) */
+    int32_t num_sctn_trans[SCFD_MAX_SPECIES];
+    double  trange_trans[SCFD_MAX_SPECIES][SCFD_MAX_TRANS_SEC][2];
+    double  trans[SCFD_MAX_SPECIES][SCFD_MAX_TRANS_SEC][4];
+    double  rtol, atol;                      /* control_chem.inp tolerances        */
+} scfd_chem;
+
+typedef struct scfd_stats {
+    double  dt_grbl;               /* global dt of the step (global / fixed mode) */
+    double  tt;                    /* accumulated physical time                   */
+    double  res, res1;             /* NR: last and first inner residual sums      */
+    double  omega;                 /* NR: last relaxation factor applied          */
+    int32_t status;                /* SCFD_* code of the step                     */
+    int32_t inner_iters;           /* NR inner iterations run                     */
+    int64_t chem_attempts;         /* CHEMEQ2 attempts summed over cells          */
+    int64_t chem_fallback_cells;   /* cells that used the implicit fallback       */
+    int32_t res_warn;              /* 1 if res/res1 > ResRateWarn                 */
+    int32_t reserved[7];
+} scfd_stats;
+
+typedef struct scfd_ctx scfd_ctx;
+
+/* ---- lifecycle ---------------------------------------------------------- */
+int  scfd_abi_version(void);
+/* Replaces the compile-time sizing of store/core/n_grid.raw.f90 and the
+ * checkout.inp selections (store/checkout/checkout_flow.py:67-327). */
+int  scfd_create(const scfd_desc* desc, scfd_ctx** out);
+int  scfd_destroy(scfd_ctx* ctx);
+/* Error text of the last failing call on this context. */
+int  scfd_last_error(const scfd_ctx* ctx, char* buf, int len);
+
+/* ---- set-up ------------------------------------------------------------- */
+/* Node coordinates of one plane, xh(0:ni,0:nj), rh(0:ni,0:nj), column-major
+ * (store/dim/2d/geometry.f90:27-78, init_xrh). */
+int  scfd_set_geometry(scfd_ctx* ctx, int plane, const double* xh, const double* rh);
+/* Block-interface records, 11 ints each, exactly the lines of cut_copro000.inp
+ * (geo width order p1 c1 s1 pm1 p2 c2 s2 pm2; store/cond/core/mod_cond.py:271-276,
+ * consumed by section_exchange, store/cond/no-nV/condition.tail.f90:2-70). */
+int  scfd_set_connectivity(scfd_ctx* ctx, const int32_t* recs, int nrec);
+/* Device boundary descriptors replacing the user loops of set_BC. */
+int  scfd_set_bc(scfd_ctx* ctx, const scfd_bc* bcs, int nbc);
+/* Chemkin tables (required for SCFD_THERMO_CHEMKIN_*). */
+int  scfd_set_chem(scfd_ctx* ctx, const scfd_chem* chem);
+/* Ends set-up: builds the metrics (init_geometry, set_vnc_dsc, set_geojac),
+ * allocates device memory and checks the connectivity. */
+int  scfd_commit(scfd_ctx* ctx);
+
+/* ---- state -------------------------------------------------------------- */
+/* q(1:dimq,-1:nimax+2,-1:njmax+2,Nplane), w(1:dimw,...), vhi(1:nY,...):
+ * the reference's module arrays (store/core/variable.f90:24-33).  vhi may be
+ * NULL (then it is computed by scfd_prepare).  qp/qpp are set to q. */
+int  scfd_upload(scfd_ctx* ctx, const double* q, const double* w, const double* vhi,
+                 double tt);
+/* part_primitive (set_w, set_thermo_prop) followed by set_BC(step):
+ * store/core/main.body.raw.f90:15-16. */
+int  scfd_prepare(scfd_ctx* ctx, int step);
+/* One physical step of the configured scheme, the body of the generated time
+ * loop (store/time_scheme/<scheme>/main.main*.f90 with part_* expanded). */
+int  scfd_step(scfd_ctx* ctx, int step, scfd_stats* stats);
+/* nsteps consecutive calls of scfd_step starting at step; stats of the last. */
+int  scfd_run(scfd_ctx* ctx, int step, int nsteps, scfd_stats* stats);
+/* RMS of check_convergence (store/core/check_convergence.f90:17-28):
+ * sqrt(sum (q(E)-qp(E))^2) / ncells over all planes. */
+int  scfd_rms(scfd_ctx* ctx, double* rms);
+/* Copies the state back in the reference layout; any pointer may be NULL. */
+int  scfd_download(scfd_ctx* ctx, double* q, double* w, double* vhi, double* tt);
+/* Same as download but for qp (the previous step's q). */
+int  scfd_download_qp(scfd_ctx* ctx, double* qp);
+/* The context's CUDA stream (cudaStream_t as void*), for event timing. */
+int  scfd_get_stream(scfd_ctx* ctx, void** stream);
+/* Number of device kernel launches issued by the last scfd_step/scfd_run. */
+int  scfd_launch_count(const scfd_ctx* ctx, int64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCFD_B200_H */

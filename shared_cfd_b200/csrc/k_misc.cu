@@ -1,0 +1,148 @@
+// k_misc.cu -- time step (store/time_step/{global,local}/set_dt.f90), the
+// check_convergence RMS (store/core/check_convergence.f90:17-28), step
+// bookkeeping of the device scalars, and the FP32 copy of the primitive
+// field used by the mixed-precision residual.
+#include "scfd_internal.h"
+
+namespace scfd {
+
+__global__ void k_dt_reset(View v) {
+    v.sc->dtmin_bits = 0x7FF0000000000000ull;  // +inf
+}
+
+__global__ void k_set_dt(View v) {
+    const int p = blockIdx.y;
+    const int ni = v.P.ni[p], nj = v.P.nj[p];
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    double dtc = 1e300;
+    if (idx < ni * nj) {
+        const int i = idx % ni + 1, j = idx / ni + 1;
+        const long long N = v.ncell;
+        const long long c = cidx(v.P, p, i, j);
+        const long long cim = cidx(v.P, p, i - 1, j), cjm = cidx(v.P, p, i, j - 1);
+        const double rho = v.w[c], u = v.w[N + c], vv = v.w[2 * N + c], pr = v.w[3 * N + c];
+        const double a = sqrt(v.w[(v.D + 1) * N + c] * pr / rho);
+        double uds = 0.0, un;
+        un = v.vni[c] * u + v.vni[N + c] * vv;
+        uds = uds + (fabs(un) + a) * v.dsi[c];
+        un = v.vni[cim] * u + v.vni[N + cim] * vv;
+        uds = uds + (fabs(un) + a) * v.dsi[cim];
+        un = v.vnj[c] * u + v.vnj[N + c] * vv;
+        uds = uds + (fabs(un) + a) * v.dsj[c];
+        un = v.vnj[cjm] * u + v.vnj[N + cjm] * vv;
+        uds = uds + (fabs(un) + a) * v.dsj[cjm];
+        dtc = v.cfl * v.Vol[c] / fmax(uds, v.w[(v.D + 4) * N + c] / rho);
+        v.dt_mat[c] = dtc;
+    }
+    if (v.dt_mode == SCFD_DT_GLOBAL) {
+        for (int o = 16; o > 0; o >>= 1) dtc = fmin(dtc, __shfl_xor_sync(0xffffffffu, dtc, o));
+        if ((threadIdx.x & 31) == 0 && dtc < 1e300)
+            atomicMin(&v.sc->dtmin_bits, (unsigned long long)__double_as_longlong(dtc));
+    }
+}
+
+// dt_grbl and tt (global: tt = tt + dt_grbl, set_dt.f90:40-42; fixed dt likewise)
+__global__ void k_dt_final(View v) {
+    if (v.dt_mode == SCFD_DT_GLOBAL) {
+        v.sc->dt_grbl = __longlong_as_double((long long)v.sc->dtmin_bits);
+        v.sc->tt = v.sc->tt + v.sc->dt_grbl;
+    } else if (v.dt_mode == SCFD_DT_FIXED) {
+        v.sc->dt_grbl = v.dt_fixed;
+        v.sc->tt = v.sc->tt + v.sc->dt_grbl;
+    }
+}
+
+int launch_set_dt(const View& v, cudaStream_t s) {
+    int n = 0;
+    if (v.dt_mode == SCFD_DT_FIXED) {
+        k_dt_final<<<1, 1, 0, s>>>(v);
+        return 1;
+    }
+    int mx = 0;
+    for (int p = 0; p < v.P.np; ++p) mx = v.P.ni[p] * v.P.nj[p] > mx ? v.P.ni[p] * v.P.nj[p] : mx;
+    if (v.dt_mode == SCFD_DT_GLOBAL) {
+        k_dt_reset<<<1, 1, 0, s>>>(v);
+        ++n;
+    }
+    dim3 grid((mx + 255) / 256, v.P.np);
+    k_set_dt<<<grid, 256, 0, s>>>(v);
+    ++n;
+    if (v.dt_mode == SCFD_DT_GLOBAL) {
+        k_dt_final<<<1, 1, 0, s>>>(v);
+        ++n;
+    }
+    return n;
+}
+
+// Deterministic two-pass RMS of q(E) - qp(E).
+__global__ void k_rms_partial(View v, double* partial) {
+    __shared__ double sh[256];
+    const int p = blockIdx.y;
+    const int ni = v.P.ni[p], nj = v.P.nj[p];
+    double acc = 0.0;
+    const long long N = v.ncell;
+    const int kE = v.nY + 2;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ni * nj; idx += gridDim.x * blockDim.x) {
+        const int i = idx % ni + 1, j = idx / ni + 1;
+        const long long c = cidx(v.P, p, i, j);
+        const double d = v.q[kE * N + c] - v.qp[kE * N + c];
+        acc += d * d;
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = sh[0];
+}
+
+__global__ void k_rms_final(const double* partial, int n, double cells, double* out) {
+    double s = 0.0;
+    for (int k = 0; k < n; ++k) s += partial[k];
+    *out = sqrt(s) / cells;
+}
+
+int launch_rms(const View& v, cudaStream_t s, double* partial, double* out) {
+    const int gx = 64;
+    dim3 grid(gx, v.P.np);
+    k_rms_partial<<<grid, 256, 0, s>>>(v, partial);
+    double cells = 0.0;
+    for (int p = 0; p < v.P.np; ++p) cells = cells + (double)(v.P.ni[p] * v.P.nj[p]);
+    k_rms_final<<<1, 1, 0, s>>>(partial, gx * v.P.np, cells, out);
+    return 2;
+}
+
+// FP32 copies of w and vhi (all slots, ghosts included) for the mixed path.
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, long long n) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        b[k] = (float)a[k];
+}
+
+int launch_to_f32(const View& v, cudaStream_t s) {
+    const long long nw = v.W * v.ncell, nv = v.nY * v.ncell;
+    k_to_f32<<<1184, 256, 0, s>>>(v.w, v.w32, nw);
+    k_to_f32<<<1184, 256, 0, s>>>(v.vhi, v.vhi32, nv);
+    return 2;
+}
+
+}  // namespace scfd
+
+namespace scfd {
+
+// check_internal_loop_convergence (NR/q2d/sch_NR.raw.f90:222-237) on the device:
+// status E_RESRATE when res/res1 > ResRateErr after the first step of the run;
+// first_dual becomes false.
+__global__ void k_step_end(View v, double warn, double err) {
+    DevScalars* sc = v.sc;
+    const double rr = sc->res / sc->res1;
+    if (rr > warn && rr > err && !sc->first_dual) atomicMax(&sc->status, SCFD_E_RESRATE);
+    sc->first_dual = 0;
+}
+
+int launch_step_end(const View& v, cudaStream_t s, double warn, double err) {
+    k_step_end<<<1, 1, 0, s>>>(v, warn, err);
+    return 1;
+}
+
+}  // namespace scfd

@@ -1,0 +1,831 @@
+// scfd_api.cu -- the C ABI of include/scfd_b200.h: context, device arena,
+// metrics, boundary expansion, state transfer and the per-step kernel sequence.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "scfd_internal.h"
+
+using namespace scfd;
+
+struct scfd_ctx {
+    scfd_desc d{};
+    std::string err;
+    int np = 0, nY = 0, D = 0, W = 0, nimax = 0, njmax = 0;
+    Planes P{};
+    long long ncell = 0;
+    std::vector<std::vector<double>> xh, rh;
+    std::vector<int> geo_set;
+    bool committed = false, have_chem = false, uploaded = false;
+    std::vector<int32_t> cut;
+    std::vector<scfd_bc> bcs;
+    scfd_chem chem{};
+    cudaStream_t stream = nullptr;
+    int device = 0, nsm = 148;
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    View v{};
+    DevScalars* d_sc = nullptr;
+    DevScalars* h_sc = nullptr;  // pinned
+    // sweeps
+    int nsf = 0, nsb = 0;
+    int* d_strips_f = nullptr;
+    int* d_strips_b = nullptr;
+    double* d_xfer = nullptr;
+    int* d_progress = nullptr;
+    int* d_tickets = nullptr;
+    double* d_partials = nullptr;
+    // boundaries
+    GhostOp* d_ops = nullptr;
+    int nops = 0;
+    double* d_bcval = nullptr;
+    int valstride = SCFD_BC_MAXVAL + 2;
+    // chemistry
+    unsigned long long* d_counter = nullptr;
+    // rms
+    double* d_rms_partial = nullptr;
+    double* d_rms_out = nullptr;
+    // pinned staging for transfers
+    double* h_stage = nullptr;
+    size_t stage_doubles = 0;
+    long long launches = 0;
+    int cells_max = 0;
+
+    int fail(int code, const std::string& m) {
+        err = m;
+        return code;
+    }
+};
+
+namespace {
+
+#define CK(x)                                                                               \
+    do {                                                                                    \
+        cudaError_t e_ = (x);                                                               \
+        if (e_ != cudaSuccess) return c->fail(SCFD_E_CUDA, std::string(#x ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+inline double sq(double a) { return a * a; }
+
+// ---------------------------------------------------------------------------
+// Metrics on the host in FP64 (store/dim/{2d,q2d}/geometry.f90, LU-SGS set_vnc_dsc,
+// viscous set_geojac), written straight into the device slot layout.
+// ---------------------------------------------------------------------------
+struct HostGeo {
+    std::vector<double> Vol, Area, dsi, dsj, vni, vnj, x, r, gjc, gji, gjj, dsci, dscj, vnci, vncj;
+};
+
+void build_geometry(scfd_ctx* c, HostGeo& g) {
+    const long long N = c->ncell;
+    auto z = [&](std::vector<double>& a, int k) { a.assign((size_t)(k * N), 0.0); };
+    z(g.Vol, 1); z(g.Area, 1); z(g.dsi, 1); z(g.dsj, 1); z(g.vni, 2); z(g.vnj, 2); z(g.x, 1); z(g.r, 1);
+    z(g.gjc, 4); z(g.gji, 4); z(g.gjj, 4); z(g.dsci, 1); z(g.dscj, 1); z(g.vnci, 2); z(g.vncj, 2);
+    const bool q2d = c->d.dim == SCFD_DIM_Q2D;
+    const bool quirk = c->d.quirk_q1 != 0;
+    for (int p = 0; p < c->np; ++p) {
+        const int ni = c->P.ni[p], nj = c->P.nj[p];
+        const std::vector<double>& XH = c->xh[p];
+        const std::vector<double>& RH = c->rh[p];
+        auto xh = [&](int i, int j) { return XH[i + (ni + 1) * j]; };
+        auto rh = [&](int i, int j) { return RH[i + (ni + 1) * j]; };
+        auto C = [&](int i, int j) { return cidx(c->P, p, i, j); };
+        // cell centres with ghost extrapolation (set_xr, geometry.f90:79-106)
+        auto X = [&](int i, int j) -> double& { return g.x[C(i, j)]; };
+        auto R = [&](int i, int j) -> double& { return g.r[C(i, j)]; };
+        for (int j = 1; j <= nj; ++j)
+            for (int i = 1; i <= ni; ++i) {
+                X(i, j) = 1.0 / 4.0 * (xh(i - 1, j - 1) + xh(i, j - 1) + xh(i - 1, j) + xh(i, j));
+                R(i, j) = 1.0 / 4.0 * (rh(i - 1, j - 1) + rh(i, j - 1) + rh(i - 1, j) + rh(i, j));
+            }
+        // The reference writes x(ni(k)+1, j) for EVERY plane k here (ni is the
+        // per-plane array: a vector subscript); with quirk_q1 this is kept.
+        std::vector<int> icols, jrows;
+        if (quirk) {
+            for (int k = 0; k < c->np; ++k) {
+                icols.push_back(c->P.ni[k]);
+                jrows.push_back(c->P.nj[k]);
+            }
+        } else {
+            icols.push_back(ni);
+            jrows.push_back(nj);
+        }
+        for (int j = 1; j <= nj; ++j) {
+            X(0, j) = 2.0 * X(1, j) - X(2, j);
+            R(0, j) = 2.0 * R(1, j) - R(2, j);
+            std::vector<double> vx, vr;
+            for (int n : icols) {
+                // out-of-plane columns (n >= this plane's ni + 2) fall into the
+                // padding of the reference's nimax-wide array; they are read
+                // nowhere, so only columns inside this plane's slots are kept
+                vx.push_back(n + 1 <= ni + 1 && n - 1 >= 0 ? 2.0 * X(n, j) - X(n - 1, j) : 0.0);
+                vr.push_back(n + 1 <= ni + 1 && n - 1 >= 0 ? 2.0 * R(n, j) - R(n - 1, j) : 0.0);
+            }
+            for (size_t k = 0; k < icols.size(); ++k)
+                if (icols[k] + 1 <= ni + 1) X(icols[k] + 1, j) = vx[k];
+            for (size_t k = 0; k < icols.size(); ++k)
+                if (icols[k] + 1 <= ni + 1) R(icols[k] + 1, j) = vr[k];
+        }
+        for (int i = 0; i <= ni + 1; ++i) {
+            X(i, 0) = 2.0 * X(i, 1) - X(i, 2);
+            R(i, 0) = 2.0 * R(i, 1) - R(i, 2);
+            std::vector<double> vx, vr;
+            for (int n : jrows) {
+                vx.push_back(n + 1 <= nj + 1 ? 2.0 * X(i, n) - X(i, n - 1) : 0.0);
+                vr.push_back(n + 1 <= nj + 1 ? 2.0 * R(i, n) - R(i, n - 1) : 0.0);
+            }
+            for (size_t k = 0; k < jrows.size(); ++k)
+                if (jrows[k] + 1 <= nj + 1) X(i, jrows[k] + 1) = vx[k];
+            for (size_t k = 0; k < jrows.size(); ++k)
+                if (jrows[k] + 1 <= nj + 1) R(i, jrows[k] + 1) = vr[k];
+        }
+        auto tri = [](double a1, double a2, double b1, double b2, double c1, double c2) {
+            return 1.0 / 2.0 * (a1 * (b2 - c2) + b1 * (c2 - a2) + c1 * (a2 - b2));
+        };
+        auto dist = [](double x1, double y1, double x2, double y2) { return std::sqrt(sq(x1 - x2) + sq(y1 - y2)); };
+        for (int j = 1; j <= nj; ++j)
+            for (int i = 1; i <= ni; ++i) {
+                const double A1 = tri(xh(i - 1, j - 1), rh(i - 1, j - 1), xh(i, j - 1), rh(i, j - 1), xh(i - 1, j), rh(i - 1, j));
+                const double A2 = tri(xh(i, j - 1), rh(i, j - 1), xh(i, j), rh(i, j), xh(i - 1, j), rh(i - 1, j));
+                const long long cc = C(i, j);
+                if (q2d) {
+                    g.Area[cc] = A1 + A2;
+                    g.Vol[cc] = (rh(i - 1, j - 1) + rh(i, j - 1) + rh(i - 1, j)) * A1 / 3.0 +
+                                (rh(i, j - 1) + rh(i, j) + rh(i - 1, j)) * A2 / 3.0;
+                } else {
+                    g.Area[cc] = 0.0;
+                    g.Vol[cc] = A1 + A2;
+                }
+            }
+        for (int j = 0; j <= nj; ++j)
+            for (int i = 1; i <= ni; ++i) {
+                double ds = dist(xh(i - 1, j), rh(i - 1, j), xh(i, j), rh(i, j));
+                if (q2d) ds = ds * (rh(i - 1, j) + rh(i, j)) / 2.0;
+                g.dsj[C(i, j)] = ds;
+                const double nx = -(rh(i, j) - rh(i - 1, j)), nr = xh(i, j) - xh(i - 1, j);
+                const double sd = std::sqrt(sq(nx) + sq(nr));
+                g.vnj[C(i, j)] = nx / sd;
+                g.vnj[N + C(i, j)] = nr / sd;
+            }
+        for (int j = 1; j <= nj; ++j)
+            for (int i = 0; i <= ni; ++i) {
+                double ds = dist(xh(i, j - 1), rh(i, j - 1), xh(i, j), rh(i, j));
+                if (q2d) ds = ds * (rh(i, j - 1) + rh(i, j)) / 2.0;
+                g.dsi[C(i, j)] = ds;
+                const double nx = rh(i, j) - rh(i, j - 1), nr = -(xh(i, j) - xh(i, j - 1));
+                const double sd = std::sqrt(sq(nx) + sq(nr));
+                g.vni[C(i, j)] = nx / sd;
+                g.vni[N + C(i, j)] = nr / sd;
+            }
+        for (int j = 1; j <= nj; ++j)
+            for (int i = 1; i <= ni; ++i) {
+                const double a1 = (xh(i - 1, j - 1) + xh(i, j - 1)) * 0.5, a2 = (rh(i - 1, j - 1) + rh(i, j - 1)) * 0.5;
+                const double b1 = (xh(i, j - 1) + xh(i, j)) * 0.5, b2 = (rh(i, j - 1) + rh(i, j)) * 0.5;
+                const double c1 = (xh(i - 1, j) + xh(i, j)) * 0.5, c2 = (rh(i - 1, j) + rh(i, j)) * 0.5;
+                const double d1 = (xh(i - 1, j - 1) + xh(i - 1, j)) * 0.5, d2 = (rh(i - 1, j - 1) + rh(i - 1, j)) * 0.5;
+                double dci = std::sqrt(sq(c1 - a1) + sq(c2 - a2));
+                double dcj = std::sqrt(sq(b1 - d1) + sq(b2 - d2));
+                const long long cc = C(i, j);
+                g.vnci[cc] = (b1 - d1) / dcj;
+                g.vnci[N + cc] = (b2 - d2) / dcj;
+                g.vncj[cc] = (c1 - a1) / dci;
+                g.vncj[N + cc] = (c2 - a2) / dci;
+                if (q2d) {
+                    dci = dci * (c2 + a2) * 0.5;
+                    dcj = dcj * (b2 + d2) * 0.5;
+                }
+                g.dsci[cc] = dci;
+                g.dscj[cc] = dcj;
+            }
+        auto put = [&](std::vector<double>& a, long long cc, double dxdxi, double dydxi, double dxdeta, double dydeta) {
+            const double det = dxdxi * dydeta - dydxi * dxdeta;
+            a[cc] = dydeta / det;
+            a[N + cc] = -dxdeta / det;
+            a[2 * N + cc] = -dydxi / det;
+            a[3 * N + cc] = dxdxi / det;
+        };
+        for (int j = 1; j <= nj; ++j)
+            for (int i = 1; i <= ni; ++i)
+                put(g.gjc, C(i, j), (X(i + 1, j) - X(i - 1, j)) * 0.5, (R(i + 1, j) - R(i - 1, j)) * 0.5,
+                    (X(i, j + 1) - X(i, j - 1)) * 0.5, (R(i, j + 1) - R(i, j - 1)) * 0.5);
+        for (int j = 1; j <= nj; ++j)
+            for (int i = 0; i <= ni; ++i)
+                put(g.gji, C(i, j), X(i + 1, j) - X(i, j), R(i + 1, j) - R(i, j),
+                    (X(i + 1, j + 1) + X(i, j + 1) - X(i + 1, j - 1) - X(i, j - 1)) * 0.25,
+                    (R(i + 1, j + 1) + R(i, j + 1) - R(i + 1, j - 1) - R(i, j - 1)) * 0.25);
+        for (int j = 0; j <= nj; ++j)
+            for (int i = 1; i <= ni; ++i)
+                put(g.gjj, C(i, j), (X(i + 1, j + 1) + X(i + 1, j) - X(i - 1, j + 1) - X(i - 1, j)) * 0.25,
+                    (R(i + 1, j + 1) + R(i + 1, j) - R(i - 1, j + 1) - R(i - 1, j)) * 0.25, X(i, j + 1) - X(i, j),
+                    R(i, j + 1) - R(i, j));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// set_BC expansion: halo copies (section_exchange), then the i- and j-boundary
+// descriptors, de-duplicated so the last writer of each ghost cell wins.
+// ---------------------------------------------------------------------------
+int build_ghost_ops(scfd_ctx* c, const HostGeo& g, std::vector<GhostOp>& out) {
+    std::vector<GhostOp> ops;
+    auto inside = [&](int p, int i, int j) {
+        return p >= 0 && p < c->np && i >= -1 && i <= c->P.ni[p] + 2 && j >= -1 && j <= c->P.nj[p] + 2;
+    };
+    auto interior = [&](int p, int i, int j) {
+        return p >= 0 && p < c->np && i >= 1 && i <= c->P.ni[p] && j >= 1 && j <= c->P.nj[p];
+    };
+    auto add = [&](int pd, int id, int jd, int ps, int is, int js, int kind, int bc, double n1, double n2) -> bool {
+        if (!inside(pd, id, jd) || !interior(ps, is, js) || interior(pd, id, jd)) return false;
+        GhostOp o;
+        o.dst = cidx(c->P, pd, id, jd);
+        o.src = cidx(c->P, ps, is, js);
+        o.kind = kind;
+        o.bc = bc;
+        o.n1 = n1;
+        o.n2 = n2;
+        ops.push_back(o);
+        return true;
+    };
+    const size_t nrec = c->cut.size() / 11;
+    for (size_t n = 0; n < nrec; ++n) {
+        const int32_t* r = &c->cut[n * 11];
+        const int geo = r[0], width = r[1], order = r[2], p1 = r[3] - 1, c1 = r[4], s1 = r[5], pm1 = r[6],
+                  p2 = r[7] - 1, c2 = r[8], s2 = r[9], pm2 = r[10];
+        if (geo < 1 || geo > 4 || width < 0 || (order != 1 && order != -1) || (pm1 != 1 && pm1 != -1) ||
+            (pm2 != 1 && pm2 != -1))
+            return c->fail(SCFD_E_CONNECT, "bad connectivity record " + std::to_string(n + 1));
+        bool ok = true;
+        for (int inc = 0; inc < width && ok; ++inc) {
+            const int a = s1 + inc, b = s2 + inc * order;
+            switch (geo) {
+                case 1:
+                    ok = add(p1, c1 + pm1, a, p2, c2, b, -1, 0, 0, 0) && add(p1, c1 + 2 * pm1, a, p2, c2 - pm2, b, -1, 0, 0, 0) &&
+                         add(p2, c2 + pm2, b, p1, c1, a, -1, 0, 0, 0) && add(p2, c2 + 2 * pm2, b, p1, c1 - pm1, a, -1, 0, 0, 0);
+                    break;
+                case 2:
+                    ok = add(p1, c1 + pm1, a, p2, b, c2, -1, 0, 0, 0) && add(p1, c1 + 2 * pm1, a, p2, b, c2 - pm2, -1, 0, 0, 0) &&
+                         add(p2, b, c2 + pm2, p1, c1, a, -1, 0, 0, 0) && add(p2, b, c2 + 2 * pm2, p1, c1 - pm1, a, -1, 0, 0, 0);
+                    break;
+                case 3:
+                    ok = add(p1, a, c1 + pm1, p2, c2, b, -1, 0, 0, 0) && add(p1, a, c1 + 2 * pm1, p2, c2 - pm2, b, -1, 0, 0, 0) &&
+                         add(p2, c2 + pm2, b, p1, a, c1, -1, 0, 0, 0) && add(p2, c2 + 2 * pm2, b, p1, a, c1 - pm1, -1, 0, 0, 0);
+                    break;
+                default:
+                    ok = add(p1, a, c1 + pm1, p2, b, c2, -1, 0, 0, 0) && add(p1, a, c1 + 2 * pm1, p2, b, c2 - pm2, -1, 0, 0, 0) &&
+                         add(p2, b, c2 + pm2, p1, a, c1, -1, 0, 0, 0) && add(p2, b, c2 + 2 * pm2, p1, a, c1 - pm1, -1, 0, 0, 0);
+                    break;
+            }
+        }
+        if (!ok) return c->fail(SCFD_E_CONNECT, "connectivity record " + std::to_string(n + 1) + " leaves the planes");
+    }
+    const long long N = c->ncell;
+    for (int phase = 0; phase < 2; ++phase)
+        for (size_t k = 0; k < c->bcs.size(); ++k) {
+            const scfd_bc& b = c->bcs[k];
+            const bool iside = b.side == SCFD_SIDE_ILO || b.side == SCFD_SIDE_IHI;
+            if ((phase == 0) != iside) continue;
+            const int p = b.plane - 1, ni = c->P.ni[p], nj = c->P.nj[p];
+            for (int s = b.first; s <= b.last; ++s) {
+                int ib, jb, i1, j1, i2, j2;
+                long long fc;
+                const std::vector<double>* nv;
+                switch (b.side) {
+                    case SCFD_SIDE_ILO: ib = 1; jb = s; i1 = 0; j1 = s; i2 = -1; j2 = s; fc = cidx(c->P, p, 0, s); nv = &g.vni; break;
+                    case SCFD_SIDE_IHI: ib = ni; jb = s; i1 = ni + 1; j1 = s; i2 = ni + 2; j2 = s; fc = cidx(c->P, p, ni, s); nv = &g.vni; break;
+                    case SCFD_SIDE_JLO: ib = s; jb = 1; i1 = s; j1 = 0; i2 = s; j2 = -1; fc = cidx(c->P, p, s, 0); nv = &g.vnj; break;
+                    default: ib = s; jb = nj; i1 = s; j1 = nj + 1; i2 = s; j2 = nj + 2; fc = cidx(c->P, p, s, nj); nv = &g.vnj; break;
+                }
+                const double n1 = (*nv)[fc], n2 = (*nv)[N + fc];
+                add(p, i1, j1, p, ib, jb, b.kind, (int)k, n1, n2);
+                add(p, i2, j2, p, ib, jb, b.kind, (int)k, n1, n2);
+            }
+        }
+    std::unordered_map<long long, size_t> last;
+    for (size_t k = 0; k < ops.size(); ++k) last[ops[k].dst] = k;
+    out.clear();
+    for (size_t k = 0; k < ops.size(); ++k)
+        if (last[ops[k].dst] == k) out.push_back(ops[k]);
+    return 0;
+}
+
+template <typename T>
+T* carve(char*& p, size_t n) {
+    T* r = reinterpret_cast<T*>(p);
+    size_t bytes = (n * sizeof(T) + 255) & ~(size_t)255;
+    p += bytes;
+    return r;
+}
+template <typename T>
+size_t need(size_t n) {
+    return (n * sizeof(T) + 255) & ~(size_t)255;
+}
+
+int sync_scalars(scfd_ctx* c) {
+    CK(cudaMemcpyAsync(c->h_sc, c->d_sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+// the kernel sequence of one physical step
+int enqueue_step(scfd_ctx* c) {
+    const View& v = c->v;
+    cudaStream_t s = c->stream;
+    long long n = 0;
+    const bool reactive = c->d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
+    const long long qbytes = sizeof(double) * (long long)c->D * c->ncell;
+    auto primitive = [&]() { n += launch_thermo(v, s, c->cells_max); };
+    auto bc = [&]() {
+        n += launch_ghosts(v, s, c->d_ops, c->nops, c->d_bcval, c->valstride);
+        if (v.precision == SCFD_PREC_MIXED) n += launch_to_f32(v, s);
+    };
+    auto chem = [&]() { n += launch_chem_impl(v, s, c->d.chem_max_substeps, c->d_counter, c->nsm); };
+    if (c->d.scheme == SCFD_SCHEME_NR) {
+        primitive();
+        n += launch_set_dt(v, s);
+        if (reactive) chem();
+        CK(cudaMemcpyAsync(v.qpp, v.qp, qbytes, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(v.qp, v.q, qbytes, cudaMemcpyDeviceToDevice, s));
+        for (int j = 1; j < c->d.num_internal_loop; ++j) {
+            primitive();
+            bc();
+            n += launch_residual(v, s, RES_NR);
+            n += launch_sweeps(v, s, c->d_xfer, c->d_progress, c->d_partials, c->d_tickets, c->nsf, c->nsb,
+                               c->d_strips_f, c->d_strips_b);
+            n += launch_nr_update(v, s, c->d_partials, c->nsb, j);
+        }
+        n += launch_step_end(v, s, c->d.res_rate_warn, c->d.res_rate_err);
+    } else {
+        if (reactive) {
+            primitive();
+            n += launch_set_dt(v, s);
+            chem();
+            CK(cudaMemcpyAsync(v.qp, v.q, qbytes, cudaMemcpyDeviceToDevice, s));
+            primitive();
+        } else {
+            CK(cudaMemcpyAsync(v.qp, v.q, qbytes, cudaMemcpyDeviceToDevice, s));
+            primitive();
+            n += launch_set_dt(v, s);
+        }
+        bc();
+        if (c->d.scheme == SCFD_SCHEME_EULER) {
+            n += launch_residual(v, s, RES_EULER);
+        } else {
+            n += launch_residual(v, s, RES_LUSGS);
+            n += launch_sweeps(v, s, c->d_xfer, c->d_progress, c->d_partials, c->d_tickets, c->nsf, c->nsb,
+                               c->d_strips_f, c->d_strips_b);
+        }
+    }
+    CK(cudaGetLastError());
+    c->launches += n;
+    return 0;
+}
+
+int fill_stats(scfd_ctx* c, scfd_stats* st, long long att0, long long fb0) {
+    const DevScalars& h = *c->h_sc;
+    if (st) {
+        std::memset(st, 0, sizeof(*st));
+        st->dt_grbl = h.dt_grbl;
+        st->tt = h.tt;
+        st->res = h.res;
+        st->res1 = h.res1;
+        st->omega = h.omega;
+        st->status = h.status;
+        st->inner_iters = c->d.scheme == SCFD_SCHEME_NR ? std::max(0, c->d.num_internal_loop - 1) : 0;
+        st->chem_attempts = h.chem_attempts - att0;
+        st->chem_fallback_cells = h.chem_fallback - fb0;
+        st->res_warn = (c->d.scheme == SCFD_SCHEME_NR && h.res / h.res1 > c->d.res_rate_warn) ? 1 : 0;
+    }
+    return h.status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int scfd_abi_version(void) { return SCFD_ABI_VERSION; }
+
+int scfd_create(const scfd_desc* d, scfd_ctx** out) {
+    if (!d || !out) return SCFD_E_ARG;
+    if (d->abi_version != SCFD_ABI_VERSION) return SCFD_E_ARG;
+    if (d->nplane < 1 || d->nplane > SCFD_MAX_PLANES || d->ny < 1 || d->ny > SCFD_MAX_SPECIES) return SCFD_E_ARG;
+    if (d->scheme != SCFD_SCHEME_EULER && d->scheme != SCFD_SCHEME_LUSGS && d->scheme != SCFD_SCHEME_NR)
+        return SCFD_E_UNSUPPORTED;
+    if (d->thermo == SCFD_THERMO_IDEAL && d->ny != 1) return SCFD_E_ARG;
+    if (d->thermo == SCFD_THERMO_CHEMKIN_REACTIVE && d->dt_mode == SCFD_DT_LOCAL) return SCFD_E_UNSUPPORTED;
+    auto* c = new scfd_ctx();
+    c->d = *d;
+    c->np = d->nplane;
+    c->nY = d->ny;
+    c->D = c->nY + 3;
+    c->W = c->D + 5;
+    c->P.np = c->np;
+    long long base = 0;
+    for (int p = 0; p < c->np; ++p) {
+        const int ni = d->ni[p], nj = d->nj[p];
+        if (ni < 2 || nj < 2) {
+            delete c;
+            return SCFD_E_ARG;
+        }
+        c->P.ni[p] = ni;
+        c->P.nj[p] = nj;
+        c->P.pitch[p] = (ni + 4 + 31) / 32 * 32;
+        c->P.base[p] = base;
+        base += (long long)(nj + 4) * c->P.pitch[p];
+        base = (base + 31) / 32 * 32;
+        c->nimax = std::max(c->nimax, ni);
+        c->njmax = std::max(c->njmax, nj);
+        c->cells_max = std::max(c->cells_max, ni * nj);
+    }
+    c->ncell = base;
+    c->xh.resize(c->np);
+    c->rh.resize(c->np);
+    c->geo_set.assign(c->np, 0);
+    *out = c;
+    return 0;
+}
+
+int scfd_destroy(scfd_ctx* c) {
+    if (!c) return SCFD_E_ARG;
+    if (c->arena) cudaFree(c->arena);
+    if (c->h_sc) cudaFreeHost(c->h_sc);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return 0;
+}
+
+int scfd_last_error(const scfd_ctx* c, char* buf, int len) {
+    if (!c || !buf || len <= 0) return SCFD_E_ARG;
+    std::snprintf(buf, (size_t)len, "%s", c->err.c_str());
+    return 0;
+}
+
+int scfd_set_geometry(scfd_ctx* c, int plane, const double* xh, const double* rh) {
+    if (!c || plane < 1 || plane > c->np || !xh || !rh) return SCFD_E_ARG;
+    if (c->committed) return c->fail(SCFD_E_STATE, "geometry after commit");
+    const size_t n = (size_t)(c->P.ni[plane - 1] + 1) * (c->P.nj[plane - 1] + 1);
+    c->xh[plane - 1].assign(xh, xh + n);
+    c->rh[plane - 1].assign(rh, rh + n);
+    c->geo_set[plane - 1] = 1;
+    return 0;
+}
+
+int scfd_set_connectivity(scfd_ctx* c, const int32_t* recs, int n) {
+    if (!c || n < 0 || (n > 0 && !recs)) return SCFD_E_ARG;
+    if (c->committed) return c->fail(SCFD_E_STATE, "connectivity after commit");
+    c->cut.assign(recs, recs + 11 * (size_t)n);
+    return 0;
+}
+
+int scfd_set_bc(scfd_ctx* c, const scfd_bc* b, int n) {
+    if (!c || n < 0 || (n > 0 && !b)) return SCFD_E_ARG;
+    if (c->committed) return c->fail(SCFD_E_STATE, "boundaries after commit");
+    for (int k = 0; k < n; ++k) {
+        const scfd_bc& x = b[k];
+        if (x.plane < 1 || x.plane > c->np || x.side < 0 || x.side > 3 || x.kind < 0 || x.kind > SCFD_BC_FIXED_PIN)
+            return c->fail(SCFD_E_ARG, "bad boundary descriptor " + std::to_string(k));
+        const int len = (x.side <= SCFD_SIDE_IHI) ? c->P.nj[x.plane - 1] : c->P.ni[x.plane - 1];
+        if (x.first < 1 || x.last > len || x.first > x.last)
+            return c->fail(SCFD_E_ARG, "boundary descriptor range " + std::to_string(k));
+    }
+    c->bcs.assign(b, b + n);
+    return 0;
+}
+
+int scfd_set_chem(scfd_ctx* c, const scfd_chem* ch) {
+    if (!c || !ch) return SCFD_E_ARG;
+    if (ch->ns != c->nY || ch->nr < 1 || ch->nr > SCFD_MAX_REACTIONS || ch->nt < 0 || ch->nt > ch->ns)
+        return c->fail(SCFD_E_ARG, "chemistry tables do not match nY");
+    c->chem = *ch;
+    c->have_chem = true;
+    return 0;
+}
+
+int scfd_commit(scfd_ctx* c) {
+    if (!c) return SCFD_E_ARG;
+    if (c->committed) return c->fail(SCFD_E_STATE, "commit called twice");
+    for (int p = 0; p < c->np; ++p)
+        if (!c->geo_set[p]) return c->fail(SCFD_E_STATE, "geometry of plane " + std::to_string(p + 1) + " not set");
+    if (c->d.thermo != SCFD_THERMO_IDEAL && !c->have_chem) return c->fail(SCFD_E_STATE, "chemistry tables not set");
+    CK(cudaGetDevice(&c->device));
+    CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->device));
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    HostGeo g;
+    build_geometry(c, g);
+    std::vector<GhostOp> ops;
+    int st = build_ghost_ops(c, g, ops);
+    if (st) return st;
+    c->nops = (int)ops.size();
+    // strips for the sweeps
+    std::vector<int> sf, sb;
+    for (int p = 0; p < c->np; ++p) {
+        const int ns = (c->P.nj[p] + 31) / 32;
+        for (int s = 0; s < ns; ++s) {
+            sf.push_back(p);
+            sf.push_back(s);
+        }
+    }
+    sb = sf;
+    c->nsf = (int)sf.size() / 2;
+    c->nsb = c->nsf;
+    const long long N = c->ncell;
+    const int D = c->D, W = c->W, nY = c->nY;
+    const bool mixed = c->d.precision == SCFD_PREC_MIXED;
+    const bool impl = c->d.scheme != SCFD_SCHEME_EULER;
+    // chemistry tables, compact
+    std::vector<double> ccoeff, ctc, cinv, cmw, cmen, cabe, ccabe, ctroe, ctrange, ctrans, cwc1, cwc2;
+    std::vector<int> crs, cind, cnum, csnu, cex, cnm, cim, ctr, cns;
+    int ns = 0, nr = 0, nt = 0;
+    if (c->have_chem) {
+        const scfd_chem& h = c->chem;
+        ns = h.ns; nr = h.nr; nt = h.nt;
+        for (int k = 0; k < ns; ++k) {
+            for (int s = 0; s < 2; ++s)
+                for (int i = 0; i < 7; ++i) ccoeff.push_back(h.coeff[k][s][i]);
+            ctc.push_back(h.tthre[k][2]);
+            cinv.push_back(1.0 / h.mws[k]);
+            cmw.push_back(h.mws[k]);
+        }
+        for (int i = 0; i < nr; ++i) {
+            crs.push_back(h.rstate[i][0]); crs.push_back(h.rstate[i][1]);
+            for (int s = 0; s < 2; ++s)
+                for (int k = 0; k < 3; ++k) cind.push_back(h.indnu[i][s][k]);
+            cnum.push_back(h.numnu[i][0]); cnum.push_back(h.numnu[i][1]);
+            csnu.push_back(h.snu[i]);
+            cex.push_back(h.exist_m[i]);
+            cnm.push_back(h.numm[i]);
+            for (int k = 0; k < ns; ++k) {
+                cim.push_back(h.indm[i][k]);
+                cmen.push_back(h.men[i][k]);
+            }
+            for (int k = 0; k < 3; ++k) { cabe.push_back(h.abe[i][k]); ccabe.push_back(h.cabe[i][k]); }
+            for (int k = 0; k < 4; ++k) ctroe.push_back(h.troe[i][k]);
+        }
+        for (int i = 0; i < nt; ++i) {
+            ctr.push_back(h.tr2th[i]);
+            cns.push_back(h.num_sctn_trans[i]);
+            for (int l = 0; l < 5; ++l) {
+                for (int m = 0; m < 2; ++m) ctrange.push_back(h.trange_trans[i][l][m]);
+                for (int m = 0; m < 4; ++m) ctrans.push_back(h.trans[i][l][m]);
+            }
+        }
+        for (int i = 0; i < nt; ++i)
+            for (int j = 0; j < nt; ++j) {
+                const double mi = h.mws[h.tr2th[i]], mj = h.mws[h.tr2th[j]];
+                cwc1.push_back(std::pow(mj / mi, 0.25));
+                cwc2.push_back(std::sqrt(2.0 * mj / (mi + mj)));
+            }
+    }
+    const int nrec = 64 * c->np;
+    // arena size
+    size_t bytes = 0;
+    bytes += 3 * need<double>(D * N);                         // q, qp, qpp
+    bytes += need<double>(W * N) + 2 * need<double>(nY * N);  // w, vhi, DHi
+    bytes += need<double>(D * N);                             // Dq
+    bytes += 4 * need<double>(N);                             // dt_mat, alpha, nuA, nuB
+    bytes += 8 * need<double>(N) + 4 * need<double>(2 * N) + 3 * need<double>(4 * N);  // geometry
+    if (mixed) bytes += need<float>(W * N) + need<float>(nY * N);
+    bytes += need<DevScalars>(1);
+    bytes += 2 * need<int>(2 * c->nsf);
+    bytes += need<double>((size_t)c->nsf * c->nimax * D);
+    bytes += need<int>(c->nsf + c->nsb) + need<int>(2) + need<double>(2 * c->nsb);
+    bytes += need<GhostOp>(std::max(1, c->nops)) + need<double>(std::max<size_t>(1, c->bcs.size()) * c->valstride);
+    bytes += need<unsigned long long>(1) + need<double>(nrec) + need<double>(1);
+    bytes += need<double>(ccoeff.size() + ctc.size() + cinv.size() + cmw.size() + cmen.size() + cabe.size() +
+                          ccabe.size() + ctroe.size() + ctrange.size() + ctrans.size() + cwc1.size() + cwc2.size() + 64);
+    bytes += need<int>(crs.size() + cind.size() + cnum.size() + csnu.size() + cex.size() + cnm.size() + cim.size() +
+                       ctr.size() + cns.size() + 64);
+    bytes += 64 * 256;
+    c->arena_bytes = bytes;
+    CK(cudaMalloc(&c->arena, bytes));
+    CK(cudaMemsetAsync(c->arena, 0, bytes, c->stream));
+    char* p = c->arena;
+    View& v = c->v;
+    v.P = c->P;
+    v.ncell = N;
+    v.nY = nY; v.D = D; v.W = W;
+    v.dim = c->d.dim; v.viscous = c->d.viscous; v.recon = c->d.recon; v.thermo = c->d.thermo;
+    v.mu_model = c->d.mu_model; v.scheme = c->d.scheme; v.dt_mode = c->d.dt_mode; v.precision = c->d.precision;
+    v.phi_mus = c->d.phi_mus; v.k_mus = c->d.k_mus; v.kappa = c->d.kappa; v.rgas = c->d.rgas; v.nu_gas = c->d.nu_gas;
+    v.suth_mu0 = c->d.suth_mu0; v.suth_t0 = c->d.suth_t0; v.suth_s = c->d.suth_s;
+    v.prandtl = c->d.prandtl; v.schmidt = c->d.schmidt; v.cfl = c->d.cfl; v.dt_fixed = c->d.dt_fixed;
+    v.omega_max = c->d.omega_max; v.omega_min = c->d.omega_min; v.dq_max = c->d.dq_max;
+    v.q = carve<double>(p, D * N); v.qp = carve<double>(p, D * N); v.qpp = carve<double>(p, D * N);
+    v.w = carve<double>(p, W * N); v.vhi = carve<double>(p, nY * N); v.DHi = carve<double>(p, nY * N);
+    v.Dq = carve<double>(p, D * N);
+    v.dt_mat = carve<double>(p, N); v.alpha = carve<double>(p, N); v.nuA = carve<double>(p, N); v.nuB = carve<double>(p, N);
+    v.Vol = carve<double>(p, N); v.Area = carve<double>(p, N); v.dsi = carve<double>(p, N); v.dsj = carve<double>(p, N);
+    v.x = carve<double>(p, N); v.r = carve<double>(p, N); v.dsci = carve<double>(p, N); v.dscj = carve<double>(p, N);
+    v.vni = carve<double>(p, 2 * N); v.vnj = carve<double>(p, 2 * N); v.vnci = carve<double>(p, 2 * N); v.vncj = carve<double>(p, 2 * N);
+    v.gjc = carve<double>(p, 4 * N); v.gji = carve<double>(p, 4 * N); v.gjj = carve<double>(p, 4 * N);
+    if (mixed) {
+        v.w32 = carve<float>(p, W * N);
+        v.vhi32 = carve<float>(p, nY * N);
+    }
+    c->d_sc = carve<DevScalars>(p, 1);
+    v.sc = c->d_sc;
+    c->d_strips_f = carve<int>(p, 2 * c->nsf);
+    c->d_strips_b = carve<int>(p, 2 * c->nsb);
+    c->d_xfer = carve<double>(p, (size_t)c->nsf * c->nimax * D);
+    c->d_progress = carve<int>(p, c->nsf + c->nsb);
+    c->d_tickets = carve<int>(p, 2);
+    c->d_partials = carve<double>(p, 2 * c->nsb);
+    c->d_ops = carve<GhostOp>(p, std::max(1, c->nops));
+    c->d_bcval = carve<double>(p, std::max<size_t>(1, c->bcs.size()) * c->valstride);
+    c->d_counter = carve<unsigned long long>(p, 1);
+    c->d_rms_partial = carve<double>(p, nrec);
+    c->d_rms_out = carve<double>(p, 1);
+    auto upd = [&](const std::vector<double>& h) -> const double* {
+        double* d = carve<double>(p, std::max<size_t>(1, h.size()));
+        if (!h.empty()) cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+        return d;
+    };
+    auto upi = [&](const std::vector<int>& h) -> const int* {
+        int* d = carve<int>(p, std::max<size_t>(1, h.size()));
+        if (!h.empty()) cudaMemcpyAsync(d, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+        return d;
+    };
+    if (p > c->arena + c->arena_bytes) return c->fail(SCFD_E_CUDA, "arena overflow");
+    // geometry upload
+    auto up = [&](double* d, const std::vector<double>& h) {
+        return cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    };
+    CK(up(v.Vol, g.Vol)); CK(up(v.Area, g.Area)); CK(up(v.dsi, g.dsi)); CK(up(v.dsj, g.dsj));
+    CK(up(v.vni, g.vni)); CK(up(v.vnj, g.vnj)); CK(up(v.x, g.x)); CK(up(v.r, g.r));
+    CK(up(v.gjc, g.gjc)); CK(up(v.gji, g.gji)); CK(up(v.gjj, g.gjj)); CK(up(v.dsci, g.dsci)); CK(up(v.dscj, g.dscj));
+    CK(up(v.vnci, g.vnci)); CK(up(v.vncj, g.vncj));
+    CK(cudaMemcpyAsync(c->d_strips_f, sf.data(), sf.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_strips_b, sb.data(), sb.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    if (c->nops)
+        CK(cudaMemcpyAsync(c->d_ops, ops.data(), ops.size() * sizeof(GhostOp), cudaMemcpyHostToDevice, c->stream));
+    if (!c->bcs.empty()) {
+        std::vector<double> val(c->bcs.size() * c->valstride);
+        for (size_t k = 0; k < c->bcs.size(); ++k)
+            std::memcpy(&val[k * c->valstride], c->bcs[k].value, sizeof(double) * c->valstride);
+        CK(cudaMemcpyAsync(c->d_bcval, val.data(), val.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if (c->have_chem) {
+        DevChem& ch = v.chem;
+        ch.ns = ns; ch.nr = nr; ch.nt = nt;
+        ch.coeff = upd(ccoeff); ch.tcommon = upd(ctc); ch.inv_mw = upd(cinv); ch.mws = upd(cmw);
+        ch.rstate = upi(crs); ch.indnu = upi(cind); ch.numnu = upi(cnum); ch.snu = upi(csnu); ch.exist_m = upi(cex);
+        ch.numm = upi(cnm); ch.indm = upi(cim); ch.men = upd(cmen); ch.abe = upd(cabe); ch.cabe = upd(ccabe);
+        ch.troe = upd(ctroe); ch.tr2th = upi(ctr); ch.nsec = upi(cns); ch.trange = upd(ctrange); ch.trans = upd(ctrans);
+        ch.wc1 = upd(cwc1); ch.wc2 = upd(cwc2);
+        ch.rtol = c->chem.rtol;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if (p > c->arena + c->arena_bytes) return c->fail(SCFD_E_CUDA, "arena overflow");
+    CK(cudaMallocHost(&c->h_sc, sizeof(DevScalars)));
+    c->stage_doubles = (size_t)std::max(W, D) * (c->nimax + 4) * (c->njmax + 4) * c->np;
+    CK(cudaMallocHost(&c->h_stage, c->stage_doubles * sizeof(double)));
+    CK(cudaStreamSynchronize(c->stream));
+    (void)impl;
+    c->committed = true;
+    return 0;
+}
+
+// reference layout f(k, -1:nimax+2, -1:njmax+2, plane) <-> SoA slots
+static void ref_to_soa(const scfd_ctx* c, const double* ref, int nk, double* soa) {
+    const int IX = c->nimax + 4, JX = c->njmax + 4;
+    const long long N = c->ncell;
+    for (int p = 0; p < c->np; ++p)
+        for (int j = -1; j <= c->P.nj[p] + 2; ++j)
+            for (int i = -1; i <= c->P.ni[p] + 2; ++i) {
+                const double* src = ref + (size_t)nk * ((i + 1) + (size_t)IX * ((j + 1) + (size_t)JX * p));
+                const long long cc = cidx(c->P, p, i, j);
+                for (int k = 0; k < nk; ++k) soa[k * N + cc] = src[k];
+            }
+}
+static void soa_to_ref(const scfd_ctx* c, const double* soa, int nk, double* ref) {
+    const int IX = c->nimax + 4, JX = c->njmax + 4;
+    const long long N = c->ncell;
+    for (int p = 0; p < c->np; ++p)
+        for (int j = -1; j <= c->P.nj[p] + 2; ++j)
+            for (int i = -1; i <= c->P.ni[p] + 2; ++i) {
+                double* dst = ref + (size_t)nk * ((i + 1) + (size_t)IX * ((j + 1) + (size_t)JX * p));
+                const long long cc = cidx(c->P, p, i, j);
+                for (int k = 0; k < nk; ++k) dst[k] = soa[k * N + cc];
+            }
+}
+
+static int upload_field(scfd_ctx* c, const double* ref, int nk, double* dev) {
+    std::fill(c->h_stage, c->h_stage + (size_t)nk * c->ncell, 0.0);
+    ref_to_soa(c, ref, nk, c->h_stage);
+    CK(cudaMemcpyAsync(dev, c->h_stage, sizeof(double) * nk * c->ncell, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+static int download_field(scfd_ctx* c, const double* dev, int nk, double* ref) {
+    CK(cudaMemcpyAsync(c->h_stage, dev, sizeof(double) * nk * c->ncell, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    soa_to_ref(c, c->h_stage, nk, ref);
+    return 0;
+}
+
+int scfd_upload(scfd_ctx* c, const double* q, const double* w, const double* vhi, double tt) {
+    if (!c || !q || !w) return SCFD_E_ARG;
+    if (!c->committed) return c->fail(SCFD_E_STATE, "upload before commit");
+    if (c->stage_doubles < (size_t)std::max(c->W, c->D) * c->ncell) {
+        cudaFreeHost(c->h_stage);
+        c->stage_doubles = (size_t)std::max(c->W, c->D) * c->ncell;
+        CK(cudaMallocHost(&c->h_stage, c->stage_doubles * sizeof(double)));
+    }
+    int st;
+    if ((st = upload_field(c, q, c->D, c->v.q))) return st;
+    if ((st = upload_field(c, w, c->W, c->v.w))) return st;
+    if (vhi && (st = upload_field(c, vhi, c->nY, c->v.vhi))) return st;
+    const long long qb = sizeof(double) * (long long)c->D * c->ncell;
+    CK(cudaMemcpyAsync(c->v.qp, c->v.q, qb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->v.qpp, c->v.q, qb, cudaMemcpyDeviceToDevice, c->stream));
+    DevScalars h{};
+    h.tt = tt;
+    h.first_dual = 1;
+    h.res1 = 1.0;
+    CK(cudaMemcpyAsync(c->d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->uploaded = true;
+    return 0;
+}
+
+int scfd_prepare(scfd_ctx* c, int step) {
+    if (!c || !c->committed || !c->uploaded) return c ? c->fail(SCFD_E_STATE, "prepare before upload") : SCFD_E_ARG;
+    (void)step;
+    c->launches = 0;
+    c->launches += launch_thermo(c->v, c->stream, c->cells_max);
+    c->launches += launch_ghosts(c->v, c->stream, c->d_ops, c->nops, c->d_bcval, c->valstride);
+    CK(cudaGetLastError());
+    int st = sync_scalars(c);
+    if (st) return st;
+    return c->h_sc->status;
+}
+
+int scfd_step(scfd_ctx* c, int step, scfd_stats* stats) {
+    if (!c || !c->committed || !c->uploaded) return c ? c->fail(SCFD_E_STATE, "step before upload") : SCFD_E_ARG;
+    (void)step;
+    int st = sync_scalars(c);
+    if (st) return st;
+    const long long att0 = c->h_sc->chem_attempts, fb0 = c->h_sc->chem_fallback;
+    c->launches = 0;
+    if ((st = enqueue_step(c))) return st;
+    if ((st = sync_scalars(c))) return st;
+    return fill_stats(c, stats, att0, fb0);
+}
+
+int scfd_run(scfd_ctx* c, int step, int nsteps, scfd_stats* stats) {
+    if (!c || !c->committed || !c->uploaded) return c ? c->fail(SCFD_E_STATE, "run before upload") : SCFD_E_ARG;
+    (void)step;
+    int st = sync_scalars(c);
+    if (st) return st;
+    const long long att0 = c->h_sc->chem_attempts, fb0 = c->h_sc->chem_fallback;
+    c->launches = 0;
+    for (int n = 0; n < nsteps; ++n)
+        if ((st = enqueue_step(c))) return st;
+    if ((st = sync_scalars(c))) return st;
+    return fill_stats(c, stats, att0, fb0);
+}
+
+int scfd_rms(scfd_ctx* c, double* rms) {
+    if (!c || !rms || !c->committed) return SCFD_E_ARG;
+    launch_rms(c->v, c->stream, c->d_rms_partial, c->d_rms_out);
+    CK(cudaMemcpyAsync(rms, c->d_rms_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return (*rms != *rms) ? SCFD_E_NAN : 0;
+}
+
+int scfd_download(scfd_ctx* c, double* q, double* w, double* vhi, double* tt) {
+    if (!c || !c->committed) return SCFD_E_ARG;
+    int st;
+    if (q && (st = download_field(c, c->v.q, c->D, q))) return st;
+    if (w && (st = download_field(c, c->v.w, c->W, w))) return st;
+    if (vhi && (st = download_field(c, c->v.vhi, c->nY, vhi))) return st;
+    if (tt) {
+        if ((st = sync_scalars(c))) return st;
+        *tt = c->h_sc->tt;
+    }
+    return 0;
+}
+
+int scfd_download_qp(scfd_ctx* c, double* qp) {
+    if (!c || !c->committed || !qp) return SCFD_E_ARG;
+    return download_field(c, c->v.qp, c->D, qp);
+}
+
+int scfd_get_stream(scfd_ctx* c, void** s) {
+    if (!c || !s) return SCFD_E_ARG;
+    *s = (void*)c->stream;
+    return 0;
+}
+
+int scfd_launch_count(const scfd_ctx* c, int64_t* n) {
+    if (!c || !n) return SCFD_E_ARG;
+    *n = c->launches;
+    return 0;
+}
+
+}  // extern "C"

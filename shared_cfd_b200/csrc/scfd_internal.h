@@ -1,0 +1,125 @@
+// scfd_internal.h -- device data layout and kernel interfaces of the B200
+// path.  Everything here is private to libscfd_b200.so.
+//
+// Layout in HBM (one arena per context):
+//   * A "cell slot" index c addresses cell (i,j) of plane p for i = -1..ni+2,
+//     j = -1..nj+2 (two ghost layers, as q(.., -1:nimax+2, -1:njmax+2, ..)):
+//         c = base[p] + (j + 2) * pitch[p] + (i + 2),
+//     pitch[p] = round_up(ni + 4, 32) so rows start on 256-byte boundaries.
+//     Planes follow each other; all planes are resident together.
+//   * Every field is structure-of-arrays: component k of field F lives at
+//     F[k * ncell + c].  Face quantities of face i+1/2 (resp. j+1/2) are stored
+//     in the slot of cell i (resp. j), so dsi(i,j) -> dsi[c(i,j)].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/scfd_b200.h"
+
+namespace scfd {
+
+constexpr int kMaxPlanes = SCFD_MAX_PLANES;
+constexpr int kMaxSpecies = SCFD_MAX_SPECIES;
+
+struct Planes {
+    int np;
+    int ni[kMaxPlanes];
+    int nj[kMaxPlanes];
+    int pitch[kMaxPlanes];
+    long long base[kMaxPlanes];
+};
+
+__host__ __device__ inline long long cidx(const Planes& P, int p, int i, int j) {
+    return P.base[p] + (long long)(j + 2) * P.pitch[p] + (i + 2);
+}
+
+// Compact chemistry tables on the device (0-based species).
+struct DevChem {
+    int ns, nr, nt;
+    const double* coeff;      // [ns][2][7]
+    const double* tcommon;    // [ns] Tthre(3,k)
+    const double* inv_mw;     // [ns] 1/MW (computed as 1d0/MWs like invMW)
+    const double* mws;        // [ns]
+    const int* rstate;        // [nr][2]
+    const int* indnu;         // [nr][2][3]
+    const int* numnu;         // [nr][2]
+    const int* snu;           // [nr]
+    const int* exist_m;       // [nr]
+    const int* numm;          // [nr]
+    const int* indm;          // [nr][ns]
+    const double* men;        // [nr][ns]
+    const double* abe;        // [nr][3]
+    const double* cabe;       // [nr][3]
+    const double* troe;       // [nr][4]
+    const int* tr2th;         // [nt]
+    const int* nsec;          // [nt]
+    const double* trange;     // [nt][5][2]
+    const double* trans;      // [nt][5][4]
+    const double* wc1;        // [nt][nt] (MW(jt)/MW(it))**0.25
+    const double* wc2;        // [nt][nt] sqrt(2 MW(jt)/(MW(it)+MW(jt)))
+    double rtol;
+};
+
+// Scalars that live on the device between kernels of one step.
+struct DevScalars {
+    double dt_grbl;
+    double tt;
+    double omega;          // omega applied by the last NR update
+    double res;            // last inner residual
+    double res1;           // first inner residual of the step
+    unsigned long long dtmin_bits;  // atomicMin target for the global dt
+    int status;            // SCFD_* code, atomicMax
+    int first_dual;
+    long long chem_attempts;
+    long long chem_fallback;
+    unsigned long long spin_abort;  // non-zero once a bounded wait gave up
+};
+
+// All device pointers of a context; passed by value to the kernels.
+struct View {
+    Planes P;
+    long long ncell;
+    int nY, D, W;
+    int dim, viscous, recon, thermo, mu_model, scheme, dt_mode, precision;
+    double phi_mus, k_mus, kappa, rgas, nu_gas, suth_mu0, suth_t0, suth_s, prandtl, schmidt, cfl, dt_fixed;
+    double omega_max, omega_min, dq_max;
+    // state
+    double *q, *qp, *qpp, *w, *vhi, *DHi, *Dq, *dt_mat;
+    double *alpha, *nuA, *nuB;   // LU-SGS coefficients per cell
+    // geometry
+    double *Vol, *Area, *dsi, *dsj, *vni, *vnj, *x, *r, *gjc, *gji, *gjj, *dsci, *dscj, *vnci, *vncj;
+    // mixed-precision copies used by the FP32 residual / sweeps
+    float *w32, *vhi32;
+    DevScalars* sc;
+    DevChem chem;
+};
+
+// One ghost-cell write of set_BC (halo copy or boundary descriptor).
+struct GhostOp {
+    long long dst;   // ghost cell slot
+    long long src;   // interior cell slot read
+    int kind;        // -1 halo copy, else SCFD_BC_*
+    int bc;          // descriptor index for values
+    double n1, n2;   // boundary face normal (SLIP)
+};
+
+// kernels / launchers (stream-ordered); each returns the number of launches
+int launch_thermo(const View& v, cudaStream_t s, int cells_per_plane_max);
+int launch_ghosts(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride);
+int launch_set_dt(const View& v, cudaStream_t s);
+int launch_residual(const View& v, cudaStream_t s, int mode);
+int launch_sweeps(const View& v, cudaStream_t s, double* xfer, int* progress, double* partials,
+                  int* tickets, int nstrips_fwd, int nstrips_bwd, const int* strip_tab_f, const int* strip_tab_b);
+int launch_nr_update(const View& v, cudaStream_t s, const double* partials, int nstrips, int inner);
+int launch_chem_impl(const View& v, cudaStream_t s, int max_substeps, unsigned long long* counter, int nsm);
+int launch_step_end(const View& v, cudaStream_t s, double warn, double err);
+int launch_rms(const View& v, cudaStream_t s, double* partial, double* out);
+int launch_copy(double* dst, const double* src, long long n, cudaStream_t s);
+int launch_scalar_begin(const View& v, cudaStream_t s);
+int launch_to_f32(const View& v, cudaStream_t s);
+
+// residual modes
+enum { RES_EULER = 0, RES_LUSGS = 1, RES_NR = 2 };
+
+}  // namespace scfd

@@ -1,0 +1,128 @@
+"""Parity of the CUDA path (called through the C ABI) with the CPU
+restatement of the reference, on seeded inputs at sizes the restatement
+finishes in seconds.
+
+Tolerance for the plain (FP64) path: 1e-10 relative L2 of the conserved
+variables after the stated step count.  Halo indexing is checked bit-exactly.
+"""
+import numpy as np
+import pytest
+
+from shared_cfd_b200 import abi, cases
+from shared_cfd_b200.solver import Solver
+
+from helpers import rel_l2, rel_l2_per_component, run_case
+
+TOL_FP64 = 1e-10
+
+pytestmark = pytest.mark.gpu
+
+
+def _parity(case, gpu, orc, n, tol=TOL_FP64):
+    a = run_case(case, gpu, n)
+    b = run_case(case, orc, n)
+    assert a["stats"] is None or a["stats"].status == 0
+    assert np.isfinite(a["q"]).all()
+    err = rel_l2(case, a["q"], b["q"])
+    errk, _ = rel_l2_per_component(case, a["q"], b["q"])
+    assert err <= tol, "rel L2 %g" % err
+    assert errk <= 100 * tol, "per-component rel L2 %g" % errk
+    return a, b, err
+
+
+def test_sod_200_steps(gpu, orc):
+    case = cases.sod()
+    a, b, err = _parity(case, gpu, orc, 200)
+    assert abs(a["tt"] - b["tt"]) <= 1e-12 * b["tt"]
+
+
+@pytest.mark.parametrize("orientation", [0, 1, 2, 3])
+def test_forward_step_euler_halo(gpu, orc, orientation):
+    case = cases.perturb(cases.forward_step(orientation, n=10), seed=orientation)
+    _parity(case, gpu, orc, 30)
+
+
+@pytest.mark.parametrize("orientation", [0, 1, 2, 3])
+def test_forward_step_lusgs_local_dt(gpu, orc, orientation):
+    case = cases.perturb(cases.forward_step(orientation, n=10, scheme=abi.SCHEME_LUSGS, dt_mode=abi.DT_LOCAL,
+                                            viscous=1), seed=10 + orientation)
+    case.desc.cfl = 2.0
+    _parity(case, gpu, orc, 10)
+
+
+def test_flat_plate_lusgs(gpu, orc):
+    case = cases.flat_plate(48, 40)
+    _parity(case, gpu, orc, 20)
+
+
+def test_nr_q2d_viscous_ideal(gpu, orc):
+    case = cases.perturb(cases.forward_step(0, n=12, scheme=abi.SCHEME_NR, dt_mode=abi.DT_GLOBAL, viscous=1,
+                                            dim=abi.DIM_Q2D), seed=7)
+    case.desc.num_internal_loop = 6
+    case.desc.res_rate_err = 1e300
+    case.desc.omega_min = 0.0
+    _parity(case, gpu, orc, 3)
+
+
+def test_lusgs_wide_strips(gpu, orc):
+    """More than one 32-row strip per plane and a partial last strip."""
+    case = cases.perturb(cases.forward_step(1, n=37, scheme=abi.SCHEME_LUSGS, dt_mode=abi.DT_LOCAL), seed=3)
+    case.desc.cfl = 3.0
+    _parity(case, gpu, orc, 4)
+
+
+def test_reacting_step_small(gpu, orc):
+    case = cases.reacting_step(scale=1.0 / 32.0, inner=4)
+    _parity(case, gpu, orc, 2)
+
+
+def test_halo_indexing_bit_exact(gpu, orc):
+    """Ghost cells written by the halo copy and the boundary descriptors hold
+    bit-identical values on both paths: q carries a unique density per cell
+    and w(1) = q(1) exactly for the ideal gas."""
+    for orientation in range(4):
+        case = cases.forward_step(orientation, n=9)
+        for p in range(2):
+            nj, ni = case.nj[p], case.ni[p]
+            jj, ii = np.meshgrid(np.arange(nj + 4), np.arange(ni + 4), indexing="ij")
+            case.q[p, :nj + 4, :ni + 4, 0] = 1.0 + 1e-3 * (p * 10000 + jj * 100 + ii)
+        a = run_case(case, gpu, 0)
+        b = run_case(case, orc, 0)
+        for p in range(2):
+            nj, ni = case.nj[p], case.ni[p]
+            ga = a["w"][p, :nj + 4, :ni + 4, 0]
+            gb = b["w"][p, :nj + 4, :ni + 4, 0]
+            assert np.array_equal(ga[1:-1, 1:-1], gb[1:-1, 1:-1]), "orientation %d plane %d" % (orientation, p)
+            assert np.array_equal(ga[2:-2, 0], gb[2:-2, 0]) and np.array_equal(ga[0, 2:-2], gb[0, 2:-2])
+
+
+def test_mixed_precision_error_is_stated(gpu, orc):
+    """The FP32-reconstruction path stays close to the FP64 restatement."""
+    case = cases.flat_plate(48, 40)
+    b = run_case(case, orc, 20)
+    case.desc.precision = abi.PREC_MIXED
+    a = run_case(case, gpu, 20)
+    err = rel_l2(case, a["q"], b["q"])
+    assert err < 1e-4, err
+
+
+def test_nan_is_reported(gpu):
+    case = cases.sod(40, 4)
+    case.q[0, 5, 10, 3] = np.nan
+    s = Solver(case, lib=gpu)
+    s.upload()
+    s.prepare(1)
+    s.run(1, 1, check=False)
+    with pytest.raises(Exception):
+        s.rms()
+    s.close()
+
+
+def test_launch_count_positive(gpu):
+    case = cases.sod(40, 4)
+    s = Solver(case, lib=gpu)
+    s.upload()
+    s.prepare(1)
+    s.run(1, 3)
+    assert s.launch_count() >= 3 * 4
+    s.close()
