@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Benchmark of the per-step residual-and-implicit-update path on B200.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
+                    [--config reacting_step|flat_plate|sod] [--scale S]
+
+Metric: Mcell-iter/s (cells x inner iterations per second; for the explicit
+Euler configuration one step is one iteration), mixed (FP32 reconstruction,
+fluxes and sweeps) and plain FP64.  `value` is the mixed path with the state
+resident in HBM; `fp64_value` the plain path; `e2e` the same metric through the
+C ABI with host buffers copied in and the result copied out every step.
+
+One JSON line is printed by rank 0.  Under torchrun every rank runs its own
+replica of the workload on its own GPU (weak scaling, no data exchange) and
+the time is the maximum over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from shared_cfd_b200 import abi, cases  # noqa: E402
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_case(config, scale, precision):
+    if config == "reacting_step":
+        return cases.reacting_step(scale=scale, precision=precision)
+    if config == "flat_plate":
+        return cases.flat_plate(int(round(256 * scale)), int(round(128 * scale)), precision=precision)
+    return cases.sod(int(round(400 * scale)), 4, precision=precision)
+
+
+def iters_per_step(case):
+    return max(1, case.desc.num_internal_loop - 1) if case.desc.scheme == abi.SCHEME_NR else 1
+
+
+def workload_name(config, scale):
+    return {"reacting_step": "axisymmetric reacting backward-facing step, 4 blocks 2x512^2+2x512x256, "
+                             "9 species / 19 seeded reactions, NR dual time dt=1e-7 s, 20 inner iterations",
+            "flat_plate": "supersonic laminar flat plate 256x128, N2 Sutherland Pr=0.72, LU-SGS local dt",
+            "sod": "Sod shock tube 400x4, MUSCL+SLAU, explicit Euler CFL 0.5"}[config] + \
+        ("" if scale == 1.0 else " (scale %g)" % scale)
+
+
+# algorithmic HBM bytes per interior cell and launch, FP64 storage
+def algo_bytes(kind, case, mixed):
+    nY, D, W = case.nY, case.D, case.W
+    nr = case.desc.scheme == abi.SCHEME_NR
+    wb = 4 if mixed else 8
+    if kind == abi.K_THERMO:
+        return 8 * ((D + 2) + W + 2 * nY)
+    if kind == abi.K_RESIDUAL:
+        geo = 28 if case.desc.viscous else 14
+        return wb * (W + nY) + 8 * ((3 * D if nr else 2 * D) + geo + D + 3)
+    if kind in (abi.K_SWEEP_FWD, abi.K_SWEEP_BWD):
+        return 8 * (D + 1 + 4 + 2 * nY + 2 + 4 + 2 + 1 + D + (nY if kind == abi.K_SWEEP_BWD else 0))
+    if kind == abi.K_UPDATE:
+        return 8 * 3 * D
+    if kind == abi.K_BC:
+        return 0
+    if kind == abi.K_CHEM:
+        return 8 * (2 * nY + 3)
+    return 0
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.f.flush()
+
+    def summary(self):
+        try:
+            with open(self.f.name) as f:
+                rows = [r.split(",") for r in f.read().strip().splitlines() if r.strip()]
+            os.unlink(self.f.name)
+        except OSError:
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                mx = float(r[1])
+                for k, nm in enumerate(names):
+                    if r[4 + k].strip().lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def time_resident(solver, steps, warmup, torch, dev, sampler_dev, barrier):
+    """Device time of `steps` steps with the state resident (CUDA events on the
+    library's stream), after `warmup` untimed steps."""
+    stream = torch.cuda.ExternalStream(solver.stream(), device=dev)
+    if warmup:
+        solver.run(1, warmup)
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(sampler_dev) as cs:
+        e0.record(stream)
+        st = solver.run(1 + warmup, steps)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier()
+    return e0.elapsed_time(e1), st, solver.launch_count(), cs.summary()
+
+
+def kernel_profile(solver, steps, case, mixed):
+    lib = solver.lib
+    lib.profile(solver.ctx, 1)
+    solver.run(100, steps)
+    out = {}
+    for k in range(abi.K_COUNT):
+        ms = C.c_double()
+        n = C.c_int64()
+        name = C.create_string_buffer(32)
+        lib.kernel_stats(solver.ctx, k, C.byref(ms), C.byref(n), name, 32)
+        if n.value:
+            out[name.value.decode()] = {"kind": k, "total_ms": ms.value, "launches": n.value,
+                                        "avg_ms": ms.value / n.value,
+                                        "bytes_per_launch": algo_bytes(k, case, mixed) * case.ncells}
+    lib.profile(solver.ctx, 0)
+    return out
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    except (OSError, ValueError):
+        return 6650.0, "fallback"
+
+
+def cpu_reference(config, scale, steps, cores):
+    """The CPU restatement of the reference (OpenMP on the host cores)."""
+    from shared_cfd_b200.solver import Solver
+    so = os.path.join(ROOT, "oracle", "_build", "liborc.so")
+    if not os.path.exists(so):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    orc = abi.Bound(C.CDLL(so), "orc_")
+    case = make_case(config, scale, abi.PREC_FP64)
+    s = Solver(case, lib=orc)
+    s.upload()
+    s.prepare(1)
+    t0 = time.perf_counter()
+    s.run(1, steps)
+    dt = time.perf_counter() - t0
+    s.close()
+    units = case.ncells * iters_per_step(case) * steps
+    return units / dt / 1e6, dt, case
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="reacting_step", choices=["reacting_step", "flat_plate", "sod"])
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cores = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        steps = max(1, args.steps)
+        val, dt, case = cpu_reference(args.config, args.scale, steps, cores)
+        unit = "Mcell-iter/s"
+        line = {"impl": "reference", "metric": "Mcell-iter/s (plain FP64)", "value": val, "unit": unit,
+                "n_gpus": args.gpus, "steps": steps, "warmup": 0, "ms_per_step": 1e3 * dt / steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded)",
+                "config": {"workload": workload_name(args.config, args.scale), "cells": case.ncells,
+                           "inner_iterations": iters_per_step(case)},
+                "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port",
+                                 "sample": "%d physical step(s) of the full workload on %d OpenMP threads "
+                                           "(C++ FP64 restatement of the reference)" % (steps, cores)},
+                "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    dev = local if torch.cuda.device_count() > 1 else 0
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", dev))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from shared_cfd_b200 import build
+    from shared_cfd_b200.solver import Solver
+    if rank == 0:
+        build.build()
+    barrier()
+
+    res = {}
+    solvers = {}
+    for prec, tag in ((abi.PREC_MIXED, "mixed"), (abi.PREC_FP64, "fp64")):
+        case = make_case(args.config, args.scale, prec)
+        s = Solver(case)
+        s.upload()
+        s.prepare(1)
+        ms, st, nl, clk = time_resident(s, args.steps, args.warmup, torch, dev, dev, barrier)
+        ms = max_over_ranks(ms)
+        units = case.ncells * iters_per_step(case) * args.steps * world
+        res[tag] = {"ms": ms, "value": units / (ms * 1e-3) / 1e6, "launches": nl, "clocks": clk,
+                    "status": st.status, "res_warn": st.res_warn, "omega": st.omega,
+                    "chem_attempts": st.chem_attempts, "chem_fallback": st.chem_fallback_cells}
+        solvers[tag] = (s, case)
+        log("%s: %.2f ms/step  %.1f Mcell-iter/s  status %d" % (tag, ms / args.steps, res[tag]["value"], st.status))
+
+    # accuracy of the mixed path against the FP64 path after the same steps
+    qm, _, _, _ = solvers["mixed"][0].download()
+    qd, _, _, _ = solvers["fp64"][0].download()
+    case = solvers["fp64"][1]
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import rel_l2
+    l2_mixed = rel_l2(case, qm, qd)
+
+    # per-kernel device times (separate, profiled pass of the mixed path)
+    s_m, case_m = solvers["mixed"]
+    prof = kernel_profile(s_m, args.steps, case_m, True)
+    prof64 = kernel_profile(solvers["fp64"][0], args.steps, case, False)
+    peak, peak_kind = measured_peaks()
+    hbm = {k: v for k, v in prof.items() if v["bytes_per_launch"] > 0 and v["kind"] != abi.K_CHEM}
+    top = max(prof.items(), key=lambda kv: kv[1]["total_ms"])
+    dom = max(hbm.items(), key=lambda kv: kv[1]["total_ms"]) if hbm else top
+    ach = dom[1]["bytes_per_launch"] / (dom[1]["avg_ms"] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "peak_source": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": dom[1]["bytes_per_launch"],
+                "avg_launch_ms": dom[1]["avg_ms"], "top_kernel_by_time": top[0]}
+    for v in list(prof.values()) + list(prof64.values()):
+        if v["bytes_per_launch"]:
+            v["gbs"] = v["bytes_per_launch"] / (v["avg_ms"] * 1e-3) / 1e9
+
+    # end to end through the C ABI with host buffers
+    s_e, case_e = solvers["mixed"]
+    q = np.ascontiguousarray(case_e.q)
+    w = np.ascontiguousarray(case_e.w)
+    vhi = np.ascontiguousarray(case_e.vhi)
+    qout = np.zeros_like(q)
+    lib = s_e.lib
+    ttc = C.c_double()
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        s_e._check(lib.upload(s_e.ctx, abi.dptr(q), abi.dptr(w), abi.dptr(vhi), 0.0), "upload")
+        st = abi.Stats()
+        lib.step(s_e.ctx, k + 1, C.byref(st))
+        s_e._check(lib.download(s_e.ctx, abi.dptr(qout), None, None, C.byref(ttc)), "download")
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    units = case_e.ncells * iters_per_step(case_e) * args.steps * world
+    e2e = {"value": units / e2e_s / 1e6, "unit": "Mcell-iter/s",
+           "h2d_bytes_per_step": int(q.nbytes + w.nbytes + vhi.nbytes), "d2h_bytes_per_step": int(qout.nbytes)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, dt, _ = cpu_reference(args.config, args.scale, args.cpu_steps, cores)
+            cpu = {"value": v, "unit": "Mcell-iter/s", "cores": cores, "kind": "port",
+                   "sample": "%d physical step(s) of the full workload (%.1f s) on %d OpenMP threads, "
+                             "C++ FP64 restatement" % (args.cpu_steps, dt, cores)}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "Mcell-iter/s", "cores": cores, "kind": "port", "sample": "failed: %s" % e}
+
+    if rank == 0:
+        m = res["mixed"]
+        line = {
+            "metric": "Mcell-iter/s (mixed FP32/FP64; plain FP64 in fp64_value)",
+            "value": m["value"], "unit": "Mcell-iter/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic (seeded)",
+            "config": {"workload": workload_name(args.config, args.scale), "cells": case.ncells,
+                       "inner_iterations": iters_per_step(case), "parallelism": "replica per GPU" if world > 1 else "1 GPU",
+                       "l2": "state larger than L2 (no flush)" if case.ncells * case.W * 8 > 126e6 else "state fits L2"},
+            "fp64_value": res["fp64"]["value"], "fp64_ms_per_step": res["fp64"]["ms"] / args.steps,
+            "mixed_over_fp64": m["value"] / res["fp64"]["value"],
+            "l2_mixed_vs_fp64": l2_mixed,
+            "e2e": e2e, "gpu_launches": m["launches"],
+            "clocks": m["clocks"], "roofline": roofline, "cpu_baseline": cpu,
+            "status": {"mixed": m["status"], "fp64": res["fp64"]["status"], "res_warn": m["res_warn"],
+                       "omega": m["omega"], "chem_attempts": m["chem_attempts"], "chem_fallback_cells": m["chem_fallback"]},
+            "kernels_mixed": {k: {kk: v[kk] for kk in ("avg_ms", "launches", "total_ms", "gbs") if kk in v}
+                              for k, v in prof.items()},
+            "kernels_fp64": {k: {kk: v[kk] for kk in ("avg_ms", "launches", "total_ms", "gbs") if kk in v}
+                             for k, v in prof64.items()},
+        }
+        print(json.dumps(line), flush=True)
+    for s, _ in solvers.values():
+        s.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -215,6 +215,16 @@ int  scfd_get_stream(scfd_ctx* ctx, void** stream);
 /* Number of device kernel launches issued by the last scfd_step/scfd_run. */
 int  scfd_launch_count(const scfd_ctx* ctx, int64_t* count);
 
+/* Per-kernel timing.  While enabled, every kernel of a step is bracketed by
+ * CUDA events on the context's stream and its device time accumulated per
+ * kind; scfd_kernel_stats reads (and scfd_profile(ctx,1) resets) the totals. */
+enum {
+    SCFD_K_THERMO = 0, SCFD_K_BC, SCFD_K_DT, SCFD_K_CHEM, SCFD_K_RESIDUAL,
+    SCFD_K_SWEEP_FWD, SCFD_K_SWEEP_BWD, SCFD_K_UPDATE, SCFD_K_COPY, SCFD_K_OTHER, SCFD_K_COUNT
+};
+int  scfd_profile(scfd_ctx* ctx, int enable);
+int  scfd_kernel_stats(scfd_ctx* ctx, int kind, double* total_ms, int64_t* launches, char* name, int namelen);
+
 #ifdef __cplusplus
 }
 #endif

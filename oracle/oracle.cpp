@@ -1287,10 +1287,31 @@ int part_main(orc_ctx& c) {  // store/core/main.part_main.f90 + dim/q2d/main.par
     return 0;
 }
 
+int step_body(orc_ctx& c, scfd_stats* st);
+
+// One physical step; the statistics are filled in also when the step stops
+// with an error code.
 int step(orc_ctx& c, int stepno, scfd_stats* st) {
+    long long att0 = c.chem_attempts, fb0 = c.chem_fallback;
+    if (st) std::memset(st, 0, sizeof(*st));
+    int s = step_body(c, st);
+    if (st) {
+        st->dt_grbl = c.dt_grbl;
+        st->tt = c.tt;
+        st->res = c.res;
+        st->res1 = c.res1;
+        st->omega = c.omega_last;
+        st->chem_attempts = c.chem_attempts - att0;
+        st->chem_fallback_cells = c.chem_fallback - fb0;
+        st->status = s;
+    }
+    (void)stepno;
+    return s;
+}
+
+int step_body(orc_ctx& c, scfd_stats* st) {
     int s = 0;
     const bool reactive = c.d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
-    long long att0 = c.chem_attempts, fb0 = c.chem_fallback;
     if (c.d.scheme == SCFD_SCHEME_NR) {
         // NR/q2d/main.main.raw.f90:1-20, with proceed_reaction after set_dt as in
         // LU-SGS/q2d/main.main.point_implicit.f90:1-3 when the model is reactive.
@@ -1301,6 +1322,7 @@ int step(orc_ctx& c, int stepno, scfd_stats* st) {
         copy_arr(c.qp, c.q);
         int j = 1;
         while (j < c.d.num_internal_loop) {
+            if (st) st->inner_iters = j;
             if ((s = part_primitive(c))) return s;
             part_main(c);
             set_ABpm(c);
@@ -1337,17 +1359,6 @@ int step(orc_ctx& c, int stepno, scfd_stats* st) {
             calc_next_step_implicit(c, 1);
         }
     }
-    if (st) {
-        st->dt_grbl = c.dt_grbl;
-        st->tt = c.tt;
-        st->res = c.res;
-        st->res1 = c.res1;
-        st->omega = c.omega_last;
-        st->chem_attempts = c.chem_attempts - att0;
-        st->chem_fallback_cells = c.chem_fallback - fb0;
-        st->status = s;
-    }
-    (void)stepno;
     return s;
 }
 
@@ -1562,6 +1573,20 @@ int orc_get_stream(orc_ctx* c, void** s) {
 int orc_launch_count(const orc_ctx* c, int64_t* n) {
     if (!c || !n) return SCFD_E_ARG;
     *n = 0;
+    return 0;
+}
+
+int orc_profile(orc_ctx* c, int enable) {
+    (void)enable;
+    return c ? 0 : SCFD_E_ARG;
+}
+
+int orc_kernel_stats(orc_ctx* c, int kind, double* ms, int64_t* n, char* name, int namelen) {
+    (void)kind;
+    if (!c) return SCFD_E_ARG;
+    if (ms) *ms = 0.0;
+    if (n) *n = 0;
+    if (name && namelen > 0) name[0] = 0;
     return 0;
 }
 

@@ -138,7 +138,10 @@ SIGNATURES = {
     "download_qp": (C.c_int, [_P, _D]),
     "get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "profile": (C.c_int, [_P, C.c_int]),
+    "kernel_stats": (C.c_int, [_P, C.c_int, _D, C.POINTER(C.c_int64), C.c_char_p, C.c_int]),
 }
+K_THERMO, K_BC, K_DT, K_CHEM, K_RESIDUAL, K_SWEEP_FWD, K_SWEEP_BWD, K_UPDATE, K_COPY, K_OTHER, K_COUNT = range(11)
 
 
 class Bound:

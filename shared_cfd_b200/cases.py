@@ -384,7 +384,7 @@ def perturb(case, seed=1, amp=0.05):
         ph = rng.uniform(0, 2 * np.pi, size=4)
         f1 = np.sin(2 * np.pi * ii / max(ni, 1) + ph[0]) * np.cos(2 * np.pi * jj / max(nj, 1) + ph[1])
         f2 = np.cos(2 * np.pi * ii / max(ni, 1) + ph[2]) * np.sin(2 * np.pi * jj / max(nj, 1) + ph[3])
-        q = case.q[p]
+        q = case.q[p, :nj + 4, :ni + 4]
         rho = q[:, :, :case.nY].sum(axis=2)
         u = q[:, :, case.nY] / rho
         v = q[:, :, case.nY + 1] / rho
@@ -398,7 +398,7 @@ def perturb(case, seed=1, amp=0.05):
         q[:, :, case.nY] = rho2 * u2
         q[:, :, case.nY + 1] = rho2 * v2
         q[:, :, D - 1] = e_int * (1.0 + 0.5 * amp * f2) + 0.5 * rho2 * (u2 * u2 + v2 * v2)
-        w = case.w[p]
+        w = case.w[p, :nj + 4, :ni + 4]
         w[:, :, 0] = rho2
         w[:, :, 1] = u2
         w[:, :, 2] = v2

@@ -34,8 +34,8 @@ __device__ __forceinline__ void st_release(int* p, int v) {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// bounded wait: about 2^26 polls (well above a second) before giving up
-constexpr long long kSpinLimit = 1ll << 26;
+// bounded wait: 2^22 polls (of the order of a second) before giving up
+constexpr long long kSpinLimit = 1ll << 22;
 
 template <typename RT>
 struct CellJ {
@@ -260,22 +260,26 @@ static void launch_rt(const View& v, cudaStream_t s, int dir, StripList sl, doub
         launch_dir<RT, 35>(v, s, dir, sl, xfer, prog, ticket, partials, upd);
 }
 
-int launch_sweeps(const View& v, cudaStream_t s, double* xfer, int* progress, double* partials, int* tickets,
-                  int nstrips_fwd, int nstrips_bwd, const int* strip_tab_f, const int* strip_tab_b) {
+int launch_sweep_reset(cudaStream_t s, int* progress, int* tickets, int nstrips_fwd, int nstrips_bwd) {
     // progress[0..nf) forward, progress[nf..nf+nb) backward; tickets[0], tickets[1]
     cudaMemsetAsync(progress, 0, sizeof(int) * (nstrips_fwd + nstrips_bwd), s);
     cudaMemsetAsync(tickets, 0, sizeof(int) * 2, s);
+    return 0;
+}
+
+int launch_sweep(const View& v, cudaStream_t s, int dir, double* xfer, int* progress, double* partials, int* tickets,
+                 int nstrips_fwd, int nstrips_bwd, const int* strip_tab_f, const int* strip_tab_b) {
     StripList f{(const int2*)strip_tab_f, nstrips_fwd}, b{(const int2*)strip_tab_b, nstrips_bwd};
     const bool mixed = v.precision == SCFD_PREC_MIXED;
     const int upd = v.scheme == SCFD_SCHEME_NR ? 0 : 1;
-    if (mixed) {
-        launch_rt<float>(v, s, 0, f, xfer, progress, tickets, partials, upd);
-        launch_rt<float>(v, s, 1, b, xfer, progress + nstrips_fwd, tickets + 1, partials, upd);
+    if (dir == 0) {
+        if (mixed) launch_rt<float>(v, s, 0, f, xfer, progress, tickets, partials, upd);
+        else launch_rt<double>(v, s, 0, f, xfer, progress, tickets, partials, upd);
     } else {
-        launch_rt<double>(v, s, 0, f, xfer, progress, tickets, partials, upd);
-        launch_rt<double>(v, s, 1, b, xfer, progress + nstrips_fwd, tickets + 1, partials, upd);
+        if (mixed) launch_rt<float>(v, s, 1, b, xfer, progress + nstrips_fwd, tickets + 1, partials, upd);
+        else launch_rt<double>(v, s, 1, b, xfer, progress + nstrips_fwd, tickets + 1, partials, upd);
     }
-    return 2;
+    return 1;
 }
 
 // NR: global omega / res from the per-strip partials (fixed order), then

@@ -56,6 +56,13 @@ struct scfd_ctx {
     size_t stage_doubles = 0;
     long long launches = 0;
     int cells_max = 0;
+    // per-kernel timing
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<int, size_t>> ev_marks;  // kind, index of the start event
+    double kind_ms[SCFD_K_COUNT] = {0};
+    long long kind_n[SCFD_K_COUNT] = {0};
 
     int fail(int code, const std::string& m) {
         err = m;
@@ -330,6 +337,38 @@ int sync_scalars(scfd_ctx* c) {
     return 0;
 }
 
+// Runs f() (which enqueues one kernel of the given kind) between two CUDA
+// events when profiling is on.
+template <typename Fn>
+int timed(scfd_ctx* c, int kind, Fn f) {
+    if (!c->profiling) return f();
+    while (c->ev_pool.size() < c->ev_used + 2) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        c->ev_pool.push_back(e);
+    }
+    const size_t k = c->ev_used;
+    c->ev_used += 2;
+    cudaEventRecord(c->ev_pool[k], c->stream);
+    const int n = f();
+    cudaEventRecord(c->ev_pool[k + 1], c->stream);
+    c->ev_marks.push_back({kind, k});
+    return n;
+}
+
+void collect_events(scfd_ctx* c) {
+    if (!c->profiling || c->ev_marks.empty()) return;
+    cudaStreamSynchronize(c->stream);
+    for (auto& m : c->ev_marks) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev_pool[m.second], c->ev_pool[m.second + 1]);
+        c->kind_ms[m.first] += ms;
+        c->kind_n[m.first] += 1;
+    }
+    c->ev_marks.clear();
+    c->ev_used = 0;
+}
+
 // the kernel sequence of one physical step
 int enqueue_step(scfd_ctx* c) {
     const View& v = c->v;
@@ -337,46 +376,61 @@ int enqueue_step(scfd_ctx* c) {
     long long n = 0;
     const bool reactive = c->d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
     const long long qbytes = sizeof(double) * (long long)c->D * c->ncell;
-    auto primitive = [&]() { n += launch_thermo(v, s, c->cells_max); };
+    auto primitive = [&]() { n += timed(c, SCFD_K_THERMO, [&] { return launch_thermo(v, s, c->cells_max); }); };
     auto bc = [&]() {
-        n += launch_ghosts(v, s, c->d_ops, c->nops, c->d_bcval, c->valstride);
-        if (v.precision == SCFD_PREC_MIXED) n += launch_to_f32(v, s);
+        n += timed(c, SCFD_K_BC, [&] { return launch_ghosts(v, s, c->d_ops, c->nops, c->d_bcval, c->valstride); });
+        if (v.precision == SCFD_PREC_MIXED) n += timed(c, SCFD_K_OTHER, [&] { return launch_to_f32(v, s); });
     };
-    auto chem = [&]() { n += launch_chem_impl(v, s, c->d.chem_max_substeps, c->d_counter, c->nsm); };
+    auto chem = [&]() {
+        n += timed(c, SCFD_K_CHEM, [&] { return launch_chem_impl(v, s, c->d.chem_max_substeps, c->d_counter, c->nsm); });
+    };
+    auto setdt = [&]() { n += timed(c, SCFD_K_DT, [&] { return launch_set_dt(v, s); }); };
+    auto sweeps = [&]() {
+        launch_sweep_reset(s, c->d_progress, c->d_tickets, c->nsf, c->nsb);
+        n += timed(c, SCFD_K_SWEEP_FWD, [&] {
+            return launch_sweep(v, s, 0, c->d_xfer, c->d_progress, c->d_partials, c->d_tickets, c->nsf, c->nsb,
+                                c->d_strips_f, c->d_strips_b);
+        });
+        n += timed(c, SCFD_K_SWEEP_BWD, [&] {
+            return launch_sweep(v, s, 1, c->d_xfer, c->d_progress, c->d_partials, c->d_tickets, c->nsf, c->nsb,
+                                c->d_strips_f, c->d_strips_b);
+        });
+    };
+    auto copyq = [&](double* dst, const double* src) {
+        timed(c, SCFD_K_COPY, [&] { return (int)(cudaMemcpyAsync(dst, src, qbytes, cudaMemcpyDeviceToDevice, s) ? 0 : 0); });
+    };
     if (c->d.scheme == SCFD_SCHEME_NR) {
         primitive();
-        n += launch_set_dt(v, s);
+        setdt();
         if (reactive) chem();
-        CK(cudaMemcpyAsync(v.qpp, v.qp, qbytes, cudaMemcpyDeviceToDevice, s));
-        CK(cudaMemcpyAsync(v.qp, v.q, qbytes, cudaMemcpyDeviceToDevice, s));
+        copyq(v.qpp, v.qp);
+        copyq(v.qp, v.q);
         for (int j = 1; j < c->d.num_internal_loop; ++j) {
             primitive();
             bc();
-            n += launch_residual(v, s, RES_NR);
-            n += launch_sweeps(v, s, c->d_xfer, c->d_progress, c->d_partials, c->d_tickets, c->nsf, c->nsb,
-                               c->d_strips_f, c->d_strips_b);
-            n += launch_nr_update(v, s, c->d_partials, c->nsb, j);
+            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_NR); });
+            sweeps();
+            n += timed(c, SCFD_K_UPDATE, [&] { return launch_nr_update(v, s, c->d_partials, c->nsb, j); });
         }
-        n += launch_step_end(v, s, c->d.res_rate_warn, c->d.res_rate_err);
+        n += timed(c, SCFD_K_OTHER, [&] { return launch_step_end(v, s, c->d.res_rate_warn, c->d.res_rate_err); });
     } else {
         if (reactive) {
             primitive();
-            n += launch_set_dt(v, s);
+            setdt();
             chem();
-            CK(cudaMemcpyAsync(v.qp, v.q, qbytes, cudaMemcpyDeviceToDevice, s));
+            copyq(v.qp, v.q);
             primitive();
         } else {
-            CK(cudaMemcpyAsync(v.qp, v.q, qbytes, cudaMemcpyDeviceToDevice, s));
+            copyq(v.qp, v.q);
             primitive();
-            n += launch_set_dt(v, s);
+            setdt();
         }
         bc();
         if (c->d.scheme == SCFD_SCHEME_EULER) {
-            n += launch_residual(v, s, RES_EULER);
+            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_EULER); });
         } else {
-            n += launch_residual(v, s, RES_LUSGS);
-            n += launch_sweeps(v, s, c->d_xfer, c->d_progress, c->d_partials, c->d_tickets, c->nsf, c->nsb,
-                               c->d_strips_f, c->d_strips_b);
+            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_LUSGS); });
+            sweeps();
         }
     }
     CK(cudaGetLastError());
@@ -450,6 +504,7 @@ int scfd_create(const scfd_desc* d, scfd_ctx** out) {
 
 int scfd_destroy(scfd_ctx* c) {
     if (!c) return SCFD_E_ARG;
+    for (auto e : c->ev_pool) cudaEventDestroy(e);
     if (c->arena) cudaFree(c->arena);
     if (c->h_sc) cudaFreeHost(c->h_sc);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -774,6 +829,7 @@ int scfd_step(scfd_ctx* c, int step, scfd_stats* stats) {
     c->launches = 0;
     if ((st = enqueue_step(c))) return st;
     if ((st = sync_scalars(c))) return st;
+    collect_events(c);
     return fill_stats(c, stats, att0, fb0);
 }
 
@@ -784,9 +840,12 @@ int scfd_run(scfd_ctx* c, int step, int nsteps, scfd_stats* stats) {
     if (st) return st;
     const long long att0 = c->h_sc->chem_attempts, fb0 = c->h_sc->chem_fallback;
     c->launches = 0;
-    for (int n = 0; n < nsteps; ++n)
+    for (int n = 0; n < nsteps; ++n) {
         if ((st = enqueue_step(c))) return st;
+        if (c->profiling && c->ev_used > 4096) collect_events(c);
+    }
     if ((st = sync_scalars(c))) return st;
+    collect_events(c);
     return fill_stats(c, stats, att0, fb0);
 }
 
@@ -825,6 +884,28 @@ int scfd_get_stream(scfd_ctx* c, void** s) {
 int scfd_launch_count(const scfd_ctx* c, int64_t* n) {
     if (!c || !n) return SCFD_E_ARG;
     *n = c->launches;
+    return 0;
+}
+
+int scfd_profile(scfd_ctx* c, int enable) {
+    if (!c) return SCFD_E_ARG;
+    c->profiling = enable != 0;
+    for (int k = 0; k < SCFD_K_COUNT; ++k) {
+        c->kind_ms[k] = 0.0;
+        c->kind_n[k] = 0;
+    }
+    c->ev_marks.clear();
+    c->ev_used = 0;
+    return 0;
+}
+
+int scfd_kernel_stats(scfd_ctx* c, int kind, double* total_ms, int64_t* launches, char* name, int namelen) {
+    static const char* names[SCFD_K_COUNT] = {"thermo", "bc", "set_dt", "chemistry", "residual",
+                                              "sweep_fwd", "sweep_bwd", "nr_update", "copy", "other"};
+    if (!c || kind < 0 || kind >= SCFD_K_COUNT) return SCFD_E_ARG;
+    if (total_ms) *total_ms = c->kind_ms[kind];
+    if (launches) *launches = c->kind_n[kind];
+    if (name && namelen > 0) std::snprintf(name, (size_t)namelen, "%s", names[kind]);
     return 0;
 }
 

@@ -109,8 +109,9 @@ int launch_thermo(const View& v, cudaStream_t s, int cells_per_plane_max);
 int launch_ghosts(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride);
 int launch_set_dt(const View& v, cudaStream_t s);
 int launch_residual(const View& v, cudaStream_t s, int mode);
-int launch_sweeps(const View& v, cudaStream_t s, double* xfer, int* progress, double* partials,
-                  int* tickets, int nstrips_fwd, int nstrips_bwd, const int* strip_tab_f, const int* strip_tab_b);
+int launch_sweep_reset(cudaStream_t s, int* progress, int* tickets, int nstrips_fwd, int nstrips_bwd);
+int launch_sweep(const View& v, cudaStream_t s, int dir, double* xfer, int* progress, double* partials,
+                 int* tickets, int nstrips_fwd, int nstrips_bwd, const int* strip_tab_f, const int* strip_tab_b);
 int launch_nr_update(const View& v, cudaStream_t s, const double* partials, int nstrips, int inner);
 int launch_chem_impl(const View& v, cudaStream_t s, int max_substeps, unsigned long long* counter, int nsm);
 int launch_step_end(const View& v, cudaStream_t s, double warn, double err);

@@ -41,8 +41,8 @@ def read_plot3d(path):
 
 
 def format_plot3d(planes):
-    """Text of a plot3d grid: 4 values per line, 16 significant digits, as the
-    sample grids are written."""
+    """Text of a plot3d grid: 4 values per line like the sample grids, with 17
+    significant digits so that the text reads back bit-identically."""
     out = ["%8d" % len(planes)]
     for xh, _ in planes:
         out.append("%8d %8d %8d" % (xh.shape[0], xh.shape[1], 1))
@@ -50,14 +50,14 @@ def format_plot3d(planes):
         for arr in (xh, rh, np.zeros_like(xh)):
             flat = arr.T.reshape(-1)
             for k in range(0, flat.size, 4):
-                out.append(" ".join("%23.15e" % v for v in flat[k:k + 4]))
+                out.append(" ".join("%24.16e" % v for v in flat[k:k + 4]))
     return "\n".join(out) + "\n"
 
 
 def roundtrip_plot3d_values(planes):
     """The node coordinates a reader of format_plot3d(planes) gets back."""
-    return [(np.array([float("%23.15e" % v) for v in xh.reshape(-1)]).reshape(xh.shape),
-             np.array([float("%23.15e" % v) for v in rh.reshape(-1)]).reshape(rh.shape))
+    return [(np.array([float("%24.16e" % v) for v in xh.reshape(-1)]).reshape(xh.shape),
+             np.array([float("%24.16e" % v) for v in rh.reshape(-1)]).reshape(rh.shape))
             for xh, rh in planes]
 
 
