@@ -220,7 +220,8 @@ int  scfd_launch_count(const scfd_ctx* ctx, int64_t* count);
  * kind; scfd_kernel_stats reads (and scfd_profile(ctx,1) resets) the totals. */
 enum {
     SCFD_K_THERMO = 0, SCFD_K_BC, SCFD_K_DT, SCFD_K_CHEM, SCFD_K_RESIDUAL,
-    SCFD_K_SWEEP_FWD, SCFD_K_SWEEP_BWD, SCFD_K_UPDATE, SCFD_K_COPY, SCFD_K_OTHER, SCFD_K_COUNT
+    SCFD_K_SWEEP_FWD, SCFD_K_SWEEP_BWD, SCFD_K_UPDATE, SCFD_K_COPY, SCFD_K_OTHER, SCFD_K_PACK,
+    SCFD_K_COUNT
 };
 int  scfd_profile(scfd_ctx* ctx, int enable);
 int  scfd_kernel_stats(scfd_ctx* ctx, int kind, double* total_ms, int64_t* launches, char* name, int namelen);

@@ -141,7 +141,8 @@ SIGNATURES = {
     "profile": (C.c_int, [_P, C.c_int]),
     "kernel_stats": (C.c_int, [_P, C.c_int, _D, C.POINTER(C.c_int64), C.c_char_p, C.c_int]),
 }
-K_THERMO, K_BC, K_DT, K_CHEM, K_RESIDUAL, K_SWEEP_FWD, K_SWEEP_BWD, K_UPDATE, K_COPY, K_OTHER, K_COUNT = range(11)
+K_THERMO, K_BC, K_DT, K_CHEM, K_RESIDUAL, K_SWEEP_FWD, K_SWEEP_BWD, K_UPDATE, K_COPY, K_OTHER, K_PACK, K_COUNT = \
+    range(12)
 
 
 class Bound:

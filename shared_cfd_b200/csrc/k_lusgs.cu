@@ -272,6 +272,9 @@ int launch_sweep(const View& v, cudaStream_t s, int dir, double* xfer, int* prog
     StripList f{(const int2*)strip_tab_f, nstrips_fwd}, b{(const int2*)strip_tab_b, nstrips_bwd};
     const bool mixed = v.precision == SCFD_PREC_MIXED;
     const int upd = v.scheme == SCFD_SCHEME_NR ? 0 : 1;
+    if (dir == 0 && launch_sweep2(v, s, 0, f.strips, f.n, xfer, progress, tickets, partials, upd)) return 1;
+    if (dir == 1 && launch_sweep2(v, s, 1, b.strips, b.n, xfer, progress + nstrips_fwd, tickets + 1, partials, upd))
+        return 1;
     if (dir == 0) {
         if (mixed) launch_rt<float>(v, s, 0, f, xfer, progress, tickets, partials, upd);
         else launch_rt<double>(v, s, 0, f, xfer, progress, tickets, partials, upd);

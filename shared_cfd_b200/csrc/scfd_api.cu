@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -46,6 +47,9 @@ struct scfd_ctx {
     int nops = 0;
     double* d_bcval = nullptr;
     int valstride = SCFD_BC_MAXVAL + 2;
+    // strip-record sweeps
+    bool use_sw3 = false;
+    Sweep3 sw3{};
     // chemistry
     unsigned long long* d_counter = nullptr;
     // rms
@@ -387,6 +391,12 @@ int enqueue_step(scfd_ctx* c) {
     auto setdt = [&]() { n += timed(c, SCFD_K_DT, [&] { return launch_set_dt(v, s); }); };
     auto sweeps = [&]() {
         launch_sweep_reset(s, c->d_progress, c->d_tickets, c->nsf, c->nsb);
+        if (c->use_sw3) {
+            n += timed(c, SCFD_K_PACK, [&] { return launch_sweep3(v, s, c->sw3, 0, 0); });
+            n += timed(c, SCFD_K_SWEEP_FWD, [&] { return launch_sweep3(v, s, c->sw3, 1, 0); });
+            n += timed(c, SCFD_K_SWEEP_BWD, [&] { return launch_sweep3(v, s, c->sw3, 2, 0); });
+            return;
+        }
         n += timed(c, SCFD_K_SWEEP_FWD, [&] {
             return launch_sweep(v, s, 0, c->d_xfer, c->d_progress, c->d_partials, c->d_tickets, c->nsf, c->nsb,
                                 c->d_strips_f, c->d_strips_b);
@@ -410,7 +420,10 @@ int enqueue_step(scfd_ctx* c) {
             bc();
             n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_NR); });
             sweeps();
-            n += timed(c, SCFD_K_UPDATE, [&] { return launch_nr_update(v, s, c->d_partials, c->nsb, j); });
+            if (c->use_sw3)
+                n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, c->sw3, 3, j); });
+            else
+                n += timed(c, SCFD_K_UPDATE, [&] { return launch_nr_update(v, s, c->d_partials, c->nsb, j); });
         }
         n += timed(c, SCFD_K_OTHER, [&] { return launch_step_end(v, s, c->d.res_rate_warn, c->d.res_rate_err); });
     } else {
@@ -431,6 +444,7 @@ int enqueue_step(scfd_ctx* c) {
         } else {
             n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_LUSGS); });
             sweeps();
+            if (c->use_sw3) n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, c->sw3, 3, 1); });
         }
     }
     CK(cudaGetLastError());
@@ -636,6 +650,34 @@ int scfd_commit(scfd_ctx* c) {
             }
     }
     const int nrec = 64 * c->np;
+    // strip records for the TMA-streamed sweeps
+    const size_t blk3 = impl ? sweep3_record_elems(nY, mixed) : 0;
+    const size_t esz3 = mixed ? sizeof(float) : sizeof(double);
+    c->use_sw3 = blk3 > 0 && std::getenv("SCFD_SWEEP_LEGACY") == nullptr;
+    std::vector<long long> rec_off;
+    std::vector<int> blks3, tabf3, tabb3;
+    long long rec_total = 0;
+    if (c->use_sw3) {
+        int fs = 0;
+        for (int pl = 0; pl < c->np; ++pl) {
+            const int ns = (c->P.nj[pl] + 31) / 32, steps = c->P.ni[pl] + 31;
+            for (int st3 = 0; st3 < ns; ++st3, ++fs) {
+                rec_off.push_back(rec_total);
+                rec_total += (long long)steps * blk3;
+                for (int t0 = 0; t0 < steps; t0 += 32) {
+                    blks3.push_back(fs);
+                    blks3.push_back(t0);
+                }
+                tabf3.insert(tabf3.end(), {pl, st3, fs, 0});
+            }
+        }
+        int base3 = 0;
+        for (int pl = 0; pl < c->np; ++pl) {
+            const int ns = (c->P.nj[pl] + 31) / 32;
+            for (int st3 = ns - 1; st3 >= 0; --st3) tabb3.insert(tabb3.end(), {pl, st3, base3 + st3, 0});
+            base3 += ns;
+        }
+    }
     // arena size
     size_t bytes = 0;
     bytes += 3 * need<double>(D * N);                         // q, qp, qpp
@@ -654,12 +696,16 @@ int scfd_commit(scfd_ctx* c) {
                           ccabe.size() + ctroe.size() + ctrange.size() + ctrans.size() + cwc1.size() + cwc2.size() + 64);
     bytes += need<int>(crs.size() + cind.size() + cnum.size() + csnu.size() + cex.size() + cnm.size() + cim.size() +
                        ctr.size() + cns.size() + 64);
+    if (c->use_sw3)
+        bytes += need<char>(rec_total * esz3) + need<long long>(rec_off.size()) + need<int>(blks3.size()) +
+                 need<int>(tabf3.size()) + need<int>(tabb3.size());
     bytes += 64 * 256;
     c->arena_bytes = bytes;
     CK(cudaMalloc(&c->arena, bytes));
     CK(cudaMemsetAsync(c->arena, 0, bytes, c->stream));
     char* p = c->arena;
     View& v = c->v;
+    v.base = reinterpret_cast<double*>(c->arena);
     v.P = c->P;
     v.ncell = N;
     v.nY = nY; v.D = D; v.W = W;
@@ -694,6 +740,30 @@ int scfd_commit(scfd_ctx* c) {
     c->d_counter = carve<unsigned long long>(p, 1);
     c->d_rms_partial = carve<double>(p, nrec);
     c->d_rms_out = carve<double>(p, 1);
+    if (c->use_sw3) {
+        Sweep3& w3 = c->sw3;
+        w3.rec = carve<char>(p, rec_total * esz3);
+        long long* ro = carve<long long>(p, rec_off.size());
+        int* bk = carve<int>(p, blks3.size());
+        int* tf = carve<int>(p, tabf3.size());
+        int* tb = carve<int>(p, tabb3.size());
+        CK(cudaMemcpyAsync(ro, rec_off.data(), rec_off.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(bk, blks3.data(), blks3.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(tf, tabf3.data(), tabf3.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(tb, tabb3.data(), tabb3.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        w3.rec_off = ro;
+        w3.blk = reinterpret_cast<const int2*>(bk);
+        w3.nblk = (int)blks3.size() / 2;
+        w3.tab_f = reinterpret_cast<const int4*>(tf);
+        w3.tab_b = reinterpret_cast<const int4*>(tb);
+        w3.nstrips = c->nsf;
+        w3.xfer = c->d_xfer;
+        w3.xstride = (long long)c->nimax * D;
+        w3.progress = c->d_progress;
+        w3.tickets = c->d_tickets;
+        w3.partials = c->d_partials;
+        CK(cudaStreamSynchronize(c->stream));
+    }
     auto upd = [&](const std::vector<double>& h) -> const double* {
         double* d = carve<double>(p, std::max<size_t>(1, h.size()));
         if (!h.empty()) cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
@@ -900,8 +970,8 @@ int scfd_profile(scfd_ctx* c, int enable) {
 }
 
 int scfd_kernel_stats(scfd_ctx* c, int kind, double* total_ms, int64_t* launches, char* name, int namelen) {
-    static const char* names[SCFD_K_COUNT] = {"thermo", "bc", "set_dt", "chemistry", "residual",
-                                              "sweep_fwd", "sweep_bwd", "nr_update", "copy", "other"};
+    static const char* names[SCFD_K_COUNT] = {"thermo", "bc", "set_dt", "chemistry", "residual", "sweep_fwd",
+                                              "sweep_bwd", "update", "copy", "other", "pack"};
     if (!c || kind < 0 || kind >= SCFD_K_COUNT) return SCFD_E_ARG;
     if (total_ms) *total_ms = c->kind_ms[kind];
     if (launches) *launches = c->kind_n[kind];

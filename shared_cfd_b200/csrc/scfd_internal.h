@@ -91,6 +91,7 @@ struct View {
     double *Vol, *Area, *dsi, *dsj, *vni, *vnj, *x, *r, *gjc, *gji, *gjj, *dsci, *dscj, *vnci, *vncj;
     // mixed-precision copies used by the FP32 residual / sweeps
     float *w32, *vhi32;
+    double* base;  // arena base: every double field above is base + a whole offset
     DevScalars* sc;
     DevChem chem;
 };
@@ -112,6 +113,25 @@ int launch_residual(const View& v, cudaStream_t s, int mode);
 int launch_sweep_reset(cudaStream_t s, int* progress, int* tickets, int nstrips_fwd, int nstrips_bwd);
 int launch_sweep(const View& v, cudaStream_t s, int dir, double* xfer, int* progress, double* partials,
                  int* tickets, int nstrips_fwd, int nstrips_bwd, const int* strip_tab_f, const int* strip_tab_b);
+bool launch_sweep2(const View& v, cudaStream_t s, int dir, const int2* strips, int n, double* xfer, int* prog,
+                   int* ticket, double* partials, int upd);
+// Strip-record LU-SGS (k_sweep3.cu), available for nY in {1, 8, 9}.
+struct Sweep3 {
+    void* rec;                 // strip records (float on the mixed path)
+    const long long* rec_off;  // per forward strip
+    const int2* blk;           // pack/unpack blocks: (strip, first step)
+    int nblk;
+    const int4* tab_f;         // forward strips (plane, s, strip, 0)
+    const int4* tab_b;         // backward order
+    int nstrips;
+    double* xfer;
+    long long xstride;
+    int* progress;             // 2*nstrips
+    int* tickets;              // 2
+    double* partials;          // 2*nstrips
+};
+size_t sweep3_record_elems(int ny, bool mixed);  // elements per step block, 0 if none
+int launch_sweep3(const View& v, cudaStream_t s, const Sweep3& w, int what, int inner);
 int launch_nr_update(const View& v, cudaStream_t s, const double* partials, int nstrips, int inner);
 int launch_chem_impl(const View& v, cudaStream_t s, int max_substeps, unsigned long long* counter, int nsm);
 int launch_step_end(const View& v, cudaStream_t s, double warn, double err);

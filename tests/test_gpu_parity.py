@@ -126,3 +126,16 @@ def test_launch_count_positive(gpu):
     s.run(1, 3)
     assert s.launch_count() >= 3 * 4
     s.close()
+
+
+@pytest.mark.parametrize("legacy", [False, True])
+def test_sweep_paths_agree(gpu, orc, legacy, monkeypatch):
+    """Both sweep implementations (strip records streamed by TMA, and the
+    generic per-lane gather used for other species counts) match the
+    restatement."""
+    if legacy:
+        monkeypatch.setenv("SCFD_SWEEP_LEGACY", "1")
+    case = cases.perturb(cases.forward_step(2, n=20, scheme=abi.SCHEME_LUSGS, dt_mode=abi.DT_LOCAL, viscous=1,
+                                            dim=abi.DIM_Q2D), seed=21)
+    case.desc.cfl = 2.0
+    _parity(case, gpu, orc, 5)
