@@ -207,6 +207,11 @@ __global__ void __launch_bounds__(1024) k_pack(View v, const int2* blk, const in
 // ---------------------------------------------------------------------------
 // the sweeps
 // ---------------------------------------------------------------------------
+// Records of one strip hold ni+31 step blocks plus kPad zero blocks before and
+// after them, so the step loop runs in unguarded blocks of 8 steps with the
+// prefetch reaching past either end.
+constexpr int kPad = 8 + PF;
+
 template <typename RT, int NY, int DIR>
 __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, double* xfer, long long xstride,
                                                int* progress, int* ticket, double* partials) {
@@ -215,6 +220,7 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
     using V = typename Vec16<RT>::type;
     constexpr int D = R::D, G = L::G, NG = L::NG, STEP = L::STEP;
     constexpr unsigned BLK = STEP * sizeof(RT);
+    static_assert(8 % PF == 0, "ring depth must divide the unroll");
     extern __shared__ __align__(128) unsigned char smraw[];
     RT* ring = reinterpret_cast<RT*>(smraw);                                        // [PF][STEP]
     double* xin = reinterpret_cast<double*>(smraw + PF * BLK);                      // [8][D]
@@ -230,6 +236,7 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
     unsigned phase = 0;  // bit k: parity of the next completion of ring slot k
     bool bail = false;
     const int lf = DIR == 0 ? lane : 31 - lane;  // this lane's slot in a record block
+    const long long gstep = DIR == 0 ? STEP : -STEP;
     for (;;) {
         int sid = 0;
         if (lane == 0) sid = atomicAdd(ticket, 1);
@@ -239,36 +246,34 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
         const int p = st.x, s = st.y, fs = st.z;
         const int ni = v.P.ni[p], nj = v.P.nj[p];
         const int nstr = (nj + 31) / 32;
-        const bool rowok = 32 * s + 1 + lf <= nj;
         const bool has_prev = DIR == 0 ? s > 0 : s < nstr - 1;
-        const bool publish = lane == 31 && rowok && (DIR == 0 ? s < nstr - 1 : s > 0);
+        const bool publish = lane == 31 && (DIR == 0 ? s < nstr - 1 : s > 0);
         double* xout = xfer + (long long)sid * xstride;
         const double* xsrc = xfer + (long long)(sid - 1) * xstride;
         int* prog_out = progress + sid;
         const int* prog_in = progress + sid - 1;
-        const int nsteps = ni + 31;
+        const int nblk8 = (ni + 31 + 7) / 8;
         RT* srec = rec + sl.rec_off[fs];
-        // forward record block of sweep step tt
-        auto blk_of = [&](int tt) { return srec + (long long)(DIR == 0 ? tt : ni + 30 - tt) * STEP; };
-        auto issue = [&](int tt) {
-            if (lane == 0 && tt < nsteps) {
-                const int slot = tt % PF;
-                mbar_expect_tx(&bar[slot], BLK);
-                tma_bulk_g2s(ring + slot * STEP, blk_of(tt), BLK, &bar[slot]);
+        // record block of sweep step tt (forward order; the backward sweep walks it back)
+        const RT* rd = srec + (DIR == 0 ? 0 : (long long)(ni + 30) * STEP);
+        if (lane == 0) {
+#pragma unroll
+            for (int tt = 0; tt < PF - 1; ++tt) {
+                mbar_expect_tx(&bar[tt], BLK);
+                tma_bulk_g2s(ring + tt * STEP, rd + tt * gstep, BLK, &bar[tt]);
             }
-        };
-        for (int tt = 0; tt < PF - 1; ++tt) issue(tt);
+        }
         RT outA[D], outB[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) { outA[k] = RT(0); outB[k] = RT(0); }
-        double res = 0.0, omega = 1e300;
-        bool omega_fail = false;
-        RT* gblk = blk_of(0) + lf * G;
-        const long long gstep = DIR == 0 ? STEP : -STEP;
-        for (int t = 0; t < nsteps; ++t, gblk += gstep) {
-            issue(t + PF - 1);
-            if (has_prev && (t & 7) == 0 && t < ni) {
-                const int need = t + 8 < ni ? t + 8 : ni;
+        double res = 0.0;
+        double on = __longlong_as_double(0x7FF0000000000000ll), od = 1.0;  // omega candidate q / (-Dq)
+        RT* gblk = const_cast<RT*>(rd) + lf * G;
+        for (int tb = 0; tb < nblk8 && !bail; ++tb) {
+            const int t0 = tb * 8;
+            const bool chunk = has_prev && t0 < ni;
+            if (chunk) {
+                const int need = t0 + 8 < ni ? t0 + 8 : ni;
                 if (lane == 0) {
                     long long spins = 0;
                     while (ld_acquire3(prog_in) < need) {
@@ -280,98 +285,117 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
                     }
                 }
                 __syncwarp();
-                for (int e = lane; e < 8 * D; e += 32)
-                    if (t + e / D < ni) xin[e] = __ldcg(xsrc + (long long)t * D + e);
+                for (int e = lane; e < 8 * D; e += 32) xin[e] = __ldcg(xsrc + (long long)t0 * D + e);
                 __syncwarp();
             }
-            RT inB[D];
-            const bool from_prev = lane == 0 && has_prev && t < ni;
 #pragma unroll
-            for (int k = 0; k < D; ++k) {
-                const RT sh = __shfl_up_sync(0xffffffffu, outB[k], 1);
-                inB[k] = lane == 0 ? (from_prev ? RT(xin[(t & 7) * D + k]) : RT(0)) : sh;
-            }
-            const int slot = t % PF;
-            {
-                long long spins = 0;
-                while (!mbar_try_wait(&bar[slot], (phase >> slot) & 1u)) {
-                    if (++spins > kSpin3) {
-                        atomicMax(&v.sc->status, SCFD_E_SPIN);
-                        bail = true;
-                        break;
+            for (int u = 0; u < 8; ++u) {
+                const int t = t0 + u;
+                constexpr int dummy = 0;
+                (void)dummy;
+                if (lane == 0) {
+                    const int sl2 = (u + PF - 1) % PF;
+                    mbar_expect_tx(&bar[sl2], BLK);
+                    tma_bulk_g2s(ring + sl2 * STEP, rd + (long long)(t + PF - 1) * gstep, BLK, &bar[sl2]);
+                }
+                RT inB[D];
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    const RT sh = __shfl_up_sync(0xffffffffu, outB[k], 1);
+                    inB[k] = lane == 0 ? (chunk ? RT(xin[u * D + k]) : RT(0)) : sh;
+                }
+                const int slot = u % PF;
+                {
+                    long long spins = 0;
+                    while (!mbar_try_wait(&bar[slot], (phase >> slot) & 1u)) {
+                        if (++spins > kSpin3) {
+                            atomicMax(&v.sc->status, SCFD_E_SPIN);
+                            bail = true;
+                            break;
+                        }
+                    }
+                    phase ^= 1u << slot;
+                }
+                // this lane's cell: NG 16-byte loads (zero-filled outside the plane)
+                RT f[NG * G];
+                const V* src = reinterpret_cast<const V*>(ring + slot * STEP) + lf;
+#pragma unroll
+                for (int g = 0; g < NG; ++g) *reinterpret_cast<V*>(&f[g * G]) = src[g * 32];
+                const RT al = f[R::AL];
+                RT x[D];
+#pragma unroll
+                for (int k = 0; k < D; ++k)
+                    x[k] = DIR == 0 ? al * (f[R::X + k] + (outA[k] + inB[k])) : f[R::X + k] - al * (outA[k] + inB[k]);
+                // P = dpdq.x; forward q2d: semi-implicit pressure source
+                // (q2d time_lusgs_viscous.f90:38-44)
+                RT P = RT(0), S = RT(0);
+#pragma unroll
+                for (int k = 0; k < D; ++k)
+                    if (k != NY + 1) P += f[R::DP + k] * x[k];
+#pragma unroll
+                for (int k = 0; k < NY; ++k) S += x[k];
+                if (DIR == 0 && q2d) x[NY + 1] = (x[NY + 1] + f[R::AA] * P) * f[R::RQ];
+                P += f[R::DP + NY + 1] * x[NY + 1];
+#pragma unroll
+                for (int dn = 0; dn < 2; ++dn) {
+                    const int b0 = dn == 0 ? R::FA : R::FB;
+                    const RT fa = f[b0], n1 = f[b0 + 1], n2 = f[b0 + 2], un = f[b0 + 3], nu = f[b0 + 4];
+                    const RT base_ = n1 * x[NY] + n2 * x[NY + 1] - un * S;
+                    const RT lam = DIR == 0 ? un + nu : un - nu;
+                    RT* o = dn == 0 ? outA : outB;
+#pragma unroll
+                    for (int k = 0; k < NY; ++k) o[k] = fa * (f[R::CV + k] * base_ + lam * x[k]);
+                    o[NY] = fa * (f[R::CV + NY] * base_ + lam * x[NY] + n1 * P);
+                    o[NY + 1] = fa * (f[R::CV + NY + 1] * base_ + lam * x[NY + 1] + n2 * P);
+                    o[NY + 2] = fa * (f[R::CV + NY + 2] * base_ + lam * x[NY + 2] + un * P);
+                }
+                // results back into the record block (16-byte stores)
+#pragma unroll
+                for (int k = 0; k < D; ++k) f[R::X + k] = x[k];
+#pragma unroll
+                for (int g = 0; g < (D + G - 1) / G; ++g)
+                    *reinterpret_cast<V*>(gblk + g * 32 * G) = *reinterpret_cast<V*>(&f[g * G]);
+                gblk += gstep;
+                if (DIR == 1 && nr) {
+                    const double dE = double(x[NY + 2]);
+                    res = res + dE * dE;
+#pragma unroll
+                    for (int k = 0; k < NY; ++k) {
+                        // smallest q_k/(-Dq_k) over Dq_k < 0, compared by cross-multiplication
+                        const double dk = double(x[k]);
+                        const double qn = double(f[R::QS + k]), qd = -dk;
+                        if (dk < 0.0 && qn * od < on * qd) {
+                            on = qn;
+                            od = qd;
+                        }
                     }
                 }
-                phase ^= 1u << slot;
-            }
-            if (bail) break;
-            // this lane's cell: NG 16-byte loads (zero-filled outside the plane)
-            RT f[NG * G];
-            const V* src = reinterpret_cast<const V*>(ring + slot * STEP) + lf;
+                const int cc = t - 31;
+                if (publish && cc >= 0) {
 #pragma unroll
-            for (int g = 0; g < NG; ++g) *reinterpret_cast<V*>(&f[g * G]) = src[g * 32];
-            const RT al = f[R::AL];
-            RT x[D];
-#pragma unroll
-            for (int k = 0; k < D; ++k)
-                x[k] = DIR == 0 ? al * (f[R::X + k] + (outA[k] + inB[k])) : f[R::X + k] - al * (outA[k] + inB[k]);
-            // P = dpdq.x; forward q2d: semi-implicit pressure source
-            // (q2d time_lusgs_viscous.f90:38-44)
-            RT P = RT(0), S = RT(0);
-#pragma unroll
-            for (int k = 0; k < D; ++k)
-                if (k != NY + 1) P += f[R::DP + k] * x[k];
-#pragma unroll
-            for (int k = 0; k < NY; ++k) S += x[k];
-            if (DIR == 0 && q2d) x[NY + 1] = (x[NY + 1] + f[R::AA] * P) * f[R::RQ];
-            P += f[R::DP + NY + 1] * x[NY + 1];
-#pragma unroll
-            for (int dn = 0; dn < 2; ++dn) {
-                const int b0 = dn == 0 ? R::FA : R::FB;
-                const RT fa = f[b0], n1 = f[b0 + 1], n2 = f[b0 + 2], un = f[b0 + 3], nu = f[b0 + 4];
-                const RT base_ = n1 * x[NY] + n2 * x[NY + 1] - un * S;
-                const RT lam = DIR == 0 ? un + nu : un - nu;
-                RT* o = dn == 0 ? outA : outB;
-#pragma unroll
-                for (int k = 0; k < NY; ++k) o[k] = fa * (f[R::CV + k] * base_ + lam * x[k]);
-                o[NY] = fa * (f[R::CV + NY] * base_ + lam * x[NY] + n1 * P);
-                o[NY + 1] = fa * (f[R::CV + NY + 1] * base_ + lam * x[NY + 1] + n2 * P);
-                o[NY + 2] = fa * (f[R::CV + NY + 2] * base_ + lam * x[NY + 2] + un * P);
-            }
-            // results back into the record block (16-byte stores)
-#pragma unroll
-            for (int k = 0; k < D; ++k) f[R::X + k] = x[k];
-#pragma unroll
-            for (int g = 0; g < (D + G - 1) / G; ++g) *reinterpret_cast<V*>(gblk + g * 32 * G) = *reinterpret_cast<V*>(&f[g * G]);
-            if (DIR == 1 && nr) {
-                const double dE = double(x[NY + 2]);
-                res = res + dE * dE;
-#pragma unroll
-                for (int k = 0; k < NY; ++k) {
-                    const double dk = double(x[k]);
-                    const double cand = dk < 0.0 ? -double(f[R::QS + k]) / dk * v.dq_max : 1e300;
-                    omega = fmin(omega, cand);
+                    for (int k = 0; k < D; ++k) xout[(long long)cc * D + k] = double(outB[k]);
                 }
-                omega_fail |= omega < v.omega_min;
+                __syncwarp();
             }
-            const int cc = t - lane;
-            if (publish && cc >= 0 && cc < ni) {
-#pragma unroll
-                for (int k = 0; k < D; ++k) xout[(long long)cc * D + k] = double(outB[k]);
-                if ((cc & 7) == 7 || cc == ni - 1) st_release3(prog_out, cc + 1);
-            }
-            __syncwarp();
+            // columns published so far by the top lane
+            const int done = t0 + 8 - 31;
+            if (publish && done > 0) st_release3(prog_out, done < ni ? done : ni);
         }
         if (bail) break;
         if (DIR == 1 && nr) {
             for (int o = 16; o > 0; o >>= 1) {
                 res += __shfl_xor_sync(0xffffffffu, res, o);
-                omega = fmin(omega, __shfl_xor_sync(0xffffffffu, omega, o));
+                const double on2 = __shfl_xor_sync(0xffffffffu, on, o), od2 = __shfl_xor_sync(0xffffffffu, od, o);
+                if (on2 * od < on * od2) {
+                    on = on2;
+                    od = od2;
+                }
             }
-            const unsigned fail = __ballot_sync(0xffffffffu, omega_fail);
             if (lane == 0) {
+                const double om = on / od * v.dq_max;   // -q/Dq*Dqmax of the limiting cell
                 partials[2 * fs] = res;
-                partials[2 * fs + 1] = omega;
-                if (fail) atomicMax(&v.sc->status, SCFD_E_OMEGA);
+                partials[2 * fs + 1] = om;
+                if (om < v.omega_min) atomicMax(&v.sc->status, SCFD_E_OMEGA);
             }
         }
     }
@@ -447,6 +471,8 @@ __global__ void __launch_bounds__(1024) k_unpack(View v, const int2* blk, const 
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+int sweep3_pad_steps() { return kPad; }
+
 size_t sweep3_record_elems(int ny, bool mixed) {
     switch (ny) {
         case 1: return mixed ? RecLayout<float, 1>::STEP : RecLayout<double, 1>::STEP;

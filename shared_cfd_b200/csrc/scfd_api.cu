@@ -662,8 +662,9 @@ int scfd_commit(scfd_ctx* c) {
         for (int pl = 0; pl < c->np; ++pl) {
             const int ns = (c->P.nj[pl] + 31) / 32, steps = c->P.ni[pl] + 31;
             for (int st3 = 0; st3 < ns; ++st3, ++fs) {
-                rec_off.push_back(rec_total);
-                rec_total += (long long)steps * blk3;
+                const int pad = sweep3_pad_steps();
+                rec_off.push_back(rec_total + (long long)pad * blk3);
+                rec_total += (long long)(steps + 2 * pad) * blk3;
                 for (int t0 = 0; t0 < steps; t0 += 32) {
                     blks3.push_back(fs);
                     blks3.push_back(t0);
@@ -688,7 +689,7 @@ int scfd_commit(scfd_ctx* c) {
     if (mixed) bytes += need<float>(W * N) + need<float>(nY * N);
     bytes += need<DevScalars>(1);
     bytes += 2 * need<int>(2 * c->nsf);
-    bytes += need<double>((size_t)c->nsf * c->nimax * D);
+    bytes += need<double>((size_t)c->nsf * (c->nimax + 8) * D);
     bytes += need<int>(c->nsf + c->nsb) + need<int>(2) + need<double>(2 * c->nsb);
     bytes += need<GhostOp>(std::max(1, c->nops)) + need<double>(std::max<size_t>(1, c->bcs.size()) * c->valstride);
     bytes += need<unsigned long long>(1) + need<double>(nrec) + need<double>(1);
@@ -731,7 +732,7 @@ int scfd_commit(scfd_ctx* c) {
     v.sc = c->d_sc;
     c->d_strips_f = carve<int>(p, 2 * c->nsf);
     c->d_strips_b = carve<int>(p, 2 * c->nsb);
-    c->d_xfer = carve<double>(p, (size_t)c->nsf * c->nimax * D);
+    c->d_xfer = carve<double>(p, (size_t)c->nsf * (c->nimax + 8) * D);
     c->d_progress = carve<int>(p, c->nsf + c->nsb);
     c->d_tickets = carve<int>(p, 2);
     c->d_partials = carve<double>(p, 2 * c->nsb);
@@ -758,7 +759,7 @@ int scfd_commit(scfd_ctx* c) {
         w3.tab_b = reinterpret_cast<const int4*>(tb);
         w3.nstrips = c->nsf;
         w3.xfer = c->d_xfer;
-        w3.xstride = (long long)c->nimax * D;
+        w3.xstride = (long long)(c->nimax + 8) * D;
         w3.progress = c->d_progress;
         w3.tickets = c->d_tickets;
         w3.partials = c->d_partials;

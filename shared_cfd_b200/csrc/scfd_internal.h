@@ -131,6 +131,7 @@ struct Sweep3 {
     double* partials;          // 2*nstrips
 };
 size_t sweep3_record_elems(int ny, bool mixed);  // elements per step block, 0 if none
+int sweep3_pad_steps();                          // zero step blocks before and after each strip
 int launch_sweep3(const View& v, cudaStream_t s, const Sweep3& w, int what, int inner);
 int launch_nr_update(const View& v, cudaStream_t s, const double* partials, int nstrips, int inner);
 int launch_chem_impl(const View& v, cudaStream_t s, int max_substeps, unsigned long long* counter, int nsm);
