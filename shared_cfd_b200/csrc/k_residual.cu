@@ -317,7 +317,10 @@ static void launch_t(const View& v, cudaStream_t s) {
     k_residual<RT, MODE><<<grid, NT, smem, s>>>(v);
 }
 
-int launch_residual(const View& v, cudaStream_t s, int mode) {
+// need_coeffs: the caller's sweep reads alpha/nuA/nuB from the cell arrays,
+// which only this generic kernel writes.
+int launch_residual(const View& v, cudaStream_t s, int mode, bool need_coeffs) {
+    if (!need_coeffs && launch_residual2(v, s, mode)) return 1;
     const bool mixed = v.precision == SCFD_PREC_MIXED;
     if (mode == RES_EULER) {
         if (mixed) launch_t<float, RES_EULER>(v, s); else launch_t<double, RES_EULER>(v, s);

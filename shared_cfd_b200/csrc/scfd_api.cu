@@ -418,7 +418,7 @@ int enqueue_step(scfd_ctx* c) {
         for (int j = 1; j < c->d.num_internal_loop; ++j) {
             primitive();
             bc();
-            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_NR); });
+            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_NR, !c->use_sw3); });
             sweeps();
             if (c->use_sw3)
                 n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, c->sw3, 3, j); });
@@ -440,9 +440,9 @@ int enqueue_step(scfd_ctx* c) {
         }
         bc();
         if (c->d.scheme == SCFD_SCHEME_EULER) {
-            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_EULER); });
+            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_EULER, false); });
         } else {
-            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_LUSGS); });
+            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_LUSGS, !c->use_sw3); });
             sweeps();
             if (c->use_sw3) n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, c->sw3, 3, 1); });
         }

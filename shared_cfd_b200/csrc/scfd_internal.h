@@ -4,8 +4,9 @@
 // Layout in HBM (one arena per context):
 //   * A "cell slot" index c addresses cell (i,j) of plane p for i = -1..ni+2,
 //     j = -1..nj+2 (two ghost layers, as q(.., -1:nimax+2, -1:njmax+2, ..)):
-//         c = base[p] + (j + 2) * pitch[p] + (i + 2),
-//     pitch[p] = round_up(ni + 4, 32) so rows start on 256-byte boundaries.
+//         c = base[p] + (j + 1) * pitch[p] + (i + 1),
+//     pitch[p] = round_up(ni + 4, 32) so rows start on 256-byte boundaries;
+//     a plane holds nj + 4 rows.
 //     Planes follow each other; all planes are resident together.
 //   * Every field is structure-of-arrays: component k of field F lives at
 //     F[k * ncell + c].  Face quantities of face i+1/2 (resp. j+1/2) are stored
@@ -31,7 +32,7 @@ struct Planes {
 };
 
 __host__ __device__ inline long long cidx(const Planes& P, int p, int i, int j) {
-    return P.base[p] + (long long)(j + 2) * P.pitch[p] + (i + 2);
+    return P.base[p] + (long long)(j + 1) * P.pitch[p] + (i + 1);
 }
 
 // Compact chemistry tables on the device (0-based species).
@@ -109,7 +110,8 @@ struct GhostOp {
 int launch_thermo(const View& v, cudaStream_t s, int cells_per_plane_max);
 int launch_ghosts(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride);
 int launch_set_dt(const View& v, cudaStream_t s);
-int launch_residual(const View& v, cudaStream_t s, int mode);
+int launch_residual(const View& v, cudaStream_t s, int mode, bool need_coeffs);
+bool launch_residual2(const View& v, cudaStream_t s, int mode);
 int launch_sweep_reset(cudaStream_t s, int* progress, int* tickets, int nstrips_fwd, int nstrips_bwd);
 int launch_sweep(const View& v, cudaStream_t s, int dir, double* xfer, int* progress, double* partials,
                  int* tickets, int nstrips_fwd, int nstrips_bwd, const int* strip_tab_f, const int* strip_tab_b);
