@@ -226,6 +226,28 @@ enum {
 int  scfd_profile(scfd_ctx* ctx, int enable);
 int  scfd_kernel_stats(scfd_ctx* ctx, int kind, double* total_ms, int64_t* launches, char* name, int namelen);
 
+/* ---- no-allocation entry point ------------------------------------------ */
+/* Capacity of the library's static scratch for scfd_rms_noalloc: partial sums
+ * of 64 blocks for each of at most SCFD_MAX_PLANES planes. */
+#define SCFD_NOALLOC_MAX_BLOCKS 4096
+
+/* scfd_rms with no device allocation (no counterpart in the reference; it is
+ * for callers that cannot call cudaMalloc, e.g. a solver whose device arrays
+ * come from its own OpenACC / CUDA Fortran data regions or memory pool).
+ * d_q and d_qp are DEVICE arrays in the layout of scfd_upload,
+ * q(1:dimq,-1:nimax+2,-1:njmax+2,Nplane); *d_rms (device) receives
+ * sqrt(sum (q(E)-qp(E))^2) / ncells over the interior cells
+ * (store/core/check_convergence.f90:17-28).  Enqueued on `stream` (a
+ * cudaStream_t, or NULL); the caller synchronises.  No context is needed.
+ * Scratch is a static device array of SCFD_NOALLOC_MAX_BLOCKS doubles that
+ * every GPU loading the library keeps until exit; its address is looked up on
+ * the first call on each device, so make that first call before any stream
+ * capture.  Calls that overlap on the GPU share the scratch and race.
+ * Returns SCFD_E_ARG for a bad descriptor or more planes than the scratch
+ * holds. */
+int  scfd_rms_noalloc(const scfd_desc* desc, const double* d_q, const double* d_qp, double* d_rms,
+                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif

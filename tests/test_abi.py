@@ -37,7 +37,11 @@ def test_cuda_library_exports_every_declared_symbol():
 
 
 def test_oracle_exports_same_entry_points(orc_raw):
+    # scfd_rms_noalloc works on device arrays only; the CPU restatement has no
+    # counterpart of it
     for n in declared():
+        if n.endswith("noalloc"):
+            continue
         assert hasattr(orc_raw, "orc_" + n), n
 
 
