@@ -57,6 +57,26 @@ def workload_name(config, scale):
 
 
 # algorithmic HBM bytes per interior cell and launch, FP64 storage
+# DRAM bytes (read + write) per interior cell and launch, from one ncu capture of
+# the reacting step at scale 0.5 (196 608 cells; ncu flushes the caches before each
+# launch, so these are cold-cache figures):
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#       --clock-control none -k regex:"k_sweep3|k_residual2|k_thermo|k_pack|k_unpack"
+#       -c 12 --csv python bench.py --scale 0.5 --steps 1 --warmup 1 --no-cpu-baseline
+# None of these kernels reuses data across launches, so the traffic of a launch
+# grows with the cell count and is scaled to the workload by cells.
+NCU_DRAM_BYTES_PER_CELL = {
+    ("reacting_step", True): {abi.K_THERMO: 434.7, abi.K_RESIDUAL: 548.4, abi.K_PACK: 538.8,
+                              abi.K_SWEEP_FWD: 273.4, abi.K_SWEEP_BWD: 273.4, abi.K_UPDATE: 155.9},
+}
+NCU_TRAFFIC_NOTE = "ncu dram__bytes_read+write per cell at scale 0.5 (cold cache), scaled by cells"
+
+
+def traffic_per_launch(config, mixed, kind, ncells):
+    t = NCU_DRAM_BYTES_PER_CELL.get((config, mixed), {}).get(kind)
+    return None if t is None else t * ncells
+
+
 def algo_bytes(kind, case, mixed):
     nY, D, W = case.nY, case.D, case.W
     nr = case.desc.scheme == abi.SCHEME_NR
@@ -93,7 +113,7 @@ class ClockSampler:
                  "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
@@ -197,10 +217,22 @@ def cpu_reference(config, scale, steps, cores):
     return units / dt / 1e6, dt, case
 
 
+def l2_note(case):
+    """Working set of one inner iteration against the 126 MB L2 (no flush is done)."""
+    D, W, nY = case.D, case.W, case.nY
+    # FP64 per cell: q, qp, qpp, Dq (D each), w (W), vhi, DHi (nY each), geometry (~16),
+    # dt; FP32 copies of w and vhi; one strip record (about 5 D values)
+    per_cell = 8 * (4 * D + W + 2 * nY + 17) + 4 * (W + nY) + 4 * (5 * D)
+    mb = per_cell * case.ncells / 1e6
+    if mb > 126:
+        return "working set ~%.0f MB per inner iteration > 126 MB L2 (no flush)" % mb
+    return "working set ~%.0f MB fits the 126 MB L2" % mb
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="reacting_step", choices=["reacting_step", "flat_plate", "sod"])
@@ -292,9 +324,18 @@ def main():
     dom = max(hbm.items(), key=lambda kv: kv[1]["total_ms"]) if hbm else top
     ach = dom[1]["bytes_per_launch"] / (dom[1]["avg_ms"] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": peak, "unit": "GB/s",
-                "frac": ach / peak, "peak_source": peak_kind, "traffic": None,
+                "frac": ach / peak, "peak_source": peak_kind,
+                "traffic": traffic_per_launch(args.config, True, dom[1]["kind"], case_m.ncells),
+                "traffic_source": NCU_TRAFFIC_NOTE,
                 "algorithmic_bytes_per_launch": dom[1]["bytes_per_launch"],
                 "avg_launch_ms": dom[1]["avg_ms"], "top_kernel_by_time": top[0]}
+    # the face-flux kernel (MUSCL + SLAU + viscous fluxes + RHS) on the same roofline
+    if "residual" in prof:
+        r = prof["residual"]
+        ach_r = r["bytes_per_launch"] / (r["avg_ms"] * 1e-3) / 1e9
+        roofline["flux_kernel"] = {"kernel": "residual", "achieved": ach_r, "frac": ach_r / peak,
+                                   "traffic": traffic_per_launch(args.config, True, abi.K_RESIDUAL, case_m.ncells),
+                                   "avg_launch_ms": r["avg_ms"]}
     for v in list(prof.values()) + list(prof64.values()):
         if v["bytes_per_launch"]:
             v["gbs"] = v["bytes_per_launch"] / (v["avg_ms"] * 1e-3) / 1e9
@@ -339,7 +380,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic (seeded)",
             "config": {"workload": workload_name(args.config, args.scale), "cells": case.ncells,
                        "inner_iterations": iters_per_step(case), "parallelism": "replica per GPU" if world > 1 else "1 GPU",
-                       "l2": "state larger than L2 (no flush)" if case.ncells * case.W * 8 > 126e6 else "state fits L2"},
+                       "l2": l2_note(case)},
             "fp64_value": res["fp64"]["value"], "fp64_ms_per_step": res["fp64"]["ms"] / args.steps,
             "mixed_over_fp64": m["value"] / res["fp64"]["value"],
             "l2_mixed_vs_fp64": l2_mixed,
