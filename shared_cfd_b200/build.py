@@ -9,7 +9,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libscfd_b200.so")
-SOURCES = ["scfd_api.cu", "k_thermo.cu", "k_bc.cu", "k_residual.cu", "k_lusgs.cu", "k_chem.cu", "k_misc.cu", "k_sweep2.cu", "k_sweep3.cu", "k_residual2.cu", "noalloc.cu"]
+HEADERS = ["scfd_internal.h", "async_ptx.h"]
+SOURCES = ["scfd_api.cu", "k_thermo.cu", "k_bc.cu", "k_residual.cu", "k_lusgs.cu", "k_chem.cu", "k_misc.cu", "k_sweep2.cu", "k_sweep3.cu", "k_sweep4.cu", "k_residual2.cu", "noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -21,8 +22,8 @@ def needs_build():
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, "scfd_internal.h"),
-                                                      os.path.join(HERE, "..", "include", "scfd_b200.h")]
+    deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, h) for h in HEADERS] + \
+        [os.path.join(HERE, "..", "include", "scfd_b200.h")]
     return any(os.path.getmtime(d) > t for d in deps)
 
 

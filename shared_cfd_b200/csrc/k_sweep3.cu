@@ -14,50 +14,23 @@
 // shared-memory transpose) into a "strip record" layout
 //     rec[strip][step t][field f][lane l]   (cell (i = t - l + 1, j = 32 s + 1 + l)),
 // which makes every step of every strip one contiguous block of NF*32 values.
-// The sweep streams those blocks with one cp.async.bulk (TMA) per step into a
-// shared-memory ring PF steps ahead (mbarrier completion), and writes its
+// The sweep streams those blocks, SPB steps per cp.async.bulk (TMA) copy, into a
+// shared-memory ring of PFB copies (mbarrier completion), and writes its
 // results back into the same block, contiguously.  The backward sweep reads the
 // same records with steps and lanes reversed (step ni+30-t, lane 31-l).
 // k_unpack applies q += omega*Dq back in the cell layout.
+#include "async_ptx.h"
 #include "scfd_internal.h"
 
 namespace scfd {
 
+using namespace ptx;
+
 namespace {
 
-__device__ __forceinline__ int ld_acquire3(const int* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release3(int* p, int v) {
-    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void tma_bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned phase) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(phase)
-        : "memory");
-    return ok != 0;
-}
-
 constexpr long long kSpin3 = 1ll << 22;
-constexpr int PF = 4;
+constexpr int SPB = 4;  // record steps per bulk copy
+constexpr int PFB = 3;  // bulk copies in the ring, PFB - 1 of them ahead of the sweep
 
 }  // namespace
 
@@ -210,7 +183,7 @@ __global__ void __launch_bounds__(1024) k_pack(View v, const int2* blk, const in
 // Records of one strip hold ni+31 step blocks plus kPad zero blocks before and
 // after them, so the step loop runs in unguarded blocks of 8 steps with the
 // prefetch reaching past either end.
-constexpr int kPad = 8 + PF;
+constexpr int kPad = 8 + SPB * PFB;
 
 template <typename RT, int NY, int DIR>
 __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, double* xfer, long long xstride,
@@ -220,20 +193,21 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
     using V = typename Vec16<RT>::type;
     constexpr int D = R::D, G = L::G, NG = L::NG, STEP = L::STEP;
     constexpr unsigned BLK = STEP * sizeof(RT);
-    static_assert(8 % PF == 0, "ring depth must divide the unroll");
+    static_assert(8 % SPB == 0, "bulk copies must tile the 8-step unroll");
     extern __shared__ __align__(128) unsigned char smraw[];
-    RT* ring = reinterpret_cast<RT*>(smraw);                                        // [PF][STEP]
-    double* xin = reinterpret_cast<double*>(smraw + PF * BLK);                      // [8][D]
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw + PF * BLK + 8 * D * sizeof(double));
+    RT* ring = reinterpret_cast<RT*>(smraw);                                        // [PFB][SPB][STEP]
+    double* xin = reinterpret_cast<double*>(smraw + PFB * SPB * BLK);               // [8][D]
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw + PFB * SPB * BLK + 8 * D * sizeof(double));
     const int lane = threadIdx.x;
     const bool nr = v.scheme == SCFD_SCHEME_NR;
     const bool q2d = v.dim == SCFD_DIM_Q2D;
     if (lane == 0) {
-        for (int k = 0; k < PF; ++k) mbar_init(&bar[k], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int k = 0; k < PFB; ++k) mbar_init(&bar[k], 1);
+        mbar_init_fence();
     }
     __syncwarp();
     unsigned phase = 0;  // bit k: parity of the next completion of ring slot k
+    unsigned pend = 0;   // ring slots with a copy in flight
     bool bail = false;
     const int lf = DIR == 0 ? lane : 31 - lane;  // this lane's slot in a record block
     const long long gstep = DIR == 0 ? STEP : -STEP;
@@ -256,13 +230,19 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
         RT* srec = rec + sl.rec_off[fs];
         // record block of sweep step tt (forward order; the backward sweep walks it back)
         const RT* rd = srec + (DIR == 0 ? 0 : (long long)(ni + 30) * STEP);
+        // bulk copy nb holds sweep steps SPB*nb .. SPB*nb+SPB-1; in memory order it
+        // starts at the first of them (forward) or the last (backward)
+        auto copy_src = [&](int nb) {
+            return DIR == 0 ? rd + (long long)nb * SPB * STEP : rd - (long long)(nb * SPB + SPB - 1) * STEP;
+        };
         if (lane == 0) {
 #pragma unroll
-            for (int tt = 0; tt < PF - 1; ++tt) {
-                mbar_expect_tx(&bar[tt], BLK);
-                tma_bulk_g2s(ring + tt * STEP, rd + tt * gstep, BLK, &bar[tt]);
+            for (int b = 0; b < PFB - 1; ++b) {
+                mbar_expect_tx(&bar[b], SPB * BLK);
+                tma_bulk_g2s(ring + b * SPB * STEP, copy_src(b), SPB * BLK, &bar[b]);
             }
         }
+        pend |= (1u << (PFB - 1)) - 1u;
         RT outA[D], outB[D];
 #pragma unroll
         for (int k = 0; k < D; ++k) { outA[k] = RT(0); outB[k] = RT(0); }
@@ -276,7 +256,7 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
                 const int need = t0 + 8 < ni ? t0 + 8 : ni;
                 if (lane == 0) {
                     long long spins = 0;
-                    while (ld_acquire3(prog_in) < need) {
+                    while (ld_acquire_gpu(prog_in) < need) {
                         if (++spins > kSpin3 || v.sc->spin_abort) {
                             atomicExch(&v.sc->spin_abort, 1ull);
                             atomicMax(&v.sc->status, SCFD_E_SPIN);
@@ -291,12 +271,15 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 const int t = t0 + u;
-                constexpr int dummy = 0;
-                (void)dummy;
-                if (lane == 0) {
-                    const int sl2 = (u + PF - 1) % PF;
-                    mbar_expect_tx(&bar[sl2], BLK);
-                    tma_bulk_g2s(ring + sl2 * STEP, rd + (long long)(t + PF - 1) * gstep, BLK, &bar[sl2]);
+                const int tq = t / SPB;  // bulk copy holding step t
+                const int slot = tq % PFB;
+                if (u % SPB == 0) {
+                    const int nb = tq + PFB - 1, sl2 = nb % PFB;
+                    if (lane == 0) {
+                        mbar_expect_tx(&bar[sl2], SPB * BLK);
+                        tma_bulk_g2s(ring + sl2 * SPB * STEP, copy_src(nb), SPB * BLK, &bar[sl2]);
+                    }
+                    pend |= 1u << sl2;
                 }
                 RT inB[D];
 #pragma unroll
@@ -304,21 +287,27 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
                     const RT sh = __shfl_up_sync(0xffffffffu, outB[k], 1);
                     inB[k] = lane == 0 ? (chunk ? RT(xin[u * D + k]) : RT(0)) : sh;
                 }
-                const int slot = u % PF;
-                {
+                if (u % SPB == 0) {
                     long long spins = 0;
+                    bool ok = true;
                     while (!mbar_try_wait(&bar[slot], (phase >> slot) & 1u)) {
                         if (++spins > kSpin3) {
-                            atomicMax(&v.sc->status, SCFD_E_SPIN);
-                            bail = true;
+                            ok = false;
                             break;
                         }
                     }
+                    if (!__all_sync(0xffffffffu, ok)) {
+                        if (lane == 0) atomicMax(&v.sc->status, SCFD_E_SPIN);
+                        bail = true;
+                        break;
+                    }
                     phase ^= 1u << slot;
+                    pend &= ~(1u << slot);
                 }
                 // this lane's cell: NG 16-byte loads (zero-filled outside the plane)
                 RT f[NG * G];
-                const V* src = reinterpret_cast<const V*>(ring + slot * STEP) + lf;
+                const int pos = DIR == 0 ? u % SPB : SPB - 1 - u % SPB;
+                const V* src = reinterpret_cast<const V*>(ring + (slot * SPB + pos) * STEP) + lf;
 #pragma unroll
                 for (int g = 0; g < NG; ++g) *reinterpret_cast<V*>(&f[g * G]) = src[g * 32];
                 const RT al = f[R::AL];
@@ -379,7 +368,18 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
             }
             // columns published so far by the top lane
             const int done = t0 + 8 - 31;
-            if (publish && done > 0) st_release3(prog_out, done < ni ? done : ni);
+            if (publish && done > 0) st_release_gpu(prog_out, done < ni ? done : ni);
+        }
+        // the copies still in flight (prefetches past the end, or all of them after
+        // a wait gave up) land before the ring takes the next strip or the CTA exits
+#pragma unroll
+        for (int k = 0; k < PFB; ++k) {
+            if (!((pend >> k) & 1u)) continue;
+            long long spins = 0;
+            while (!mbar_try_wait(&bar[k], (phase >> k) & 1u) && ++spins < kSpin3) {
+            }
+            phase ^= 1u << k;
+            pend &= ~(1u << k);
         }
         if (bail) break;
         if (DIR == 1 && nr) {
@@ -396,14 +396,6 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
                 partials[2 * fs] = res;
                 partials[2 * fs + 1] = om;
                 if (om < v.omega_min) atomicMax(&v.sc->status, SCFD_E_OMEGA);
-            }
-        }
-    }
-    if (bail) {
-        // let copies still in flight land before the CTA exits (bounded)
-        for (int k = 0; k < PF; ++k) {
-            long long spins = 0;
-            while (!mbar_try_wait(&bar[k], (phase >> k) & 1u) && ++spins < kSpin3) {
             }
         }
     }
@@ -485,10 +477,10 @@ size_t sweep3_record_elems(int ny, bool mixed) {
 template <typename RT, int NY, int DIR>
 static void sweep_launch(const View& v, cudaStream_t s, const Sweep3& w) {
     using L = RecLayout<RT, NY>;
-    const size_t smem = (size_t)PF * L::STEP * sizeof(RT) + 8 * (NY + 3) * sizeof(double) + PF * 8;
+    const size_t smem = (size_t)PFB * SPB * L::STEP * sizeof(RT) + 8 * (NY + 3) * sizeof(double) + PFB * 8;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_sweep3<RT, NY, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(k_sweep3<RT, NY, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
     StripRec sl{DIR == 0 ? w.tab_f : w.tab_b, w.rec_off, w.nstrips};

@@ -47,9 +47,11 @@ struct scfd_ctx {
     int nops = 0;
     double* d_bcval = nullptr;
     int valstride = SCFD_BC_MAXVAL + 2;
-    // strip-record sweeps
+    // strip-record sweeps: one lane per cell (sw3) or a quad per cell (sw4)
     bool use_sw3 = false;
     Sweep3 sw3{};
+    bool use_sw4 = false;
+    Sweep4 sw4{};
     // chemistry
     unsigned long long* d_counter = nullptr;
     // rms
@@ -390,6 +392,14 @@ int enqueue_step(scfd_ctx* c) {
     };
     auto setdt = [&]() { n += timed(c, SCFD_K_DT, [&] { return launch_set_dt(v, s); }); };
     auto sweeps = [&]() {
+        if (c->use_sw4) {
+            const Sweep4& w4 = c->sw4;
+            cudaMemsetAsync(w4.progress, 0, sizeof(int) * (2 * w4.ntasks + 2), s);
+            n += timed(c, SCFD_K_PACK, [&] { return launch_sweep4(v, s, w4, 0, 0); });
+            n += timed(c, SCFD_K_SWEEP_FWD, [&] { return launch_sweep4(v, s, w4, 1, 0); });
+            n += timed(c, SCFD_K_SWEEP_BWD, [&] { return launch_sweep4(v, s, w4, 2, 0); });
+            return;
+        }
         launch_sweep_reset(s, c->d_progress, c->d_tickets, c->nsf, c->nsb);
         if (c->use_sw3) {
             n += timed(c, SCFD_K_PACK, [&] { return launch_sweep3(v, s, c->sw3, 0, 0); });
@@ -418,9 +428,11 @@ int enqueue_step(scfd_ctx* c) {
         for (int j = 1; j < c->d.num_internal_loop; ++j) {
             primitive();
             bc();
-            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_NR, !c->use_sw3); });
+            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_NR, !c->use_sw3 && !c->use_sw4); });
             sweeps();
-            if (c->use_sw3)
+            if (c->use_sw4)
+                n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep4(v, s, c->sw4, 3, j); });
+            else if (c->use_sw3)
                 n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, c->sw3, 3, j); });
             else
                 n += timed(c, SCFD_K_UPDATE, [&] { return launch_nr_update(v, s, c->d_partials, c->nsb, j); });
@@ -442,9 +454,13 @@ int enqueue_step(scfd_ctx* c) {
         if (c->d.scheme == SCFD_SCHEME_EULER) {
             n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_EULER, false); });
         } else {
-            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_LUSGS, !c->use_sw3); });
+            n += timed(c, SCFD_K_RESIDUAL,
+                       [&] { return launch_residual(v, s, RES_LUSGS, !c->use_sw3 && !c->use_sw4); });
             sweeps();
-            if (c->use_sw3) n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, c->sw3, 3, 1); });
+            if (c->use_sw4)
+                n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep4(v, s, c->sw4, 3, 1); });
+            else if (c->use_sw3)
+                n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, c->sw3, 3, 1); });
         }
     }
     CK(cudaGetLastError());
@@ -653,7 +669,37 @@ int scfd_commit(scfd_ctx* c) {
     // strip records for the TMA-streamed sweeps
     const size_t blk3 = impl ? sweep3_record_elems(nY, mixed) : 0;
     const size_t esz3 = mixed ? sizeof(float) : sizeof(double);
-    c->use_sw3 = blk3 > 0 && std::getenv("SCFD_SWEEP_LEGACY") == nullptr;
+    const char* sweep_env = std::getenv("SCFD_SWEEP");
+    const bool legacy = std::getenv("SCFD_SWEEP_LEGACY") != nullptr;
+    int qc4 = 0;
+    const size_t blk4 = impl ? sweep4_record_elems(nY, mixed, &qc4) : 0;
+    c->use_sw4 = blk4 > 0 && !legacy && sweep_env && std::strcmp(sweep_env, "4") == 0;
+    c->use_sw3 = blk3 > 0 && !legacy && !c->use_sw4;
+    // quad-per-cell sweeps: strips of R rows, tasks of up to WPC strips
+    std::vector<long long> rec_off4;
+    std::vector<int> strips4, blks4, tasksf4, tasksb4;
+    long long rec_total4 = 0;
+    int ntasks4 = 0;
+    if (c->use_sw4) {
+        const int R = sweep4_rows(), WPC = sweep4_strips_per_task(mixed), pad = sweep4_pad_steps();
+        const int SB = sweep4_steps_per_block();
+        int fs = 0;
+        for (int pl = 0; pl < c->np; ++pl) {
+            const int ns = (c->P.nj[pl] + R - 1) / R, steps = c->P.ni[pl] + R - 1;
+            const int fs_plane = fs;
+            for (int st4 = 0; st4 < ns; ++st4, ++fs) {
+                rec_off4.push_back(rec_total4 + (long long)pad * blk4);
+                rec_total4 += (long long)(steps + 2 * pad) * blk4;
+                strips4.insert(strips4.end(), {pl, st4, 0, 0});
+                for (int t0 = 0; t0 < steps; t0 += SB) blks4.insert(blks4.end(), {fs, t0});
+            }
+            std::vector<int> tk;
+            for (int g0 = 0; g0 < ns; g0 += WPC) tk.insert(tk.end(), {pl, g0, std::min(WPC, ns - g0), fs_plane + g0});
+            tasksf4.insert(tasksf4.end(), tk.begin(), tk.end());
+            for (int k = (int)tk.size() / 4 - 1; k >= 0; --k) tasksb4.insert(tasksb4.end(), tk.begin() + 4 * k, tk.begin() + 4 * k + 4);
+        }
+        ntasks4 = (int)tasksf4.size() / 4;
+    }
     std::vector<long long> rec_off;
     std::vector<int> blks3, tabf3, tabb3;
     long long rec_total = 0;
@@ -697,6 +743,11 @@ int scfd_commit(scfd_ctx* c) {
                           ccabe.size() + ctroe.size() + ctrange.size() + ctrans.size() + cwc1.size() + cwc2.size() + 64);
     bytes += need<int>(crs.size() + cind.size() + cnum.size() + csnu.size() + cex.size() + cnm.size() + cim.size() +
                        ctr.size() + cns.size() + 64);
+    if (c->use_sw4)
+        bytes += need<char>(rec_total4 * esz3) + need<long long>(rec_off4.size()) + need<int>(strips4.size()) +
+                 need<int>(blks4.size()) + 2 * need<int>(tasksf4.size()) +
+                 need<char>((size_t)ntasks4 * (c->nimax + 8) * qc4 * esz3) + need<int>(2 * ntasks4 + 2) +
+                 need<double>(2 * strips4.size() / 4);
     if (c->use_sw3)
         bytes += need<char>(rec_total * esz3) + need<long long>(rec_off.size()) + need<int>(blks3.size()) +
                  need<int>(tabf3.size()) + need<int>(tabb3.size());
@@ -763,6 +814,34 @@ int scfd_commit(scfd_ctx* c) {
         w3.progress = c->d_progress;
         w3.tickets = c->d_tickets;
         w3.partials = c->d_partials;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if (c->use_sw4) {
+        Sweep4& w4 = c->sw4;
+        w4.rec = carve<char>(p, rec_total4 * esz3);
+        long long* ro = carve<long long>(p, rec_off4.size());
+        int* sp = carve<int>(p, strips4.size());
+        int* bk = carve<int>(p, blks4.size());
+        int* tf = carve<int>(p, tasksf4.size());
+        int* tb = carve<int>(p, tasksb4.size());
+        w4.xfer = carve<char>(p, (size_t)ntasks4 * (c->nimax + 8) * qc4 * esz3);
+        w4.progress = carve<int>(p, 2 * ntasks4 + 2);
+        w4.tickets = w4.progress + 2 * ntasks4;
+        w4.partials = carve<double>(p, 2 * strips4.size() / 4);
+        CK(cudaMemcpyAsync(ro, rec_off4.data(), rec_off4.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(sp, strips4.data(), strips4.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(bk, blks4.data(), blks4.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(tf, tasksf4.data(), tasksf4.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(tb, tasksb4.data(), tasksb4.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        w4.rec_off = ro;
+        w4.strips = reinterpret_cast<const int4*>(sp);
+        w4.nstrips = (int)strips4.size() / 4;
+        w4.blk = reinterpret_cast<const int2*>(bk);
+        w4.nblk = (int)blks4.size() / 2;
+        w4.tasks_f = reinterpret_cast<const int4*>(tf);
+        w4.tasks_b = reinterpret_cast<const int4*>(tb);
+        w4.ntasks = ntasks4;
+        w4.xstride = (long long)(c->nimax + 8) * qc4;
         CK(cudaStreamSynchronize(c->stream));
     }
     auto upd = [&](const std::vector<double>& h) -> const double* {

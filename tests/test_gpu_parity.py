@@ -128,14 +128,35 @@ def test_launch_count_positive(gpu):
     s.close()
 
 
-@pytest.mark.parametrize("legacy", [False, True])
-def test_sweep_paths_agree(gpu, orc, legacy, monkeypatch):
-    """Both sweep implementations (strip records streamed by TMA, and the
-    generic per-lane gather used for other species counts) match the
-    restatement."""
-    if legacy:
-        monkeypatch.setenv("SCFD_SWEEP_LEGACY", "1")
+SWEEP_ENV = {"lane": {}, "quad": {"SCFD_SWEEP": "4"}, "legacy": {"SCFD_SWEEP_LEGACY": "1"}}
+
+
+@pytest.mark.parametrize("path", sorted(SWEEP_ENV))
+def test_sweep_paths_agree(gpu, orc, path, monkeypatch):
+    """All three sweep implementations match the restatement: lane-per-cell
+    strip records streamed by bulk copies (default), quad-per-cell strips with
+    warp-to-warp hand-off, and the generic per-lane gather."""
+    for k, val in SWEEP_ENV[path].items():
+        monkeypatch.setenv(k, val)
     case = cases.perturb(cases.forward_step(2, n=20, scheme=abi.SCHEME_LUSGS, dt_mode=abi.DT_LOCAL, viscous=1,
                                             dim=abi.DIM_Q2D), seed=21)
     case.desc.cfl = 2.0
     _parity(case, gpu, orc, 5)
+
+
+@pytest.mark.parametrize("path", sorted(SWEEP_ENV))
+def test_sweep_many_tasks_ragged(gpu, orc, path, monkeypatch):
+    """One plane of 150 rows: 19 eight-row strips in three tasks (the last with
+    three strips, its last strip six rows high), so the hand-off crosses CTAs
+    through global memory as well as warps through shared memory."""
+    for k, val in SWEEP_ENV[path].items():
+        monkeypatch.setenv(k, val)
+    case = cases.perturb(cases.flat_plate(40, 150), seed=5)
+    _parity(case, gpu, orc, 3)
+
+
+def test_reacting_step_two_tasks_per_plane(gpu, orc):
+    """Reacting NR q2d step at a quarter of the resolution per direction:
+    128-row planes run as two tasks of eight strips."""
+    case = cases.reacting_step(scale=0.25, inner=3)
+    _parity(case, gpu, orc, 1)
