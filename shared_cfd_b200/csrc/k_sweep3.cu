@@ -29,7 +29,24 @@ using namespace ptx;
 namespace {
 
 constexpr long long kSpin3 = 1ll << 22;
-constexpr int SPB = 4;  // record steps per bulk copy
+
+// sum of a[B..E) as a balanced pairwise tree (short dependency chain)
+template <int B, int E, typename T>
+__device__ __forceinline__ T tree_sum(const T* a) {
+    if constexpr (E - B == 1) {
+        return a[B];
+    } else {
+        constexpr int M = (B + E) / 2;
+        return tree_sum<B, M>(a) + tree_sum<M, E>(a);
+    }
+}
+// record steps per bulk copy (FP64 records are twice as large: half as many
+// steps, so that the ring of PFB copies fits in shared memory)
+template <typename RT>
+struct Spb {
+    static constexpr int value = sizeof(RT) == 4 ? 8 : 4;
+};
+constexpr int SPB_MAX = 8;
 constexpr int PFB = 3;  // bulk copies in the ring, PFB - 1 of them ahead of the sweep
 
 }  // namespace
@@ -183,7 +200,7 @@ __global__ void __launch_bounds__(1024) k_pack(View v, const int2* blk, const in
 // Records of one strip hold ni+31 step blocks plus kPad zero blocks before and
 // after them, so the step loop runs in unguarded blocks of 8 steps with the
 // prefetch reaching past either end.
-constexpr int kPad = 8 + SPB * PFB;
+constexpr int kPad = 8 + SPB_MAX * PFB;
 
 template <typename RT, int NY, int DIR>
 __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, double* xfer, long long xstride,
@@ -193,10 +210,11 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
     using V = typename Vec16<RT>::type;
     constexpr int D = R::D, G = L::G, NG = L::NG, STEP = L::STEP;
     constexpr unsigned BLK = STEP * sizeof(RT);
+    constexpr int SPB = Spb<RT>::value;
     static_assert(8 % SPB == 0, "bulk copies must tile the 8-step unroll");
     extern __shared__ __align__(128) unsigned char smraw[];
     RT* ring = reinterpret_cast<RT*>(smraw);                                        // [PFB][SPB][STEP]
-    double* xin = reinterpret_cast<double*>(smraw + PFB * SPB * BLK);               // [8][D]
+    RT* xin = reinterpret_cast<RT*>(smraw + PFB * SPB * BLK);                       // [8][D]
     unsigned long long* bar = reinterpret_cast<unsigned long long*>(smraw + PFB * SPB * BLK + 8 * D * sizeof(double));
     const int lane = threadIdx.x;
     const bool nr = v.scheme == SCFD_SCHEME_NR;
@@ -222,8 +240,9 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
         const int nstr = (nj + 31) / 32;
         const bool has_prev = DIR == 0 ? s > 0 : s < nstr - 1;
         const bool publish = lane == 31 && (DIR == 0 ? s < nstr - 1 : s > 0);
-        double* xout = xfer + (long long)sid * xstride;
-        const double* xsrc = xfer + (long long)(sid - 1) * xstride;
+        // hand-off columns in the record precision (the values are the sweep's own)
+        RT* xout = reinterpret_cast<RT*>(xfer) + (long long)sid * xstride;
+        const RT* xsrc = reinterpret_cast<const RT*>(xfer) + (long long)(sid - 1) * xstride;
         int* prog_out = progress + sid;
         const int* prog_in = progress + sid - 1;
         const int nblk8 = (ni + 31 + 7) / 8;
@@ -285,7 +304,7 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
 #pragma unroll
                 for (int k = 0; k < D; ++k) {
                     const RT sh = __shfl_up_sync(0xffffffffu, outB[k], 1);
-                    inB[k] = lane == 0 ? (chunk ? RT(xin[u * D + k]) : RT(0)) : sh;
+                    inB[k] = lane == 0 ? (chunk ? xin[u * D + k] : RT(0)) : sh;
                 }
                 if (u % SPB == 0) {
                     long long spins = 0;
@@ -316,27 +335,31 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
                 for (int k = 0; k < D; ++k)
                     x[k] = DIR == 0 ? al * (f[R::X + k] + (outA[k] + inB[k])) : f[R::X + k] - al * (outA[k] + inB[k]);
                 // P = dpdq.x; forward q2d: semi-implicit pressure source
-                // (q2d time_lusgs_viscous.f90:38-44)
-                RT P = RT(0), S = RT(0);
+                // (q2d time_lusgs_viscous.f90:38-44).  Both sums are pairwise trees.
+                RT pr[D - 1];
 #pragma unroll
-                for (int k = 0; k < D; ++k)
-                    if (k != NY + 1) P += f[R::DP + k] * x[k];
-#pragma unroll
-                for (int k = 0; k < NY; ++k) S += x[k];
+                for (int k = 0; k < D - 1; ++k) {
+                    const int kk = k < NY + 1 ? k : k + 1;  // every component but rho v
+                    pr[k] = f[R::DP + kk] * x[kk];
+                }
+                RT P = tree_sum<0, D - 1>(pr);
+                const RT S = tree_sum<0, NY>(x);
                 if (DIR == 0 && q2d) x[NY + 1] = (x[NY + 1] + f[R::AA] * P) * f[R::RQ];
                 P += f[R::DP + NY + 1] * x[NY + 1];
 #pragma unroll
                 for (int dn = 0; dn < 2; ++dn) {
                     const int b0 = dn == 0 ? R::FA : R::FB;
                     const RT fa = f[b0], n1 = f[b0 + 1], n2 = f[b0 + 2], un = f[b0 + 3], nu = f[b0 + 4];
-                    const RT base_ = n1 * x[NY] + n2 * x[NY + 1] - un * S;
-                    const RT lam = DIR == 0 ? un + nu : un - nu;
+                    // ds/2 folded into the coefficients: o = cv (fa base) + (fa lam) x [+ (fa P) n]
+                    const RT fb = fa * (n1 * x[NY] + n2 * x[NY + 1] - un * S);
+                    const RT fl = fa * (DIR == 0 ? un + nu : un - nu);
+                    const RT fp = fa * P;
                     RT* o = dn == 0 ? outA : outB;
 #pragma unroll
-                    for (int k = 0; k < NY; ++k) o[k] = fa * (f[R::CV + k] * base_ + lam * x[k]);
-                    o[NY] = fa * (f[R::CV + NY] * base_ + lam * x[NY] + n1 * P);
-                    o[NY + 1] = fa * (f[R::CV + NY + 1] * base_ + lam * x[NY + 1] + n2 * P);
-                    o[NY + 2] = fa * (f[R::CV + NY + 2] * base_ + lam * x[NY + 2] + un * P);
+                    for (int k = 0; k < NY; ++k) o[k] = f[R::CV + k] * fb + fl * x[k];
+                    o[NY] = f[R::CV + NY] * fb + fl * x[NY] + n1 * fp;
+                    o[NY + 1] = f[R::CV + NY + 1] * fb + fl * x[NY + 1] + n2 * fp;
+                    o[NY + 2] = f[R::CV + NY + 2] * fb + fl * x[NY + 2] + un * fp;
                 }
                 // results back into the record block (16-byte stores)
 #pragma unroll
@@ -362,7 +385,7 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
                 const int cc = t - 31;
                 if (publish && cc >= 0) {
 #pragma unroll
-                    for (int k = 0; k < D; ++k) xout[(long long)cc * D + k] = double(outB[k]);
+                    for (int k = 0; k < D; ++k) xout[(long long)cc * D + k] = outB[k];
                 }
                 __syncwarp();
             }
@@ -477,7 +500,7 @@ size_t sweep3_record_elems(int ny, bool mixed) {
 template <typename RT, int NY, int DIR>
 static void sweep_launch(const View& v, cudaStream_t s, const Sweep3& w) {
     using L = RecLayout<RT, NY>;
-    const size_t smem = (size_t)PFB * SPB * L::STEP * sizeof(RT) + 8 * (NY + 3) * sizeof(double) + PFB * 8;
+    const size_t smem = (size_t)PFB * Spb<RT>::value * L::STEP * sizeof(RT) + 8 * (NY + 3) * sizeof(double) + PFB * 8;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_sweep3<RT, NY, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
