@@ -266,7 +266,8 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
 #pragma unroll
         for (int k = 0; k < D; ++k) { outA[k] = RT(0); outB[k] = RT(0); }
         double res = 0.0;
-        double on = __longlong_as_double(0x7FF0000000000000ll), od = 1.0;  // omega candidate q / (-Dq)
+        // omega candidate q / (-Dq), kept as the pair (q, -Dq) in the record precision
+        RT on = RT(__longlong_as_double(0x7FF0000000000000ll)), od = RT(1);
         RT* gblk = const_cast<RT*>(rd) + lf * G;
         for (int tb = 0; tb < nblk8 && !bail; ++tb) {
             const int t0 = tb * 8;
@@ -374,9 +375,9 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
 #pragma unroll
                     for (int k = 0; k < NY; ++k) {
                         // smallest q_k/(-Dq_k) over Dq_k < 0, compared by cross-multiplication
-                        const double dk = double(x[k]);
-                        const double qn = double(f[R::QS + k]), qd = -dk;
-                        if (dk < 0.0 && qn * od < on * qd) {
+                        const RT dk = x[k];
+                        const RT qn = f[R::QS + k], qd = -dk;
+                        if (dk < RT(0) && qn * od < on * qd) {
                             on = qn;
                             od = qd;
                         }
@@ -408,14 +409,14 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
         if (DIR == 1 && nr) {
             for (int o = 16; o > 0; o >>= 1) {
                 res += __shfl_xor_sync(0xffffffffu, res, o);
-                const double on2 = __shfl_xor_sync(0xffffffffu, on, o), od2 = __shfl_xor_sync(0xffffffffu, od, o);
+                const RT on2 = __shfl_xor_sync(0xffffffffu, on, o), od2 = __shfl_xor_sync(0xffffffffu, od, o);
                 if (on2 * od < on * od2) {
                     on = on2;
                     od = od2;
                 }
             }
             if (lane == 0) {
-                const double om = on / od * v.dq_max;   // -q/Dq*Dqmax of the limiting cell
+                const double om = double(on) / double(od) * v.dq_max;  // -q/Dq*Dqmax of the limiting cell
                 partials[2 * fs] = res;
                 partials[2 * fs + 1] = om;
                 if (om < v.omega_min) atomicMax(&v.sc->status, SCFD_E_OMEGA);
