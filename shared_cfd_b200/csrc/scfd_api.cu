@@ -64,6 +64,11 @@ struct scfd_ctx {
     int cells_max = 0;
     // per-kernel timing
     bool profiling = false;
+    // the whole physical step as one CUDA graph (captured at the second step)
+    bool use_graph = true;
+    int eager_steps = 0;
+    cudaGraphExec_t graph = nullptr;
+    long long graph_launches = 0;
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
     std::vector<std::pair<int, size_t>> ev_marks;  // kind, index of the start event
@@ -534,6 +539,7 @@ int scfd_create(const scfd_desc* d, scfd_ctx** out) {
 
 int scfd_destroy(scfd_ctx* c) {
     if (!c) return SCFD_E_ARG;
+    if (c->graph) cudaGraphExecDestroy(c->graph);
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     if (c->arena) cudaFree(c->arena);
     if (c->h_sc) cudaFreeHost(c->h_sc);
@@ -671,6 +677,8 @@ int scfd_commit(scfd_ctx* c) {
     const size_t esz3 = mixed ? sizeof(float) : sizeof(double);
     const char* sweep_env = std::getenv("SCFD_SWEEP");
     const bool legacy = std::getenv("SCFD_SWEEP_LEGACY") != nullptr;
+    const char* graph_env = std::getenv("SCFD_GRAPH");
+    c->use_graph = !(graph_env && std::strcmp(graph_env, "0") == 0);
     int qc4 = 0;
     const size_t blk4 = impl ? sweep4_record_elems(nY, mixed, &qc4) : 0;
     c->use_sw4 = blk4 > 0 && !legacy && sweep_env && std::strcmp(sweep_env, "4") == 0;
@@ -970,6 +978,42 @@ int scfd_prepare(scfd_ctx* c, int step) {
     return c->h_sc->status;
 }
 
+// One physical step.  The first step of a context runs eagerly (it also sets
+// the kernels' shared-memory attributes); the second is captured into a CUDA
+// graph, which every later step replays with one launch.  The graph holds
+// device pointers and host constants of the context only: dt, time and status
+// live on the device.  Profiled steps run eagerly (their events are recorded
+// between the kernels).
+int step_once(scfd_ctx* c) {
+    if (c->profiling || !c->use_graph || c->eager_steps < 1) {
+        ++c->eager_steps;
+        return enqueue_step(c);
+    }
+    if (!c->graph) {
+        const long long before = c->launches;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const int st = enqueue_step(c);
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (st) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (e != cudaSuccess) return c->fail(SCFD_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        const cudaError_t ei = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            c->graph = nullptr;
+            return c->fail(SCFD_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        }
+        c->graph_launches = c->launches - before;
+        c->launches = before;
+    }
+    CK(cudaGraphLaunch(c->graph, c->stream));
+    c->launches += c->graph_launches;
+    return 0;
+}
+
 int scfd_step(scfd_ctx* c, int step, scfd_stats* stats) {
     if (!c || !c->committed || !c->uploaded) return c ? c->fail(SCFD_E_STATE, "step before upload") : SCFD_E_ARG;
     (void)step;
@@ -977,7 +1021,7 @@ int scfd_step(scfd_ctx* c, int step, scfd_stats* stats) {
     if (st) return st;
     const long long att0 = c->h_sc->chem_attempts, fb0 = c->h_sc->chem_fallback;
     c->launches = 0;
-    if ((st = enqueue_step(c))) return st;
+    if ((st = step_once(c))) return st;
     if ((st = sync_scalars(c))) return st;
     collect_events(c);
     return fill_stats(c, stats, att0, fb0);
@@ -991,7 +1035,7 @@ int scfd_run(scfd_ctx* c, int step, int nsteps, scfd_stats* stats) {
     const long long att0 = c->h_sc->chem_attempts, fb0 = c->h_sc->chem_fallback;
     c->launches = 0;
     for (int n = 0; n < nsteps; ++n) {
-        if ((st = enqueue_step(c))) return st;
+        if ((st = step_once(c))) return st;
         if (c->profiling && c->ev_used > 4096) collect_events(c);
     }
     if ((st = sync_scalars(c))) return st;

@@ -160,3 +160,24 @@ def test_reacting_step_two_tasks_per_plane(gpu, orc):
     128-row planes run as two tasks of eight strips."""
     case = cases.reacting_step(scale=0.25, inner=3)
     _parity(case, gpu, orc, 1)
+
+
+def test_graph_replay_matches_eager(gpu, monkeypatch):
+    """Steps replayed from the captured CUDA graph give bit-identical states to
+    the same kernels launched one by one."""
+    out = {}
+    for mode in ("eager", "graph"):
+        if mode == "eager":
+            monkeypatch.setenv("SCFD_GRAPH", "0")
+        else:
+            monkeypatch.delenv("SCFD_GRAPH", raising=False)
+        case = cases.reacting_step(scale=1.0 / 32.0, inner=4, precision=abi.PREC_MIXED)
+        s = Solver(case)
+        s.upload()
+        s.prepare(1)
+        st = s.run(1, 4)
+        assert st.status == 0
+        out[mode] = (s.download()[0], s.launch_count())
+        s.close()
+    assert np.array_equal(out["eager"][0], out["graph"][0])
+    assert out["eager"][1] == out["graph"][1]
