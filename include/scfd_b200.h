@@ -226,6 +226,60 @@ enum {
 int  scfd_profile(scfd_ctx* ctx, int enable);
 int  scfd_kernel_stats(scfd_ctx* ctx, int kind, double* total_ms, int64_t* launches, char* name, int namelen);
 
+/* ---- batched constant-volume 0-D reactors ---------------------------------
+ * Replaces per-reactor calls of reaction_chemeq2 / reaction_one_steps
+ * (store/therm_lib/chemkin/core/sub_chem.f90:1684-1713 and 1396-1504).  Each
+ * reactor integrates its moles n_1..n_ns (mol/cm^3, from the partial densities
+ * as n = vrho/MW*1e-3, floored at 1e-40) and T from t = 0 to t_end by
+ * successive reaction_chemeq2 calls over dt_call (CHEMEQ2, sub_chem.f90:1714-1819,
+ * on the UV source terms; each call starts its own attempt count and floors n
+ * at 1e-40 on entry and exit, as the reference's), and records the ignition
+ * delay of reaction_one_steps (sub_chem.f90:1467-1472): the first time
+ * T >= T0 + dT_ign, interpolated linearly between the accepted substeps around
+ * it (the state at t = 0 is the first of them).  Where the reference hands the
+ * rest of a call to DVODE after 10 CHEMEQ2 attempts, the library takes
+ * two-stage Rosenbrock (ROS2) substeps and flags the reactor
+ * SCFD_REACTOR_FELL_BACK. */
+enum {
+    SCFD_REACTOR_QUEUE = 0,      /* one persistent launch, reactors drawn from a device work queue
+                                    (replayed from a CUDA graph after the first run) */
+    SCFD_REACTOR_PER_LAUNCH = 1  /* one kernel launch per reactor */
+};
+enum { SCFD_REACTOR_IGNITED = 1, SCFD_REACTOR_FELL_BACK = 2, SCFD_REACTOR_FAILED = 4 };
+
+typedef struct scfd_reactor_desc {
+    int32_t abi_version;
+    int32_t n;             /* reactors in this run (<= n_max of scfd_reactors_create) */
+    int32_t mode;          /* SCFD_REACTOR_QUEUE / SCFD_REACTOR_PER_LAUNCH */
+    int32_t max_substeps;  /* accepted substeps per call before SCFD_E_CHEM (<= 0: 1e6) */
+    double  t_end;         /* s */
+    double  dT_ign;        /* K (the reference uses 400) */
+    double  dt_call;       /* s: interval of each reaction_chemeq2 call (a flow solver's
+                              time step); <= 0 means one call over [0, t_end] */
+    int32_t reserved[6];
+} scfd_reactor_desc;
+
+typedef struct scfd_reactors scfd_reactors;
+
+int   scfd_reactors_create(const scfd_chem* chem, int n_max, scfd_reactors** out);
+int   scfd_reactors_destroy(scfd_reactors* r);
+/* T0[n] in K; vrho0[n][ns] partial densities in kg/m^3 (the q(1:ns) of a cell) */
+int   scfd_reactors_upload(scfd_reactors* r, int n, const double* T0, const double* vrho0);
+/* integrates the uploaded reactors, asynchronously on scfd_reactors_stream(r) */
+int   scfd_reactors_launch(scfd_reactors* r, const scfd_reactor_desc* d);
+/* after a launch: T_end[n], vrho_end[n][ns], t_ign[n] (s, -1 when T never
+ * reached T0 + dT_ign), evals[n] = source-term (Fex_var) evaluations (2 per
+ * CHEMEQ2 attempt, ns+3 per Rosenbrock substep), flags[n]; any pointer may be
+ * NULL.  Returns the worst status of the run. */
+int   scfd_reactors_download(scfd_reactors* r, double* T_end, double* vrho_end, double* t_ign, int64_t* evals,
+                             int32_t* flags);
+/* upload + launch + download */
+int   scfd_reactors_run(scfd_reactors* r, const scfd_reactor_desc* d, const double* T0, const double* vrho0,
+                        double* T_end, double* vrho_end, double* t_ign, int64_t* evals, int32_t* flags);
+void* scfd_reactors_stream(scfd_reactors* r);
+/* kernel launches made by the last scfd_reactors_launch */
+int   scfd_reactors_launch_count(const scfd_reactors* r, int64_t* launches);
+
 /* ---- no-allocation entry point ------------------------------------------ */
 /* Capacity of the library's static scratch for scfd_rms_noalloc: partial sums
  * of 64 blocks for each of at most SCFD_MAX_PLANES planes. */

@@ -494,9 +494,137 @@ void fex_var(const scfd_chem& ch, const double* n, double* dndtp, double* dndtm)
 
 namespace {
 
-// chemeq2, sub_chem.f90:1714-1819; returns 0, or SCFD_E_CHEM.
+// Ignition delay of reaction_one_steps (sub_chem.f90:1467-1472), taken after
+// every accepted substep: the first time T >= T0 + dT, interpolated linearly
+// from the previous accepted substep (initially t = 0, T0).
+struct Ignition {
+    double T0, dT, t_old, T_old, t_ign;
+    bool ignited;
+    double t_off;  // time at the start of the current reaction_chemeq2 call
+};
+
+void track_ignition(Ignition& g, double tt, double T) {
+    const double t = g.t_off + tt;
+    const double Tig = g.T0 + g.dT;
+    if (!g.ignited && T >= Tig) {
+        g.t_ign = t - (T - Tig) / (T - g.T_old) * (t - g.t_old);
+        g.ignited = true;
+    }
+    g.T_old = T;
+    g.t_old = t;
+}
+
+void rates(const scfd_chem& ch, const double* y, double* f, double* tmp) {
+    fex_var(ch, y, f, tmp);
+    for (int i = 0; i <= ch.ns; ++i) f[i] = f[i] + tmp[i];
+}
+
+// CHEMEQ2 tolerance y*rtol + rtol*1e-5 for the species (sub_chem.f90:1801), rtol*T for T
+double be_weight(int i, int ns, double yi, double rtol) {
+    return i < ns ? std::fabs(yi) * rtol + rtol * 1e-5 : std::fabs(yi) * rtol;
+}
+
+bool lu_factor(double* M, int* piv, int N) {
+    for (int k = 0; k < N; ++k) {
+        int pk = k;
+        double best = std::fabs(M[k * N + k]);
+        for (int i = k + 1; i < N; ++i)
+            if (std::fabs(M[i * N + k]) > best) {
+                best = std::fabs(M[i * N + k]);
+                pk = i;
+            }
+        piv[k] = pk;
+        if (!(best > 0.0)) return false;
+        if (pk != k)
+            for (int j = 0; j < N; ++j) std::swap(M[k * N + j], M[pk * N + j]);
+        const double inv = 1.0 / M[k * N + k];
+        for (int i = k + 1; i < N; ++i) {
+            const double l = M[i * N + k] * inv;
+            M[i * N + k] = l;
+            for (int j = k + 1; j < N; ++j) M[i * N + j] = M[i * N + j] - l * M[k * N + j];
+        }
+    }
+    return true;
+}
+
+void lu_solve(const double* M, const int* piv, int N, double* b) {
+    for (int k = 0; k < N; ++k)
+        if (piv[k] != k) std::swap(b[k], b[piv[k]]);
+    for (int i = 1; i < N; ++i)
+        for (int j = 0; j < i; ++j) b[i] = b[i] - M[i * N + j] * b[j];
+    for (int i = N - 1; i >= 0; --i) {
+        for (int j = i + 1; j < N; ++j) b[i] = b[i] - M[i * N + j] * b[j];
+        b[i] = b[i] / M[i * N + i];
+    }
+}
+
+// Rest of an interval after 10 CHEMEQ2 attempts (where sub_chem.f90:1755-1775
+// calls DVODE): substeps of the two-stage Rosenbrock method ROS2 (Verwer,
+// Spee, Blom, Hundsdorfer, SIAM J. Sci. Comput. 20, 1999), gamma = 1 + 1/sqrt(2),
+//     (I - gamma h J) k1 = f(y0),  (I - gamma h J) k2 = f(y0 + h k1) - 2 k1,
+//     y = y0 + 3/2 h k1 + 1/2 h k2,  error |h/2 (k1 + k2)|,
+// with a forward-difference Jacobian at y0 and step factor 0.8/sqrt(err) in
+// [0.2, 2].  y holds the accepted state at tt on entry and the state at tout
+// on return.  The same substeps as be_attempt of the CUDA path, in the same order.
+int implicit_rest(const scfd_chem& ch, double* y, double tt, double tout, double dt, double rtol,
+                  long long& attempts, int& substeps, int max_substeps, Ignition* ign, long long& evals) {
+    const int ns = ch.ns, N = ns + 1;
+    const double gam = 1.7071067811865475;
+    double y0[SCFD_MAX_SPECIES + 1], f0[SCFD_MAX_SPECIES + 1], f[SCFD_MAX_SPECIES + 1], tmp[SCFD_MAX_SPECIES + 1],
+        k1[SCFD_MAX_SPECIES + 1], k2[SCFD_MAX_SPECIES + 1], M[(SCFD_MAX_SPECIES + 1) * (SCFD_MAX_SPECIES + 1)];
+    int piv[SCFD_MAX_SPECIES + 1];
+    for (int i = 0; i < N; ++i) y0[i] = y[i];
+    int rejects = 0;
+    for (;;) {
+        ++attempts;
+        double h = dt;
+        if (tout - tt < h) h = tout - tt;
+        rates(ch, y0, f0, tmp);
+        for (int j = 0; j < N; ++j) {
+            for (int i = 0; i < N; ++i) y[i] = y0[i];
+            const double dj = 1.4901161193847656e-8 * std::max(std::fabs(y0[j]), j < ns ? 1e-10 : 1.0);
+            y[j] = y0[j] + dj;
+            rates(ch, y, f, tmp);
+            for (int i = 0; i < N; ++i) M[i * N + j] = (i == j ? 1.0 : 0.0) - gam * h * (f[i] - f0[i]) / dj;
+        }
+        double err = 1e300;
+        if (lu_factor(M, piv, N)) {
+            for (int i = 0; i < N; ++i) k1[i] = f0[i];
+            lu_solve(M, piv, N, k1);
+            for (int i = 0; i < N; ++i) y[i] = y0[i] + h * k1[i];
+            rates(ch, y, f, tmp);
+            for (int i = 0; i < N; ++i) k2[i] = f[i] - 2.0 * k1[i];
+            lu_solve(M, piv, N, k2);
+            err = 0.0;
+            for (int i = 0; i < N; ++i) {
+                y[i] = y0[i] + 1.5 * h * k1[i] + 0.5 * h * k2[i];
+                const double e = std::fabs(0.5 * h * (k1[i] + k2[i])) / be_weight(i, ns, y[i], rtol);
+                err = (e > err || e != e) ? e : err;
+            }
+        }
+        evals += N + 2;
+        if (!(err <= 1.0)) {
+            dt = h * (err == err && err < 1e300 ? std::max(0.2, 0.8 / std::sqrt(err)) : 0.25);
+            if (++rejects > 30) return SCFD_E_CHEM;
+            continue;
+        }
+        rejects = 0;
+        tt = tt + h;
+        for (int i = 0; i < N; ++i) y0[i] = y[i];
+        dt = h * std::min(2.0, std::max(0.2, 0.8 / std::sqrt(std::max(err, 1e-10))));
+        if (ign) track_ignition(*ign, tt, y[ns]);
+        if (tout <= tt) return 0;
+        if (++substeps > max_substeps) return SCFD_E_CHEM;
+    }
+}
+
+// chemeq2, sub_chem.f90:1714-1819; returns 0, or SCFD_E_CHEM.  With `ign`,
+// the ignition test runs after every accepted substep; `evals` counts the
+// source-term evaluations.
 int chemeq2(const scfd_chem& ch, double* y, double tt, double tout, double rtol, long long& attempts,
-            bool& fell_back, int max_substeps) {
+            bool& fell_back, int max_substeps, Ignition* ign = nullptr, long long* evals = nullptr) {
+    long long ev_local = 0;
+    long long& ev = evals ? *evals : ev_local;
     const int ns = ch.ns;
     double y0[SCFD_MAX_SPECIES + 1], yp[SCFD_MAX_SPECIES + 1], p[SCFD_MAX_SPECIES + 1], q[SCFD_MAX_SPECIES + 1],
         p0[SCFD_MAX_SPECIES + 1], q0[SCFD_MAX_SPECIES + 1];
@@ -512,10 +640,14 @@ int chemeq2(const scfd_chem& ch, double* y, double tt, double tout, double rtol,
             for (int i = 0; i <= ns; ++i) y[i] = y0[i];
             countersum = countersum + 1;
             // Reference: after 10 attempts the rest of the interval goes to DVODE
-            // (sub_chem.f90:1755-1775).  Fallback shared with the CUDA path: keep
-            // taking alpha-QSS substeps; the cell is counted as a deviation.
-            if (countersum > 10) fell_back = true;
+            // (sub_chem.f90:1755-1775); here to the Rosenbrock substeps of
+            // implicit_rest (shared with the CUDA path), and the cell is counted.
+            if (countersum > 10) {
+                fell_back = true;
+                return implicit_rest(ch, y, tt, tout, dt, rtol, attempts, substeps, max_substeps, ign, ev);
+            }
             ++attempts;
+            ev += 2;
             // predictor
             fex_var(ch, y, q0, p0);
             for (int i = 0; i < ns; ++i) {
@@ -536,7 +668,7 @@ int chemeq2(const scfd_chem& ch, double* y, double tt, double tout, double rtol,
                 q[i] = alp * q[i] + (1.0 - alp) * q0[i];
                 y[i] = y0[i] + dt * (q[i] - p[i] * y0[i]) / (1.0 + alp * p[i] * dt);
                 var = (y[i] * rtol + rtol * 1e-5) / std::fabs(y[i] - yp[i] + 1e-300);
-                ratio = std::min(ratio, var);
+                ratio = (var < ratio || var != var) ? var : ratio;  // a NaN ratio rejects the attempt
             }
             y[ns] = y0[ns] + 0.5 * dt * (q[ns] + p[ns] + q0[ns] + p0[ns]);
             if (1.0 < ratio) break;
@@ -545,6 +677,7 @@ int chemeq2(const scfd_chem& ch, double* y, double tt, double tout, double rtol,
             if (counter > 10.0) return SCFD_E_CHEM;
         }
         tt = tt + dt;
+        if (ign) track_ignition(*ign, tt, y[ns]);
         if (tout <= tt) break;
         dt = dt * std::sqrt(ratio);
         if (++substeps > max_substeps) return SCFD_E_CHEM;
@@ -1608,6 +1741,125 @@ int orc_chemeq2(const scfd_chem* ch, double* y, double tout, int64_t* attempts, 
     if (attempts) *attempts = a;
     if (fell_back) *fell_back = fb ? 1 : 0;
     return s;
+}
+
+// ---- batched constant-volume 0-D reactors: successive reaction_chemeq2 calls
+// (sub_chem.f90:1684-1713) over dt_call up to t_end per reactor, with the
+// ignition test of reaction_one_steps; reactors in parallel over OpenMP threads.
+struct orc_reactors {
+    scfd_chem ch;
+    int n_max = 0, n = 0, status = 0;
+    long long launches = 0;
+    std::vector<double> T0, vrho0, T_end, vrho_end, t_ign;
+    std::vector<int64_t> evals;
+    std::vector<int32_t> flags;
+};
+
+int orc_reactors_create(const scfd_chem* ch, int n_max, orc_reactors** out) {
+    if (!ch || !out || n_max < 1 || ch->ns < 1 || ch->ns > SCFD_MAX_SPECIES || ch->nr < 0 ||
+        ch->nr > SCFD_MAX_REACTIONS)
+        return SCFD_E_ARG;
+    orc_reactors* r = new orc_reactors();
+    r->ch = *ch;
+    r->n_max = n_max;
+    const size_t nn = (size_t)n_max, nv = nn * ch->ns;
+    r->T0.assign(nn, 0.0);
+    r->vrho0.assign(nv, 0.0);
+    r->T_end.assign(nn, 0.0);
+    r->vrho_end.assign(nv, 0.0);
+    r->t_ign.assign(nn, -1.0);
+    r->evals.assign(nn, 0);
+    r->flags.assign(nn, 0);
+    *out = r;
+    return 0;
+}
+
+int orc_reactors_destroy(orc_reactors* r) {
+    if (!r) return SCFD_E_ARG;
+    delete r;
+    return 0;
+}
+
+int orc_reactors_upload(orc_reactors* r, int n, const double* T0, const double* vrho0) {
+    if (!r || !T0 || !vrho0 || n < 1 || n > r->n_max) return SCFD_E_ARG;
+    std::copy(T0, T0 + n, r->T0.begin());
+    std::copy(vrho0, vrho0 + (size_t)n * r->ch.ns, r->vrho0.begin());
+    r->n = n;
+    return 0;
+}
+
+int orc_reactors_launch(orc_reactors* r, const scfd_reactor_desc* d) {
+    if (!r || !d || d->abi_version != SCFD_ABI_VERSION || d->n < 1 || d->n != r->n || !(d->t_end > 0.0) ||
+        (d->mode != SCFD_REACTOR_QUEUE && d->mode != SCFD_REACTOR_PER_LAUNCH))
+        return SCFD_E_ARG;
+    const scfd_chem& ch = r->ch;
+    const int ns = ch.ns, maxsub = d->max_substeps > 0 ? d->max_substeps : 1000000;
+    double inv[SCFD_MAX_SPECIES];
+    for (int j = 0; j < ns; ++j) inv[j] = 1.0 / ch.mws[j];  // invMW
+    int worst = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(max : worst)
+    for (int k = 0; k < d->n; ++k) {
+        double y[SCFD_MAX_SPECIES + 1];
+        for (int j = 0; j < ns; ++j) y[j] = std::max(r->vrho0[(size_t)k * ns + j] * inv[j] * 1e-3, 1e-40);
+        y[ns] = r->T0[k];
+        Ignition g{r->T0[k], d->dT_ign, 0.0, r->T0[k], -1.0, false, 0.0};
+        long long att = 0, ev = 0;
+        bool fb = false, any_fb = false;
+        int rc = 0;
+        // successive reaction_chemeq2 calls over dt_call: moles floored at n_eps
+        // and passed through the partial densities between calls
+        double tg = 0.0;
+        for (;;) {
+            const double rest = d->t_end - tg;
+            const double tout = (d->dt_call > 0.0 && d->dt_call < rest) ? d->dt_call : rest;
+            g.t_off = tg;
+            rc = chemeq2(ch, y, 0.0, tout, ch.rtol, att, fb, maxsub, &g, &ev);
+            any_fb = any_fb || fb;
+            if (rc) break;
+            tg = tg + tout;
+            for (int j = 0; j < ns; ++j) y[j] = std::max(std::max(y[j], 1e-40) * ch.mws[j] * 1e3 * inv[j] * 1e-3, 1e-40);
+            if (!(d->t_end - tg > 1e-12 * d->t_end)) break;
+        }
+        r->T_end[k] = y[ns];
+        for (int j = 0; j < ns; ++j) r->vrho_end[(size_t)k * ns + j] = std::max(y[j], 1e-40) * ch.mws[j] * 1e3;
+        r->t_ign[k] = g.ignited ? g.t_ign : -1.0;
+        r->evals[k] = ev;
+        r->flags[k] = (g.ignited ? SCFD_REACTOR_IGNITED : 0) | (any_fb ? SCFD_REACTOR_FELL_BACK : 0) |
+                      (rc ? SCFD_REACTOR_FAILED : 0);
+        worst = std::max(worst, rc);
+    }
+    r->status = worst;
+    r->launches = 0;
+    return 0;
+}
+
+int orc_reactors_download(orc_reactors* r, double* T_end, double* vrho_end, double* t_ign, int64_t* evals,
+                          int32_t* flags) {
+    if (!r || r->n < 1) return SCFD_E_ARG;
+    const size_t n = (size_t)r->n, nv = n * r->ch.ns;
+    if (T_end) std::copy(r->T_end.begin(), r->T_end.begin() + n, T_end);
+    if (vrho_end) std::copy(r->vrho_end.begin(), r->vrho_end.begin() + nv, vrho_end);
+    if (t_ign) std::copy(r->t_ign.begin(), r->t_ign.begin() + n, t_ign);
+    if (evals) std::copy(r->evals.begin(), r->evals.begin() + n, evals);
+    if (flags) std::copy(r->flags.begin(), r->flags.begin() + n, flags);
+    return r->status;
+}
+
+int orc_reactors_run(orc_reactors* r, const scfd_reactor_desc* d, const double* T0, const double* vrho0,
+                     double* T_end, double* vrho_end, double* t_ign, int64_t* evals, int32_t* flags) {
+    if (!d) return SCFD_E_ARG;
+    int st = orc_reactors_upload(r, d->n, T0, vrho0);
+    if (st) return st;
+    if ((st = orc_reactors_launch(r, d))) return st;
+    return orc_reactors_download(r, T_end, vrho_end, t_ign, evals, flags);
+}
+
+void* orc_reactors_stream(orc_reactors*) { return nullptr; }
+
+int orc_reactors_launch_count(const orc_reactors* r, int64_t* launches) {
+    if (!r || !launches) return SCFD_E_ARG;
+    *launches = r->launches;
+    return 0;
 }
 
 }  // extern "C"

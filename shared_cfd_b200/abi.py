@@ -115,6 +115,23 @@ class Stats(C.Structure):
     ]
 
 
+REACTOR_QUEUE, REACTOR_PER_LAUNCH = 0, 1
+REACTOR_IGNITED, REACTOR_FELL_BACK, REACTOR_FAILED = 1, 2, 4
+
+
+class ReactorDesc(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32),
+        ("n", C.c_int32),
+        ("mode", C.c_int32),
+        ("max_substeps", C.c_int32),
+        ("t_end", C.c_double),
+        ("dT_ign", C.c_double),
+        ("dt_call", C.c_double),
+        ("reserved", C.c_int32 * 6),
+    ]
+
+
 # Exported entry points: name -> (restype, argtypes); the prefix (scfd_ for the
 # CUDA library) is added by bind().
 _P = C.c_void_p
@@ -140,6 +157,15 @@ SIGNATURES = {
     "launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "profile": (C.c_int, [_P, C.c_int]),
     "kernel_stats": (C.c_int, [_P, C.c_int, _D, C.POINTER(C.c_int64), C.c_char_p, C.c_int]),
+    "reactors_create": (C.c_int, [C.POINTER(Chem), C.c_int, C.POINTER(_P)]),
+    "reactors_destroy": (C.c_int, [_P]),
+    "reactors_upload": (C.c_int, [_P, C.c_int, _D, _D]),
+    "reactors_launch": (C.c_int, [_P, C.POINTER(ReactorDesc)]),
+    "reactors_download": (C.c_int, [_P, _D, _D, _D, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "reactors_run": (C.c_int, [_P, C.POINTER(ReactorDesc), _D, _D, _D, _D, _D, C.POINTER(C.c_int64),
+                               C.POINTER(C.c_int32)]),
+    "reactors_stream": (_P, [_P]),
+    "reactors_launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
 }
 K_THERMO, K_BC, K_DT, K_CHEM, K_RESIDUAL, K_SWEEP_FWD, K_SWEEP_BWD, K_UPDATE, K_COPY, K_OTHER, K_PACK, K_COUNT = \
     range(12)

@@ -13,6 +13,9 @@ All inputs are generated here from seeds; no dataset is read.
                       with dt = 1e-7 s and 20 inner iterations, chemistry split.
 * forward_step(...)   two-block ideal-gas case in the four orientations of the
                       reference's forward-step samples (halo exchange checks).
+* reactor_batch(...)  constant-volume H2/air 0-D reactors on the reacting-step
+                      mechanism: T0 uniform in [900, 1600] K, p uniform in
+                      [1, 20] atm, equivalence ratio uniform in [0.3, 3.0].
 """
 import math
 import os
@@ -404,3 +407,35 @@ def perturb(case, seed=1, amp=0.05):
         w[:, :, 2] = v2
         w[:, :, 3] = w[:, :, 3] * (1.0 + 0.5 * amp * f2)
     return case
+
+
+ATM = 101325.0
+
+
+def reactor_batch(n=8192, seed=20240611, mech_seed=20240607, T_range=(900.0, 1600.0), p_atm=(1.0, 20.0),
+                  phi_range=(0.3, 3.0)):
+    """Initial states of n constant-volume H2/air reactors.
+
+    Mole fractions H2 : O2 : N2 = 2 phi : 1 : 3.76; the partial densities follow
+    from p and T0 as rho_rel2abs (sub_chem.f90:1036-1085) forms them from
+    relative densities (here the mass fractions).  Returns (mechanism, scfd_chem,
+    T0[n], vrho0[n][ns], draws) with draws = (T0, p [Pa], phi)."""
+    m, _ = h2air_mechanism(mech_seed)
+    ns = len(m.species)
+    rng = np.random.default_rng(seed)
+    T0 = rng.uniform(T_range[0], T_range[1], n)
+    p = rng.uniform(p_atm[0], p_atm[1], n) * ATM
+    phi = rng.uniform(phi_range[0], phi_range[1], n)
+    idx = {s.strip().upper(): k for k, s in enumerate(m.species)}
+    mw = np.asarray(m.mws)
+    vrho = np.zeros((n, ns))
+    for r in range(n):
+        X = np.zeros(ns)
+        X[idx["H2"]] = 2.0 * phi[r]
+        X[idx["O2"]] = 1.0
+        X[idx["N2"]] = 3.76
+        Y = X * mw
+        Y = Y / Y.sum()
+        _, _, v = CH.rho_rel2abs(m, p[r], T0[r], list(Y))
+        vrho[r] = v
+    return m, CH.to_struct(m), T0, vrho, (T0, p, phi)

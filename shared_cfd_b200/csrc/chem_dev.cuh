@@ -1,0 +1,290 @@
+// chem_dev.cuh -- device restatement of the UV source terms Fex_var
+// (store/therm_lib/chemkin/uvhp/uv/FJ.f90:301-453) and of one CHEMEQ2 attempt
+// (store/therm_lib/chemkin/core/sub_chem.f90:1714-1819), with the implicit
+// substeps that take over where the reference calls DVODE; shared by the flow
+// chemistry kernel and the batched 0-D reactors.
+#pragma once
+
+#include "scfd_internal.h"
+
+namespace scfd {
+
+__device__ inline void dev_fex_var(const DevChem& ch, const double* n, double* dndtp, double* dndtm) {
+    const int ns = ch.ns;
+    const double pst = 1.01325e6, Ru = 8.3144621e7;
+    const double loge210 = (double)0.43429448190325f;
+    const double T = n[ns];
+    const double logT = log(T), Tinv = 1.0 / T;
+    const double logPRT = log(pst / Ru) - logT;
+    double sn = 0.0;
+    for (int j = 0; j < ns; ++j) sn += n[j];
+    const double logsn = log(sn);
+    const double T2 = T * T, T3 = T2 * T, T4 = T3 * T;
+    const double cmurt[7] = {1.0 - logT, -T / 2.0, -T2 / 6.0, -T3 / 12.0, -T4 / 20.0, Tinv, -1.0};
+    const double chrt[7] = {1.0, T / 2.0, T2 / 3.0, T3 / 4.0, T4 / 5.0, Tinv, 0.0};
+    const double ccpr[7] = {1.0, T, T2, T3, T4, 0.0, 0.0};
+    double vmu0rt[kMaxSpecies], vert[kMaxSpecies], vcvr[kMaxSpecies];
+    for (int j = 0; j < ns; ++j) {
+        const double* cf = ch.coeff + (j * 2 + (T <= ch.tcommon[j] ? 0 : 1)) * 7;
+        double t1 = 0.0, t2 = -1.0, t3 = -1.0;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+            const double c = cf[i];
+            t1 = t1 + c * cmurt[i];
+            t2 = t2 + c * chrt[i];
+            t3 = t3 + c * ccpr[i];
+        }
+        vmu0rt[j] = t1;
+        vert[j] = t2;
+        vcvr[j] = t3;
+        dndtp[j] = 0.0;
+        dndtm[j] = 0.0;
+    }
+    const double dd = 0.14;
+    double vlogM = 0.0;
+    for (int i = 0; i < ch.nr; ++i) {
+        const int rs0 = ch.rstate[2 * i], rs1 = ch.rstate[2 * i + 1];
+        if (ch.exist_m[i]) {
+            double tmp = sn;
+            const int nm = ch.numm[i];
+            for (int j = 0; j < nm; ++j) tmp = tmp + ch.men[i * ns + j] * n[ch.indm[i * ns + j]];
+            vlogM = (tmp == sn) ? logsn : log(tmp);
+        }
+        const double* abe = ch.abe + 3 * i;
+        double vlogk1 = abe[0] + abe[1] * logT - abe[2] * Tinv;
+        double vlogk2 = 0.0;
+        if (rs1 >= 4) vlogk1 = vlogk1 + vlogM;
+        const int* ind = ch.indnu + 6 * i;
+        const int nreac = ch.numnu[2 * i], nprod = ch.numnu[2 * i + 1];
+        if (rs0 == 0) {
+            const double* cabe = ch.cabe + 3 * i;
+            if (rs1 == 1 || rs1 == 5) {
+                vlogk2 = cabe[0] + cabe[1] * logT - cabe[2] * Tinv;
+                if (rs1 == 5) vlogk2 = vlogk2 + vlogM;
+            } else {
+                if (rs1 == 2 || rs1 == 3) {
+                    const double logk0 = cabe[0] + cabe[1] * logT - cabe[2] * Tinv;
+                    const double logkinf = vlogk1;
+                    const double log_Pr = logk0 - logkinf + vlogM;
+                    const double Pr = exp(log_Pr);
+                    vlogk1 = logkinf + log(Pr / (1.0 + Pr));
+                    if (rs1 == 3) {
+                        const double* tr = ch.troe + 4 * i;
+                        const double aa = tr[0];
+                        const double logFcent =
+                            log10((1.0 - aa) * exp(-T * tr[1]) + aa * exp(-T * tr[2]) + exp(-Tinv * tr[3]));
+                        const double cc = -0.4 - 0.67 * logFcent;
+                        const double nn = 0.75 - 1.27 * logFcent;
+                        const double logPrc = log_Pr * loge210 + cc;
+                        const double a = logPrc / (nn - dd * logPrc);
+                        const double logF = 1.0 / (1.0 + a * a) * logFcent;
+                        vlogk1 = vlogk1 + logF / loge210;
+                    }
+                }
+                double t1 = 0.0;
+                for (int k = 0; k < nreac; ++k) t1 = t1 - vmu0rt[ind[k]];
+                for (int k = 0; k < nprod; ++k) t1 = t1 + vmu0rt[ind[3 + k]];
+                vlogk2 = vlogk1 - ch.snu[i] * logPRT + t1;
+            }
+        }
+        double r = exp(vlogk1);
+        for (int k = 0; k < nreac; ++k) r = r * n[ind[k]];
+        for (int k = 0; k < nreac; ++k) dndtm[ind[k]] = dndtm[ind[k]] - r;
+        for (int k = 0; k < nprod; ++k) dndtp[ind[3 + k]] = dndtp[ind[3 + k]] + r;
+        if (rs0 == 0) {
+            r = exp(vlogk2);
+            for (int k = 0; k < nprod; ++k) r = r * n[ind[3 + k]];
+            for (int k = 0; k < nreac; ++k) dndtp[ind[k]] = dndtp[ind[k]] + r;
+            for (int k = 0; k < nprod; ++k) dndtm[ind[3 + k]] = dndtm[ind[3 + k]] - r;
+        }
+    }
+    double de = 0.0, cv = 0.0;
+    for (int j = 0; j < ns; ++j) {
+        de = de + vert[j] * (dndtp[j] + dndtm[j]);
+        cv = cv + vcvr[j] * n[j];
+    }
+    dndtp[ns] = fmax(-de * T / cv, 0.0);
+    dndtm[ns] = fmin(-de * T / cv, 0.0);
+}
+
+// Per-thread CHEMEQ2 state machine (sub_chem.f90:1714-1819).
+struct Ceq {
+    double y[kMaxSpecies + 1], y0[kMaxSpecies + 1];
+    double tt, tout, dt, ratio, counter;
+    int countersum, substeps;
+    bool fell_back;   // the implicit fallback took over (the reference calls DVODE here)
+    int rejects;      // consecutive rejected implicit substeps
+    long long evals;  // source-term evaluations
+};
+
+// Sum of production and destruction rates: dy/dt of the UV source terms.
+__device__ inline void dev_rates(const DevChem& ch, const double* y, double* f, double* tmp) {
+    dev_fex_var(ch, y, f, tmp);
+    for (int i = 0; i <= ch.ns; ++i) f[i] = f[i] + tmp[i];
+}
+
+// Weight of component i in the error norm: the CHEMEQ2 tolerance
+// y*rtol + rtol*1e-5 for the species (sub_chem.f90:1801), rtol*T for T.
+__device__ inline double be_weight(int i, int ns, double yi, double rtol) {
+    return i < ns ? fabs(yi) * rtol + rtol * 1e-5 : fabs(yi) * rtol;
+}
+
+// Dense LU with partial pivoting of the N x N row-major M; false if singular.
+__device__ inline bool lu_factor(double* M, int* piv, int N) {
+    for (int k = 0; k < N; ++k) {
+        int pk = k;
+        double best = fabs(M[k * N + k]);
+        for (int i = k + 1; i < N; ++i)
+            if (fabs(M[i * N + k]) > best) {
+                best = fabs(M[i * N + k]);
+                pk = i;
+            }
+        piv[k] = pk;
+        if (!(best > 0.0)) return false;
+        if (pk != k)
+            for (int j = 0; j < N; ++j) {
+                const double t = M[k * N + j];
+                M[k * N + j] = M[pk * N + j];
+                M[pk * N + j] = t;
+            }
+        const double inv = 1.0 / M[k * N + k];
+        for (int i = k + 1; i < N; ++i) {
+            const double l = M[i * N + k] * inv;
+            M[i * N + k] = l;
+            for (int j = k + 1; j < N; ++j) M[i * N + j] = M[i * N + j] - l * M[k * N + j];
+        }
+    }
+    return true;
+}
+
+// Solves L U x = P b in place (factors and row swaps of lu_factor).
+__device__ inline void lu_solve(const double* M, const int* piv, int N, double* b) {
+    for (int k = 0; k < N; ++k) {
+        const int pk = piv[k];
+        if (pk != k) {
+            const double t = b[k];
+            b[k] = b[pk];
+            b[pk] = t;
+        }
+    }
+    for (int i = 1; i < N; ++i)
+        for (int j = 0; j < i; ++j) b[i] = b[i] - M[i * N + j] * b[j];
+    for (int i = N - 1; i >= 0; --i) {
+        for (int j = i + 1; j < N; ++j) b[i] = b[i] - M[i * N + j] * b[j];
+        b[i] = b[i] / M[i * N + i];
+    }
+}
+
+// Implicit fallback substep: the two-stage Rosenbrock method ROS2 of Verwer,
+// Spee, Blom and Hundsdorfer (SIAM J. Sci. Comput. 20, 1999), L-stable, order
+// 2, with gamma = 1 + 1/sqrt(2):
+//     (I - gamma h J) k1 = f(y0),   (I - gamma h J) k2 = f(y0 + h k1) - 2 k1,
+//     y = y0 + 3/2 h k1 + 1/2 h k2,  error estimate |h/2 (k1 + k2)| (vs. y0 + h k1),
+// J a forward-difference Jacobian of the rates at y0, step factor
+// 0.8/sqrt(err) in [0.2, 2].  Used for the rest of an interval once CHEMEQ2
+// has made 10 attempts (where sub_chem.f90:1755-1775 calls DVODE).
+// Returns 1 when the interval is done, 0 to continue, <0 error.
+__device__ inline int be_attempt(const DevChem& ch, Ceq& s, double rtol, int max_substeps, long long& attempts) {
+    const int ns = ch.ns, N = ns + 1;
+    const double gam = 1.7071067811865475;  // 1 + 1/sqrt(2)
+    double f0[kMaxSpecies + 1], f[kMaxSpecies + 1], tmp[kMaxSpecies + 1], k1[kMaxSpecies + 1], k2[kMaxSpecies + 1];
+    double M[(kMaxSpecies + 1) * (kMaxSpecies + 1)];
+    int piv[kMaxSpecies + 1];
+    ++attempts;
+    double h = s.dt;
+    if (s.tout - s.tt < h) h = s.tout - s.tt;
+    dev_rates(ch, s.y0, f0, tmp);
+    // M = I - gamma h J,  J(:, j) = (f(y0 + e_j dj) - f0) / dj
+    for (int j = 0; j < N; ++j) {
+        for (int i = 0; i < N; ++i) s.y[i] = s.y0[i];
+        const double dj = 1.4901161193847656e-8 * fmax(fabs(s.y0[j]), j < ns ? 1e-10 : 1.0);
+        s.y[j] = s.y0[j] + dj;
+        dev_rates(ch, s.y, f, tmp);
+        for (int i = 0; i < N; ++i) M[i * N + j] = (i == j ? 1.0 : 0.0) - gam * h * (f[i] - f0[i]) / dj;
+    }
+    double err = 1e300;
+    if (lu_factor(M, piv, N)) {
+        for (int i = 0; i < N; ++i) k1[i] = f0[i];
+        lu_solve(M, piv, N, k1);
+        for (int i = 0; i < N; ++i) s.y[i] = s.y0[i] + h * k1[i];
+        dev_rates(ch, s.y, f, tmp);
+        for (int i = 0; i < N; ++i) k2[i] = f[i] - 2.0 * k1[i];
+        lu_solve(M, piv, N, k2);
+        err = 0.0;
+        for (int i = 0; i < N; ++i) {
+            s.y[i] = s.y0[i] + 1.5 * h * k1[i] + 0.5 * h * k2[i];
+            const double e = fabs(0.5 * h * (k1[i] + k2[i])) / be_weight(i, ns, s.y[i], rtol);
+            err = (e > err || e != e) ? e : err;
+        }
+    }
+    s.evals += N + 2;
+    if (!(err <= 1.0)) {
+        s.dt = h * (err == err && err < 1e300 ? fmax(0.2, 0.8 / sqrt(err)) : 0.25);
+        if (++s.rejects > 30) return -SCFD_E_CHEM;
+        return 0;
+    }
+    s.rejects = 0;
+    s.tt = s.tt + h;
+    for (int i = 0; i < N; ++i) s.y0[i] = s.y[i];
+    s.dt = h * fmin(2.0, fmax(0.2, 0.8 / sqrt(fmax(err, 1e-10))));
+    if (s.tout <= s.tt) return 1;
+    if (++s.substeps > max_substeps) return -SCFD_E_CHEM;
+    return 0;
+}
+
+// One attempt; returns 1 when the interval is done, 0 to continue, <0 error.
+// After 10 CHEMEQ2 attempts in an interval the rest of it goes to be_attempt.
+__device__ inline int ceq_attempt(const DevChem& ch, Ceq& s, double rtol, int max_substeps, long long& attempts) {
+    if (s.fell_back) return be_attempt(ch, s, rtol, max_substeps, attempts);
+    const int ns = ch.ns;
+    double yp[kMaxSpecies + 1], p[kMaxSpecies + 1], q[kMaxSpecies + 1], p0[kMaxSpecies + 1], q0[kMaxSpecies + 1];
+    for (int i = 0; i <= ns; ++i) s.y[i] = s.y0[i];
+    s.countersum += 1;
+    if (s.countersum > 10) {
+        s.fell_back = true;
+        s.rejects = 0;
+        return be_attempt(ch, s, rtol, max_substeps, attempts);
+    }
+    ++attempts;
+    s.evals += 2;
+    const double dt = s.dt;
+    dev_fex_var(ch, s.y, q0, p0);
+    for (int i = 0; i < ns; ++i) {
+        p0[i] = -p0[i] / (s.y[i] + 1e-300);
+        const double var = p0[i] * dt, var2 = var * var, var3 = var * var2;
+        const double alp = (180.0 + 60.0 * var + 11.0 * var2 + var3) / (360.0 + 60.0 * var + 12.0 * var2 + var3);
+        yp[i] = s.y0[i] + dt * (q0[i] - p0[i] * s.y0[i]) / (1.0 + alp * p0[i] * dt);
+    }
+    yp[ns] = s.y0[ns] + dt * (q0[ns] + p0[ns]);
+    double ratio = 1e300;
+    dev_fex_var(ch, yp, q, p);
+    for (int i = 0; i < ns; ++i) {
+        p[i] = -p[i] / (yp[i] + 1e-300);
+        p[i] = 0.5 * (p0[i] + p[i]);
+        const double var = p[i] * dt, var2 = var * var, var3 = var * var2;
+        const double alp = (180.0 + 60.0 * var + 11.0 * var2 + var3) / (360.0 + 60.0 * var + 12.0 * var2 + var3);
+        q[i] = alp * q[i] + (1.0 - alp) * q0[i];
+        s.y[i] = s.y0[i] + dt * (q[i] - p[i] * s.y0[i]) / (1.0 + alp * p[i] * dt);
+        const double v2 = (s.y[i] * rtol + rtol * 1e-5) / fabs(s.y[i] - yp[i] + 1e-300);
+        ratio = (v2 < ratio || v2 != v2) ? v2 : ratio;  // a NaN ratio rejects the attempt
+    }
+    s.y[ns] = s.y0[ns] + 0.5 * dt * (q[ns] + p[ns] + q0[ns] + p0[ns]);
+    s.ratio = ratio;
+    if (1.0 < ratio) {
+        // accepted
+        s.tt = s.tt + dt;
+        if (s.tout <= s.tt) return 1;
+        s.dt = dt * sqrt(ratio);
+        if (++s.substeps > max_substeps) return -SCFD_E_CHEM;
+        for (int i = 0; i <= ns; ++i) s.y0[i] = s.y[i];
+        s.counter = 0.0;
+        if (s.tout - s.tt < s.dt) s.dt = s.tout - s.tt;
+        return 0;
+    }
+    s.counter = s.counter + 1.0;
+    s.dt = dt * sqrt(ratio) / s.counter;
+    if (s.counter > 10.0) return -SCFD_E_CHEM;
+    return 0;
+}
+
+}  // namespace scfd

@@ -11,6 +11,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "chem_tables.h"
 #include "scfd_internal.h"
 
 using namespace scfd;
@@ -628,49 +629,7 @@ int scfd_commit(scfd_ctx* c) {
     const bool mixed = c->d.precision == SCFD_PREC_MIXED;
     const bool impl = c->d.scheme != SCFD_SCHEME_EULER;
     // chemistry tables, compact
-    std::vector<double> ccoeff, ctc, cinv, cmw, cmen, cabe, ccabe, ctroe, ctrange, ctrans, cwc1, cwc2;
-    std::vector<int> crs, cind, cnum, csnu, cex, cnm, cim, ctr, cns;
-    int ns = 0, nr = 0, nt = 0;
-    if (c->have_chem) {
-        const scfd_chem& h = c->chem;
-        ns = h.ns; nr = h.nr; nt = h.nt;
-        for (int k = 0; k < ns; ++k) {
-            for (int s = 0; s < 2; ++s)
-                for (int i = 0; i < 7; ++i) ccoeff.push_back(h.coeff[k][s][i]);
-            ctc.push_back(h.tthre[k][2]);
-            cinv.push_back(1.0 / h.mws[k]);
-            cmw.push_back(h.mws[k]);
-        }
-        for (int i = 0; i < nr; ++i) {
-            crs.push_back(h.rstate[i][0]); crs.push_back(h.rstate[i][1]);
-            for (int s = 0; s < 2; ++s)
-                for (int k = 0; k < 3; ++k) cind.push_back(h.indnu[i][s][k]);
-            cnum.push_back(h.numnu[i][0]); cnum.push_back(h.numnu[i][1]);
-            csnu.push_back(h.snu[i]);
-            cex.push_back(h.exist_m[i]);
-            cnm.push_back(h.numm[i]);
-            for (int k = 0; k < ns; ++k) {
-                cim.push_back(h.indm[i][k]);
-                cmen.push_back(h.men[i][k]);
-            }
-            for (int k = 0; k < 3; ++k) { cabe.push_back(h.abe[i][k]); ccabe.push_back(h.cabe[i][k]); }
-            for (int k = 0; k < 4; ++k) ctroe.push_back(h.troe[i][k]);
-        }
-        for (int i = 0; i < nt; ++i) {
-            ctr.push_back(h.tr2th[i]);
-            cns.push_back(h.num_sctn_trans[i]);
-            for (int l = 0; l < 5; ++l) {
-                for (int m = 0; m < 2; ++m) ctrange.push_back(h.trange_trans[i][l][m]);
-                for (int m = 0; m < 4; ++m) ctrans.push_back(h.trans[i][l][m]);
-            }
-        }
-        for (int i = 0; i < nt; ++i)
-            for (int j = 0; j < nt; ++j) {
-                const double mi = h.mws[h.tr2th[i]], mj = h.mws[h.tr2th[j]];
-                cwc1.push_back(std::pow(mj / mi, 0.25));
-                cwc2.push_back(std::sqrt(2.0 * mj / (mi + mj)));
-            }
-    }
+    const ChemTables tabs = c->have_chem ? ChemTables(c->chem) : ChemTables();
     const int nrec = 64 * c->np;
     // strip records for the TMA-streamed sweeps
     const size_t blk3 = impl ? sweep3_record_elems(nY, mixed) : 0;
@@ -747,10 +706,7 @@ int scfd_commit(scfd_ctx* c) {
     bytes += need<int>(c->nsf + c->nsb) + need<int>(2) + need<double>(2 * c->nsb);
     bytes += need<GhostOp>(std::max(1, c->nops)) + need<double>(std::max<size_t>(1, c->bcs.size()) * c->valstride);
     bytes += need<unsigned long long>(1) + need<double>(nrec) + need<double>(1);
-    bytes += need<double>(ccoeff.size() + ctc.size() + cinv.size() + cmw.size() + cmen.size() + cabe.size() +
-                          ccabe.size() + ctroe.size() + ctrange.size() + ctrans.size() + cwc1.size() + cwc2.size() + 64);
-    bytes += need<int>(crs.size() + cind.size() + cnum.size() + csnu.size() + cex.size() + cnm.size() + cim.size() +
-                       ctr.size() + cns.size() + 64);
+    bytes += tabs.bytes();
     if (c->use_sw4)
         bytes += need<char>(rec_total4 * esz3) + need<long long>(rec_off4.size()) + need<int>(strips4.size()) +
                  need<int>(blks4.size()) + 2 * need<int>(tasksf4.size()) +
@@ -852,16 +808,6 @@ int scfd_commit(scfd_ctx* c) {
         w4.xstride = (long long)(c->nimax + 8) * qc4;
         CK(cudaStreamSynchronize(c->stream));
     }
-    auto upd = [&](const std::vector<double>& h) -> const double* {
-        double* d = carve<double>(p, std::max<size_t>(1, h.size()));
-        if (!h.empty()) cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
-        return d;
-    };
-    auto upi = [&](const std::vector<int>& h) -> const int* {
-        int* d = carve<int>(p, std::max<size_t>(1, h.size()));
-        if (!h.empty()) cudaMemcpyAsync(d, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
-        return d;
-    };
     if (p > c->arena + c->arena_bytes) return c->fail(SCFD_E_CUDA, "arena overflow");
     // geometry upload
     auto up = [&](double* d, const std::vector<double>& h) {
@@ -883,14 +829,7 @@ int scfd_commit(scfd_ctx* c) {
         CK(cudaStreamSynchronize(c->stream));
     }
     if (c->have_chem) {
-        DevChem& ch = v.chem;
-        ch.ns = ns; ch.nr = nr; ch.nt = nt;
-        ch.coeff = upd(ccoeff); ch.tcommon = upd(ctc); ch.inv_mw = upd(cinv); ch.mws = upd(cmw);
-        ch.rstate = upi(crs); ch.indnu = upi(cind); ch.numnu = upi(cnum); ch.snu = upi(csnu); ch.exist_m = upi(cex);
-        ch.numm = upi(cnm); ch.indm = upi(cim); ch.men = upd(cmen); ch.abe = upd(cabe); ch.cabe = upd(ccabe);
-        ch.troe = upd(ctroe); ch.tr2th = upi(ctr); ch.nsec = upi(cns); ch.trange = upd(ctrange); ch.trans = upd(ctrans);
-        ch.wc1 = upd(cwc1); ch.wc2 = upd(cwc2);
-        ch.rtol = c->chem.rtol;
+        CK(tabs.upload(v.chem, p, c->stream));
         CK(cudaStreamSynchronize(c->stream));
     }
     if (p > c->arena + c->arena_bytes) return c->fail(SCFD_E_CUDA, "arena overflow");

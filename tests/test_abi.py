@@ -16,7 +16,7 @@ HEADER = os.path.join(ROOT, "include", "scfd_b200.h")
 
 def declared():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"^int\s+scfd_(\w+)\s*\(", txt, flags=re.M)))
+    return sorted(set(re.findall(r"^(?:int|void\*)\s+scfd_(\w+)\s*\(", txt, flags=re.M)))
 
 
 def cuda_lib_path():
@@ -47,12 +47,14 @@ def test_oracle_exports_same_entry_points(orc_raw):
 
 def test_struct_sizes_match_c(tmp_path):
     src = tmp_path / "sz.c"
-    src.write_text('#include <stdio.h>\n#include "%s"\nint main(void){printf("%%zu %%zu %%zu %%zu\\n",'
-                   'sizeof(scfd_desc),sizeof(scfd_bc),sizeof(scfd_chem),sizeof(scfd_stats));return 0;}\n' % HEADER)
+    src.write_text('#include <stdio.h>\n#include "%s"\nint main(void){printf("%%zu %%zu %%zu %%zu %%zu\\n",'
+                   'sizeof(scfd_desc),sizeof(scfd_bc),sizeof(scfd_chem),sizeof(scfd_stats),'
+                   'sizeof(scfd_reactor_desc));return 0;}\n' % HEADER)
     exe = tmp_path / "sz"
     subprocess.check_call(["gcc", "-o", str(exe), str(src)])
     out = [int(v) for v in subprocess.check_output([str(exe)]).split()]
-    assert out == [C.sizeof(abi.Desc), C.sizeof(abi.BC), C.sizeof(abi.Chem), C.sizeof(abi.Stats)]
+    assert out == [C.sizeof(abi.Desc), C.sizeof(abi.BC), C.sizeof(abi.Chem), C.sizeof(abi.Stats),
+                   C.sizeof(abi.ReactorDesc)]
 
 
 def test_create_rejects_bad_descriptors_without_gpu():
