@@ -2,13 +2,16 @@
 """Benchmark of the per-step residual-and-implicit-update path on B200.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
-                    [--config reacting_step|flat_plate|sod] [--scale S]
+                    [--config reacting_step|flat_plate|sod|reactors] [--scale S]
 
 Metric: Mcell-iter/s (cells x inner iterations per second; for the explicit
 Euler configuration one step is one iteration), mixed (FP32 reconstruction,
 fluxes and sweeps) and plain FP64.  `value` is the mixed path with the state
 resident in HBM; `fp64_value` the plain path; `e2e` the same metric through the
 C ABI with host buffers copied in and the result copied out every step.
+
+--config reactors measures the batched 0-D reactors instead: reactors/s for
+one batch of 8192 H2/air reactors integrated to 2 ms (a step is one batch).
 
 One JSON line is printed by rank 0.  Under torchrun every rank runs its own
 replica of the workload on its own GPU (weak scaling, no data exchange) and
@@ -229,13 +232,148 @@ def l2_note(case):
     return "working set ~%.0f MB fits the 126 MB L2" % mb
 
 
+# ---------------------------------------------------------------------------
+# batched 0-D reactors (scfd_reactors_*)
+# ---------------------------------------------------------------------------
+REACTOR_N = 8192
+REACTOR_T_END = 2e-3
+REACTOR_DT_CALL = 1e-6
+
+
+def reactor_flops_per_eval(ns, nr):
+    """Algorithmic flops of one Fex_var evaluation (an estimate, the unit of the
+    reactors' FP64 roofline): NASA-7 thermo, 3 x 7 multiply-adds per species and
+    the T sums (~45 flops per species); per reaction the Arrhenius exponent,
+    concentration products and two exponentials counted at ~20 flops each (~60)."""
+    return 45 * ns + 60 * nr
+
+
+def reactor_workload():
+    return ("%d constant-volume H2/air 0-D reactors (T0 900-1600 K, p 1-20 atm, phi 0.3-3), reacting-step "
+            "mechanism (9 species, 19 seeded reactions), CHEMEQ2 calls every %g s to %g s" %
+            (REACTOR_N, REACTOR_DT_CALL, REACTOR_T_END))
+
+
+def cpu_reactors(cores, n=REACTOR_N):
+    from shared_cfd_b200.reactors import Reactors
+    so = os.path.join(ROOT, "oracle", "_build", "liborc.so")
+    if not os.path.exists(so):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    orc = abi.Bound(C.CDLL(so), "orc_")
+    _, ch, T0, v, _ = cases.reactor_batch(n)
+    with Reactors(ch, n, lib=orc) as r:
+        t0 = time.perf_counter()
+        out = r.run(T0, v, REACTOR_T_END, dt_call=REACTOR_DT_CALL)
+        dt = time.perf_counter() - t0
+    return n / dt, dt, out
+
+
+def run_reactors(args, rank, cores):
+    """One JSON line for the 0-D reactor batch (rank 0 only; the batch does not
+    shard across ranks in this benchmark)."""
+    unit = "reactors/s"
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        steps = max(1, args.steps)
+        t = 0.0
+        for _ in range(steps):
+            _, dt, _ = cpu_reactors(cores)
+            t += dt
+        val = REACTOR_N * steps / t
+        print(json.dumps({
+            "impl": "reference", "metric": "reactors/s (0-D, FP64)", "value": val, "unit": unit,
+            "n_gpus": args.gpus, "steps": steps, "warmup": 0, "ms_per_step": 1e3 * t / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": reactor_workload()},
+            "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port",
+                             "sample": "%d batch(es) of %d reactors on %d OpenMP threads (C++ FP64 restatement)"
+                                       % (steps, REACTOR_N, cores)},
+            "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
+    if rank != 0:
+        return 0
+    import torch
+    from shared_cfd_b200 import build
+    from shared_cfd_b200.reactors import Reactors
+    build.build()
+    m, ch, T0, v, _ = cases.reactor_batch(REACTOR_N)
+    r = Reactors(ch, REACTOR_N)
+    d = r.desc(REACTOR_N, REACTOR_T_END, dt_call=REACTOR_DT_CALL)
+    stream = torch.cuda.ExternalStream(r.stream(), device=0)
+    r.upload(T0, v)
+    for _ in range(max(1, args.warmup)):
+        r.launch(d)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as cs:
+        e0.record(stream)
+        for _ in range(args.steps):
+            r.launch(d)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    out = r.download(REACTOR_N)
+    launches = r.launch_count() * args.steps
+    value = REACTOR_N / (ms * 1e-3)
+    # end to end: host arrays in, results out, every batch
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r.run(T0, v, REACTOR_T_END, dt_call=REACTOR_DT_CALL)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    # one kernel launch per reactor, on a bounded sample (serial by construction)
+    ns_pl = 64
+    t0 = time.perf_counter()
+    r.run(T0[:ns_pl], v[:ns_pl], REACTOR_T_END, mode=abi.REACTOR_PER_LAUNCH, dt_call=REACTOR_DT_CALL)
+    pl_s = time.perf_counter() - t0
+    r.close()
+    evals = int(out["evals"].sum())
+    flops = evals * reactor_flops_per_eval(ch.ns, ch.nr)
+    ach = flops / (ms * 1e-3) / 1e9
+    line = {
+        "metric": "reactors/s (0-D, FP64)", "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": reactor_workload(), "reactors": REACTOR_N, "mode": "persistent work queue, CUDA graph",
+                   "l2": "state of all reactors (~1 MB) is L2-resident; the kernel is latency-bound"},
+        "e2e": {"value": REACTOR_N / e2e_s, "unit": unit,
+                "h2d_bytes_per_step": int(T0.nbytes + v.nbytes),
+                "d2h_bytes_per_step": int(T0.nbytes * 3 + v.nbytes + out["flags"].nbytes)},
+        "gpu_launches": launches, "clocks": cs.summary(),
+        "per_launch": {"value": ns_pl / pl_s, "unit": unit, "sample": "first %d reactors, one launch each" % ns_pl},
+        "roofline": {"bound": "fp64", "achieved": ach, "peak": 40000.0, "unit": "GFLOP/s", "frac": ach / 40000.0,
+                     "peak_source": "nominal B200 FP64 (not measured)", "traffic": None,
+                     "flops_per_eval": reactor_flops_per_eval(ch.ns, ch.nr), "evals_per_batch": evals},
+        "reactors": {"ignited": int(((out["flags"] & abi.REACTOR_IGNITED) > 0).sum()),
+                     "fell_back": int(((out["flags"] & abi.REACTOR_FELL_BACK) > 0).sum()),
+                     "failed": int(((out["flags"] & abi.REACTOR_FAILED) > 0).sum()),
+                     "evals_max": int(out["evals"].max()), "status": int(out["status"])},
+    }
+    if not args.no_cpu_baseline:
+        v_cpu, dt, ref = cpu_reactors(cores)
+        ign = (ref["flags"] & abi.REACTOR_IGNITED) > 0
+        line["cpu_baseline"] = {"value": v_cpu, "unit": unit, "cores": cores, "kind": "port",
+                                "sample": "the full batch (%.1f s) on %d OpenMP threads, C++ FP64 restatement"
+                                          % (dt, cores)}
+        line["accuracy_vs_cpu"] = {
+            "flags_differ": int((ref["flags"] != out["flags"]).sum()),
+            "t_ign_max_rel": float(np.max(np.abs(out["t_ign"][ign] - ref["t_ign"][ign]) / ref["t_ign"][ign]))
+            if ign.any() else None,
+            "T_end_max_rel": float(np.max(np.abs(out["T_end"] - ref["T_end"]) / ref["T_end"])),
+            "T_end_median_rel": float(np.median(np.abs(out["T_end"] - ref["T_end"]) / ref["T_end"]))}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="reacting_step", choices=["reacting_step", "flat_plate", "sod"])
+    ap.add_argument("--config", default="reacting_step", choices=["reacting_step", "flat_plate", "sod", "reactors"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -244,6 +382,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     cores = os.cpu_count() or 1
+
+    if args.config == "reactors":
+        return run_reactors(args, rank, cores)
 
     if args.impl == "reference":
         if rank != 0:

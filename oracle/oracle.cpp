@@ -567,13 +567,15 @@ void lu_solve(const double* M, const int* piv, int N, double* b) {
 // [0.2, 2].  y holds the accepted state at tt on entry and the state at tout
 // on return.  The same substeps as be_attempt of the CUDA path, in the same order.
 int implicit_rest(const scfd_chem& ch, double* y, double tt, double tout, double dt, double rtol,
-                  long long& attempts, int& substeps, int max_substeps, Ignition* ign, long long& evals) {
+                  long long& attempts, int& substeps, int max_substeps, Ignition* ign, long long& evals,
+                  double& h_carry) {
     const int ns = ch.ns, N = ns + 1;
     const double gam = 1.7071067811865475;
     double y0[SCFD_MAX_SPECIES + 1], f0[SCFD_MAX_SPECIES + 1], f[SCFD_MAX_SPECIES + 1], tmp[SCFD_MAX_SPECIES + 1],
         k1[SCFD_MAX_SPECIES + 1], k2[SCFD_MAX_SPECIES + 1], M[(SCFD_MAX_SPECIES + 1) * (SCFD_MAX_SPECIES + 1)];
     int piv[SCFD_MAX_SPECIES + 1];
     for (int i = 0; i < N; ++i) y0[i] = y[i];
+    if (h_carry > 0.0) dt = h_carry;  // warm start from the previous call's last step
     int rejects = 0;
     for (;;) {
         ++attempts;
@@ -612,6 +614,7 @@ int implicit_rest(const scfd_chem& ch, double* y, double tt, double tout, double
         tt = tt + h;
         for (int i = 0; i < N; ++i) y0[i] = y[i];
         dt = h * std::min(2.0, std::max(0.2, 0.8 / std::sqrt(std::max(err, 1e-10))));
+        h_carry = dt;
         if (ign) track_ignition(*ign, tt, y[ns]);
         if (tout <= tt) return 0;
         if (++substeps > max_substeps) return SCFD_E_CHEM;
@@ -622,9 +625,12 @@ int implicit_rest(const scfd_chem& ch, double* y, double tt, double tout, double
 // the ignition test runs after every accepted substep; `evals` counts the
 // source-term evaluations.
 int chemeq2(const scfd_chem& ch, double* y, double tt, double tout, double rtol, long long& attempts,
-            bool& fell_back, int max_substeps, Ignition* ign = nullptr, long long* evals = nullptr) {
+            bool& fell_back, int max_substeps, Ignition* ign = nullptr, long long* evals = nullptr,
+            double* h_carry = nullptr) {
     long long ev_local = 0;
     long long& ev = evals ? *evals : ev_local;
+    double hc_local = 0.0;
+    double& hc = h_carry ? *h_carry : hc_local;
     const int ns = ch.ns;
     double y0[SCFD_MAX_SPECIES + 1], yp[SCFD_MAX_SPECIES + 1], p[SCFD_MAX_SPECIES + 1], q[SCFD_MAX_SPECIES + 1],
         p0[SCFD_MAX_SPECIES + 1], q0[SCFD_MAX_SPECIES + 1];
@@ -644,7 +650,7 @@ int chemeq2(const scfd_chem& ch, double* y, double tt, double tout, double rtol,
             // implicit_rest (shared with the CUDA path), and the cell is counted.
             if (countersum > 10) {
                 fell_back = true;
-                return implicit_rest(ch, y, tt, tout, dt, rtol, attempts, substeps, max_substeps, ign, ev);
+                return implicit_rest(ch, y, tt, tout, dt, rtol, attempts, substeps, max_substeps, ign, ev, hc);
             }
             ++attempts;
             ev += 2;
@@ -1804,6 +1810,7 @@ int orc_reactors_launch(orc_reactors* r, const scfd_reactor_desc* d) {
         y[ns] = r->T0[k];
         Ignition g{r->T0[k], d->dT_ign, 0.0, r->T0[k], -1.0, false, 0.0};
         long long att = 0, ev = 0;
+        double hc = 0.0;  // Rosenbrock step carried from call to call
         bool fb = false, any_fb = false;
         int rc = 0;
         // successive reaction_chemeq2 calls over dt_call: moles floored at n_eps
@@ -1813,7 +1820,7 @@ int orc_reactors_launch(orc_reactors* r, const scfd_reactor_desc* d) {
             const double rest = d->t_end - tg;
             const double tout = (d->dt_call > 0.0 && d->dt_call < rest) ? d->dt_call : rest;
             g.t_off = tg;
-            rc = chemeq2(ch, y, 0.0, tout, ch.rtol, att, fb, maxsub, &g, &ev);
+            rc = chemeq2(ch, y, 0.0, tout, ch.rtol, att, fb, maxsub, &g, &ev, &hc);
             any_fb = any_fb || fb;
             if (rc) break;
             tg = tg + tout;

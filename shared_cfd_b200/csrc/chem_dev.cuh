@@ -9,93 +9,140 @@
 
 namespace scfd {
 
+// Per-evaluation constants of Fex_var (FJ.f90:301-453) at temperature T.
+struct FexPre {
+    double T, logT, Tinv, logPRT, sn, logsn;
+    double cmurt[7], chrt[7], ccpr[7];
+};
+
+__device__ inline void fex_pre(FexPre& f, double T, double sn) {
+    const double pst = 1.01325e6, Ru = 8.3144621e7;
+    f.T = T;
+    f.logT = log(T);
+    f.Tinv = 1.0 / T;
+    f.logPRT = log(pst / Ru) - f.logT;
+    f.sn = sn;
+    f.logsn = log(sn);
+    const double T2 = T * T, T3 = T2 * T, T4 = T3 * T;
+    const double cm[7] = {1.0 - f.logT, -T / 2.0, -T2 / 6.0, -T3 / 12.0, -T4 / 20.0, f.Tinv, -1.0};
+    const double ch[7] = {1.0, T / 2.0, T2 / 3.0, T3 / 4.0, T4 / 5.0, f.Tinv, 0.0};
+    const double cp[7] = {1.0, T, T2, T3, T4, 0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        f.cmurt[i] = cm[i];
+        f.chrt[i] = ch[i];
+        f.ccpr[i] = cp[i];
+    }
+}
+
+// mu0/RT, e/RT and cv/R of species j (NASA-7).
+__device__ inline void species_thermo(const DevChem& ch, int j, const FexPre& f, double& mu, double& e, double& cv) {
+    const double* cf = ch.coeff + (j * 2 + (f.T <= ch.tcommon[j] ? 0 : 1)) * 7;
+    double t1 = 0.0, t2 = -1.0, t3 = -1.0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        const double c = cf[i];
+        t1 = t1 + c * f.cmurt[i];
+        t2 = t2 + c * f.chrt[i];
+        t3 = t3 + c * f.ccpr[i];
+    }
+    mu = t1;
+    e = t2;
+    cv = t3;
+}
+
+// log of the third-body concentration of reaction i (reactions with exist_m).
+__device__ inline double third_body_logM(const DevChem& ch, int i, const double* n, const FexPre& f) {
+    const int ns = ch.ns;
+    double tmp = f.sn;
+    const int nm = ch.numm[i];
+    for (int j = 0; j < nm; ++j) tmp = tmp + ch.men[i * ns + j] * n[ch.indm[i * ns + j]];
+    return (tmp == f.sn) ? f.logsn : log(tmp);
+}
+
+// Forward and reverse rates of reaction i (rr = 0 for irreversible reactions);
+// vlogM is the third-body term in effect for it.
+__device__ inline void reaction_rates(const DevChem& ch, int i, const double* n, const FexPre& f, double vlogM,
+                                      const double* vmu0rt, double& rf, double& rr) {
+    const double loge210 = (double)0.43429448190325f;
+    const double dd = 0.14;
+    const int rs0 = ch.rstate[2 * i], rs1 = ch.rstate[2 * i + 1];
+    const double* abe = ch.abe + 3 * i;
+    double vlogk1 = abe[0] + abe[1] * f.logT - abe[2] * f.Tinv;
+    double vlogk2 = 0.0;
+    if (rs1 >= 4) vlogk1 = vlogk1 + vlogM;
+    const int* ind = ch.indnu + 6 * i;
+    const int nreac = ch.numnu[2 * i], nprod = ch.numnu[2 * i + 1];
+    if (rs0 == 0) {
+        const double* cabe = ch.cabe + 3 * i;
+        if (rs1 == 1 || rs1 == 5) {
+            vlogk2 = cabe[0] + cabe[1] * f.logT - cabe[2] * f.Tinv;
+            if (rs1 == 5) vlogk2 = vlogk2 + vlogM;
+        } else {
+            if (rs1 == 2 || rs1 == 3) {
+                const double logk0 = cabe[0] + cabe[1] * f.logT - cabe[2] * f.Tinv;
+                const double logkinf = vlogk1;
+                const double log_Pr = logk0 - logkinf + vlogM;
+                const double Pr = exp(log_Pr);
+                vlogk1 = logkinf + log(Pr / (1.0 + Pr));
+                if (rs1 == 3) {
+                    const double* tr = ch.troe + 4 * i;
+                    const double aa = tr[0];
+                    const double logFcent =
+                        log10((1.0 - aa) * exp(-f.T * tr[1]) + aa * exp(-f.T * tr[2]) + exp(-f.Tinv * tr[3]));
+                    const double cc = -0.4 - 0.67 * logFcent;
+                    const double nn = 0.75 - 1.27 * logFcent;
+                    const double logPrc = log_Pr * loge210 + cc;
+                    const double a = logPrc / (nn - dd * logPrc);
+                    const double logF = 1.0 / (1.0 + a * a) * logFcent;
+                    vlogk1 = vlogk1 + logF / loge210;
+                }
+            }
+            double t1 = 0.0;
+            for (int k = 0; k < nreac; ++k) t1 = t1 - vmu0rt[ind[k]];
+            for (int k = 0; k < nprod; ++k) t1 = t1 + vmu0rt[ind[3 + k]];
+            vlogk2 = vlogk1 - ch.snu[i] * f.logPRT + t1;
+        }
+    }
+    double r = exp(vlogk1);
+    for (int k = 0; k < nreac; ++k) r = r * n[ind[k]];
+    rf = r;
+    rr = 0.0;
+    if (rs0 == 0) {
+        r = exp(vlogk2);
+        for (int k = 0; k < nprod; ++k) r = r * n[ind[3 + k]];
+        rr = r;
+    }
+}
+
+// Fex_var (FJ.f90:301-453): production (dndtp >= 0) and destruction (dndtm <= 0)
+// rates of the species, and the positive / negative part of dT/dt at
+// constant volume.  As in the reference, a reaction with a third-body flag but
+// no third-body table uses the third-body term of the last reaction that had one.
 __device__ inline void dev_fex_var(const DevChem& ch, const double* n, double* dndtp, double* dndtm) {
     const int ns = ch.ns;
-    const double pst = 1.01325e6, Ru = 8.3144621e7;
-    const double loge210 = (double)0.43429448190325f;
-    const double T = n[ns];
-    const double logT = log(T), Tinv = 1.0 / T;
-    const double logPRT = log(pst / Ru) - logT;
     double sn = 0.0;
     for (int j = 0; j < ns; ++j) sn += n[j];
-    const double logsn = log(sn);
-    const double T2 = T * T, T3 = T2 * T, T4 = T3 * T;
-    const double cmurt[7] = {1.0 - logT, -T / 2.0, -T2 / 6.0, -T3 / 12.0, -T4 / 20.0, Tinv, -1.0};
-    const double chrt[7] = {1.0, T / 2.0, T2 / 3.0, T3 / 4.0, T4 / 5.0, Tinv, 0.0};
-    const double ccpr[7] = {1.0, T, T2, T3, T4, 0.0, 0.0};
+    FexPre f;
+    fex_pre(f, n[ns], sn);
     double vmu0rt[kMaxSpecies], vert[kMaxSpecies], vcvr[kMaxSpecies];
     for (int j = 0; j < ns; ++j) {
-        const double* cf = ch.coeff + (j * 2 + (T <= ch.tcommon[j] ? 0 : 1)) * 7;
-        double t1 = 0.0, t2 = -1.0, t3 = -1.0;
-#pragma unroll
-        for (int i = 0; i < 7; ++i) {
-            const double c = cf[i];
-            t1 = t1 + c * cmurt[i];
-            t2 = t2 + c * chrt[i];
-            t3 = t3 + c * ccpr[i];
-        }
-        vmu0rt[j] = t1;
-        vert[j] = t2;
-        vcvr[j] = t3;
+        species_thermo(ch, j, f, vmu0rt[j], vert[j], vcvr[j]);
         dndtp[j] = 0.0;
         dndtm[j] = 0.0;
     }
-    const double dd = 0.14;
     double vlogM = 0.0;
     for (int i = 0; i < ch.nr; ++i) {
-        const int rs0 = ch.rstate[2 * i], rs1 = ch.rstate[2 * i + 1];
-        if (ch.exist_m[i]) {
-            double tmp = sn;
-            const int nm = ch.numm[i];
-            for (int j = 0; j < nm; ++j) tmp = tmp + ch.men[i * ns + j] * n[ch.indm[i * ns + j]];
-            vlogM = (tmp == sn) ? logsn : log(tmp);
-        }
-        const double* abe = ch.abe + 3 * i;
-        double vlogk1 = abe[0] + abe[1] * logT - abe[2] * Tinv;
-        double vlogk2 = 0.0;
-        if (rs1 >= 4) vlogk1 = vlogk1 + vlogM;
+        if (ch.exist_m[i]) vlogM = third_body_logM(ch, i, n, f);
+        double rf, rr;
+        reaction_rates(ch, i, n, f, vlogM, vmu0rt, rf, rr);
         const int* ind = ch.indnu + 6 * i;
         const int nreac = ch.numnu[2 * i], nprod = ch.numnu[2 * i + 1];
-        if (rs0 == 0) {
-            const double* cabe = ch.cabe + 3 * i;
-            if (rs1 == 1 || rs1 == 5) {
-                vlogk2 = cabe[0] + cabe[1] * logT - cabe[2] * Tinv;
-                if (rs1 == 5) vlogk2 = vlogk2 + vlogM;
-            } else {
-                if (rs1 == 2 || rs1 == 3) {
-                    const double logk0 = cabe[0] + cabe[1] * logT - cabe[2] * Tinv;
-                    const double logkinf = vlogk1;
-                    const double log_Pr = logk0 - logkinf + vlogM;
-                    const double Pr = exp(log_Pr);
-                    vlogk1 = logkinf + log(Pr / (1.0 + Pr));
-                    if (rs1 == 3) {
-                        const double* tr = ch.troe + 4 * i;
-                        const double aa = tr[0];
-                        const double logFcent =
-                            log10((1.0 - aa) * exp(-T * tr[1]) + aa * exp(-T * tr[2]) + exp(-Tinv * tr[3]));
-                        const double cc = -0.4 - 0.67 * logFcent;
-                        const double nn = 0.75 - 1.27 * logFcent;
-                        const double logPrc = log_Pr * loge210 + cc;
-                        const double a = logPrc / (nn - dd * logPrc);
-                        const double logF = 1.0 / (1.0 + a * a) * logFcent;
-                        vlogk1 = vlogk1 + logF / loge210;
-                    }
-                }
-                double t1 = 0.0;
-                for (int k = 0; k < nreac; ++k) t1 = t1 - vmu0rt[ind[k]];
-                for (int k = 0; k < nprod; ++k) t1 = t1 + vmu0rt[ind[3 + k]];
-                vlogk2 = vlogk1 - ch.snu[i] * logPRT + t1;
-            }
-        }
-        double r = exp(vlogk1);
-        for (int k = 0; k < nreac; ++k) r = r * n[ind[k]];
-        for (int k = 0; k < nreac; ++k) dndtm[ind[k]] = dndtm[ind[k]] - r;
-        for (int k = 0; k < nprod; ++k) dndtp[ind[3 + k]] = dndtp[ind[3 + k]] + r;
-        if (rs0 == 0) {
-            r = exp(vlogk2);
-            for (int k = 0; k < nprod; ++k) r = r * n[ind[3 + k]];
-            for (int k = 0; k < nreac; ++k) dndtp[ind[k]] = dndtp[ind[k]] + r;
-            for (int k = 0; k < nprod; ++k) dndtm[ind[3 + k]] = dndtm[ind[3 + k]] - r;
+        for (int k = 0; k < nreac; ++k) dndtm[ind[k]] = dndtm[ind[k]] - rf;
+        for (int k = 0; k < nprod; ++k) dndtp[ind[3 + k]] = dndtp[ind[3 + k]] + rf;
+        if (ch.rstate[2 * i] == 0) {
+            for (int k = 0; k < nreac; ++k) dndtp[ind[k]] = dndtp[ind[k]] + rr;
+            for (int k = 0; k < nprod; ++k) dndtm[ind[3 + k]] = dndtm[ind[3 + k]] - rr;
         }
     }
     double de = 0.0, cv = 0.0;
@@ -103,8 +150,8 @@ __device__ inline void dev_fex_var(const DevChem& ch, const double* n, double* d
         de = de + vert[j] * (dndtp[j] + dndtm[j]);
         cv = cv + vcvr[j] * n[j];
     }
-    dndtp[ns] = fmax(-de * T / cv, 0.0);
-    dndtm[ns] = fmin(-de * T / cv, 0.0);
+    dndtp[ns] = fmax(-de * f.T / cv, 0.0);
+    dndtm[ns] = fmin(-de * f.T / cv, 0.0);
 }
 
 // Per-thread CHEMEQ2 state machine (sub_chem.f90:1714-1819).
@@ -115,6 +162,8 @@ struct Ceq {
     bool fell_back;   // the implicit fallback took over (the reference calls DVODE here)
     int rejects;      // consecutive rejected implicit substeps
     long long evals;  // source-term evaluations
+    double h_carry;   // step proposed by the last accepted implicit substep (0: none), kept
+                      // across the reaction_chemeq2 calls of one 0-D reactor
 };
 
 // Sum of production and destruction rates: dy/dt of the UV source terms.
@@ -227,6 +276,7 @@ __device__ inline int be_attempt(const DevChem& ch, Ceq& s, double rtol, int max
     s.tt = s.tt + h;
     for (int i = 0; i < N; ++i) s.y0[i] = s.y[i];
     s.dt = h * fmin(2.0, fmax(0.2, 0.8 / sqrt(fmax(err, 1e-10))));
+    s.h_carry = s.dt;
     if (s.tout <= s.tt) return 1;
     if (++s.substeps > max_substeps) return -SCFD_E_CHEM;
     return 0;
@@ -243,6 +293,7 @@ __device__ inline int ceq_attempt(const DevChem& ch, Ceq& s, double rtol, int ma
     if (s.countersum > 10) {
         s.fell_back = true;
         s.rejects = 0;
+        if (s.h_carry > 0.0) s.dt = s.h_carry;
         return be_attempt(ch, s, rtol, max_substeps, attempts);
     }
     ++attempts;

@@ -53,6 +53,7 @@ __device__ bool ceq_load(const View& v, long long c, Ceq& s) {
     s.fell_back = false;
     s.rejects = 0;
     s.evals = 0;
+    s.h_carry = 0.0;
     return true;
 }
 
