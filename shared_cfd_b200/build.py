@@ -14,7 +14,8 @@ SOURCES = ["scfd_api.cu", "k_thermo.cu", "k_bc.cu", "k_residual.cu", "k_lusgs.cu
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared", "-cudart", "shared",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fopenmp", "-shared",
+    "-cudart", "shared",
 ]
 
 

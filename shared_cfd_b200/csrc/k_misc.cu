@@ -2,6 +2,8 @@
 // check_convergence RMS (store/core/check_convergence.f90:17-28), step
 // bookkeeping of the device scalars, and the FP32 copy of the primitive
 // field used by the mixed-precision residual.
+#include <algorithm>
+
 #include "scfd_internal.h"
 
 namespace scfd {
@@ -138,6 +140,36 @@ __global__ void k_step_end(View v, double warn, double err) {
     const double rr = sc->res / sc->res1;
     if (rr > warn && rr > err && !sc->first_dual) atomicMax(&sc->status, SCFD_E_RESRATE);
     sc->first_dual = 0;
+}
+
+// Field transposes between the reference layout f(1:nk,-1:nimax+2,-1:njmax+2,Nplane)
+// (component fastest) and the structure-of-arrays cell slots: one thread per
+// reference cell; dir 0 scatters ref -> SoA, dir 1 gathers SoA -> ref (cells
+// beyond a smaller plane's ghost layers are written as zero).
+__global__ void k_ref_soa(Planes P, long long N, int nk, int IX, int JX, long long nref, const double* ref,
+                          double* soa, double* ref_out, int dir) {
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < nref;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % IX) - 1;
+        const long long r = idx / IX;
+        const int j = (int)(r % JX) - 1, p = (int)(r / JX);
+        const bool in = i <= P.ni[p] + 2 && j <= P.nj[p] + 2;
+        const long long c = in ? cidx(P, p, i, j) : 0;
+        if (dir == 0) {
+            if (in)
+                for (int k = 0; k < nk; ++k) soa[k * N + c] = ref[idx * nk + k];
+        } else {
+            for (int k = 0; k < nk; ++k) ref_out[idx * nk + k] = in ? soa[k * N + c] : 0.0;
+        }
+    }
+}
+
+int launch_ref_soa(const View& v, cudaStream_t s, int nk, int IX, int JX, const double* ref, double* soa,
+                   double* ref_out, int dir) {
+    const long long nref = (long long)IX * JX * v.P.np;
+    const int blocks = (int)std::min<long long>((nref + 255) / 256, 148LL * 16);
+    k_ref_soa<<<blocks, 256, 0, s>>>(v.P, v.ncell, nk, IX, JX, nref, ref, soa, ref_out, dir);
+    return 1;
 }
 
 int launch_step_end(const View& v, cudaStream_t s, double warn, double err) {

@@ -16,6 +16,9 @@
 
 using namespace scfd;
 
+// bytes of each pinned chunk of the host <-> device copies (two chunks per context)
+constexpr size_t kRingChunk = 32ull << 20;
+
 struct scfd_ctx {
     scfd_desc d{};
     std::string err;
@@ -59,8 +62,9 @@ struct scfd_ctx {
     double* d_rms_partial = nullptr;
     double* d_rms_out = nullptr;
     // pinned staging for transfers
-    double* h_stage = nullptr;
-    size_t stage_doubles = 0;
+    double* d_ref = nullptr;  // device staging of one field in the reference layout
+    void* h_ring[2] = {nullptr, nullptr};  // pinned chunks of the host <-> device copies
+    cudaEvent_t ring_ev[2] = {nullptr, nullptr};
     long long launches = 0;
     int cells_max = 0;
     // per-kernel timing
@@ -541,10 +545,13 @@ int scfd_create(const scfd_desc* d, scfd_ctx** out) {
 int scfd_destroy(scfd_ctx* c) {
     if (!c) return SCFD_E_ARG;
     if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (int b = 0; b < 2; ++b) {
+        if (c->h_ring[b]) cudaFreeHost(c->h_ring[b]);
+        if (c->ring_ev[b]) cudaEventDestroy(c->ring_ev[b]);
+    }
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     if (c->arena) cudaFree(c->arena);
     if (c->h_sc) cudaFreeHost(c->h_sc);
-    if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return 0;
@@ -707,6 +714,8 @@ int scfd_commit(scfd_ctx* c) {
     bytes += need<GhostOp>(std::max(1, c->nops)) + need<double>(std::max<size_t>(1, c->bcs.size()) * c->valstride);
     bytes += need<unsigned long long>(1) + need<double>(nrec) + need<double>(1);
     bytes += tabs.bytes();
+    const size_t nref = (size_t)(c->nimax + 4) * (c->njmax + 4) * c->np;
+    bytes += need<double>((size_t)std::max(std::max(W, D), nY) * nref);
     if (c->use_sw4)
         bytes += need<char>(rec_total4 * esz3) + need<long long>(rec_off4.size()) + need<int>(strips4.size()) +
                  need<int>(blks4.size()) + 2 * need<int>(tasksf4.size()) +
@@ -756,6 +765,11 @@ int scfd_commit(scfd_ctx* c) {
     c->d_counter = carve<unsigned long long>(p, 1);
     c->d_rms_partial = carve<double>(p, nrec);
     c->d_rms_out = carve<double>(p, 1);
+    c->d_ref = carve<double>(p, (size_t)std::max(std::max(W, D), nY) * nref);
+    for (int b = 0; b < 2; ++b) {
+        CK(cudaMallocHost(&c->h_ring[b], kRingChunk));
+        CK(cudaEventCreateWithFlags(&c->ring_ev[b], cudaEventDisableTiming));
+    }
     if (c->use_sw3) {
         Sweep3& w3 = c->sw3;
         w3.rec = carve<char>(p, rec_total * esz3);
@@ -834,8 +848,6 @@ int scfd_commit(scfd_ctx* c) {
     }
     if (p > c->arena + c->arena_bytes) return c->fail(SCFD_E_CUDA, "arena overflow");
     CK(cudaMallocHost(&c->h_sc, sizeof(DevScalars)));
-    c->stage_doubles = (size_t)std::max(W, D) * (c->nimax + 4) * (c->njmax + 4) * c->np;
-    CK(cudaMallocHost(&c->h_stage, c->stage_doubles * sizeof(double)));
     CK(cudaStreamSynchronize(c->stream));
     (void)impl;
     c->committed = true;
@@ -843,51 +855,80 @@ int scfd_commit(scfd_ctx* c) {
 }
 
 // reference layout f(k, -1:nimax+2, -1:njmax+2, plane) <-> SoA slots
-static void ref_to_soa(const scfd_ctx* c, const double* ref, int nk, double* soa) {
-    const int IX = c->nimax + 4, JX = c->njmax + 4;
-    const long long N = c->ncell;
-    for (int p = 0; p < c->np; ++p)
-        for (int j = -1; j <= c->P.nj[p] + 2; ++j)
-            for (int i = -1; i <= c->P.ni[p] + 2; ++i) {
-                const double* src = ref + (size_t)nk * ((i + 1) + (size_t)IX * ((j + 1) + (size_t)JX * p));
-                const long long cc = cidx(c->P, p, i, j);
-                for (int k = 0; k < nk; ++k) soa[k * N + cc] = src[k];
-            }
-}
-static void soa_to_ref(const scfd_ctx* c, const double* soa, int nk, double* ref) {
-    const int IX = c->nimax + 4, JX = c->njmax + 4;
-    const long long N = c->ncell;
-    for (int p = 0; p < c->np; ++p)
-        for (int j = -1; j <= c->P.nj[p] + 2; ++j)
-            for (int i = -1; i <= c->P.ni[p] + 2; ++i) {
-                double* dst = ref + (size_t)nk * ((i + 1) + (size_t)IX * ((j + 1) + (size_t)JX * p));
-                const long long cc = cidx(c->P, p, i, j);
-                for (int k = 0; k < nk; ++k) dst[k] = soa[k * N + cc];
-            }
+// Host <-> device copies of the caller's (pageable) arrays go through two
+// pinned chunks: the host threads copy one chunk while the DMA engine moves the
+// other.
+
+static void par_copy(void* dst, const void* src, size_t bytes) {
+    const size_t piece = 1ull << 20;
+    const long long n = (long long)((bytes + piece - 1) / piece);
+#pragma omp parallel for schedule(static)
+    for (long long k = 0; k < n; ++k) {
+        const size_t off = (size_t)k * piece, len = std::min(piece, bytes - off);
+        std::memcpy(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off, len);
+    }
 }
 
+static int h2d_pipelined(scfd_ctx* c, void* dev, const void* host, size_t bytes) {
+    size_t off = 0;
+    for (int k = 0; off < bytes; ++k) {
+        const int b = k & 1;
+        const size_t len = std::min(kRingChunk, bytes - off);
+        CK(cudaEventSynchronize(c->ring_ev[b]));  // the copy that last read chunk b has finished
+        par_copy(c->h_ring[b], static_cast<const char*>(host) + off, len);
+        CK(cudaMemcpyAsync(static_cast<char*>(dev) + off, c->h_ring[b], len, cudaMemcpyHostToDevice, c->stream));
+        CK(cudaEventRecord(c->ring_ev[b], c->stream));
+        off += len;
+    }
+    return 0;
+}
+
+static int d2h_pipelined(scfd_ctx* c, void* host, const void* dev, size_t bytes) {
+    size_t off = 0, prev_off = 0, prev_len = 0;
+    int k = 0;
+    for (; off < bytes; ++k) {
+        const int b = k & 1;
+        const size_t len = std::min(kRingChunk, bytes - off);
+        CK(cudaMemcpyAsync(c->h_ring[b], static_cast<const char*>(dev) + off, len, cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaEventRecord(c->ring_ev[b], c->stream));
+        if (k > 0) {  // the previous chunk has landed: copy it out while this one moves
+            CK(cudaEventSynchronize(c->ring_ev[b ^ 1]));
+            par_copy(static_cast<char*>(host) + prev_off, c->h_ring[b ^ 1], prev_len);
+        }
+        prev_off = off;
+        prev_len = len;
+        off += len;
+    }
+    if (k > 0) {
+        CK(cudaEventSynchronize(c->ring_ev[(k - 1) & 1]));
+        par_copy(static_cast<char*>(host) + prev_off, c->h_ring[(k - 1) & 1], prev_len);
+    }
+    return 0;
+}
+
+// The reference-layout arrays cross PCIe unchanged into a device staging
+// buffer (d_ref) and are transposed to / from the cell slots on the GPU.
 static int upload_field(scfd_ctx* c, const double* ref, int nk, double* dev) {
-    std::fill(c->h_stage, c->h_stage + (size_t)nk * c->ncell, 0.0);
-    ref_to_soa(c, ref, nk, c->h_stage);
-    CK(cudaMemcpyAsync(dev, c->h_stage, sizeof(double) * nk * c->ncell, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
+    const int IX = c->nimax + 4, JX = c->njmax + 4;
+    const size_t bytes = sizeof(double) * (size_t)nk * IX * JX * c->np;
+    int st = h2d_pipelined(c, c->d_ref, ref, bytes);
+    if (st) return st;
+    launch_ref_soa(c->v, c->stream, nk, IX, JX, c->d_ref, dev, nullptr, 0);
+    CK(cudaGetLastError());
     return 0;
 }
 static int download_field(scfd_ctx* c, const double* dev, int nk, double* ref) {
-    CK(cudaMemcpyAsync(c->h_stage, dev, sizeof(double) * nk * c->ncell, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    soa_to_ref(c, c->h_stage, nk, ref);
-    return 0;
+    const int IX = c->nimax + 4, JX = c->njmax + 4;
+    const size_t bytes = sizeof(double) * (size_t)nk * IX * JX * c->np;
+    launch_ref_soa(c->v, c->stream, nk, IX, JX, nullptr, const_cast<double*>(dev), c->d_ref, 1);
+    CK(cudaGetLastError());
+    return d2h_pipelined(c, ref, c->d_ref, bytes);
 }
 
 int scfd_upload(scfd_ctx* c, const double* q, const double* w, const double* vhi, double tt) {
     if (!c || !q || !w) return SCFD_E_ARG;
     if (!c->committed) return c->fail(SCFD_E_STATE, "upload before commit");
-    if (c->stage_doubles < (size_t)std::max(c->W, c->D) * c->ncell) {
-        cudaFreeHost(c->h_stage);
-        c->stage_doubles = (size_t)std::max(c->W, c->D) * c->ncell;
-        CK(cudaMallocHost(&c->h_stage, c->stage_doubles * sizeof(double)));
-    }
     int st;
     if ((st = upload_field(c, q, c->D, c->v.q))) return st;
     if ((st = upload_field(c, w, c->W, c->v.w))) return st;

@@ -165,6 +165,9 @@ int launch_rms(const View& v, cudaStream_t s, double* partial, double* out);
 int launch_copy(double* dst, const double* src, long long n, cudaStream_t s);
 int launch_scalar_begin(const View& v, cudaStream_t s);
 int launch_to_f32(const View& v, cudaStream_t s);
+// reference layout <-> SoA slots (dir 0: ref -> soa, dir 1: soa -> ref_out)
+int launch_ref_soa(const View& v, cudaStream_t s, int nk, int IX, int JX, const double* ref, double* soa,
+                   double* ref_out, int dir);
 
 // residual modes
 enum { RES_EULER = 0, RES_LUSGS = 1, RES_NR = 2 };
