@@ -226,6 +226,55 @@ enum {
 int  scfd_profile(scfd_ctx* ctx, int enable);
 int  scfd_kernel_stats(scfd_ctx* ctx, int kind, double* total_ms, int64_t* launches, char* name, int namelen);
 
+/* ---- block-sharded step over several processes (one GPU each) -------------
+ * Replaces the MPI decomposition of the reference: the cross-rank halo copies
+ * of set_BC (store/cond/no-nV/condition.tail.f90:71-330, MPI_Isend/Recv of w
+ * and vhi) and the reductions of dt_grbl (store/time_step/global/set_dt.f90:40),
+ * of omega and the inner residual (store/time_scheme/NR/q2d/time_NR_viscous.f90:
+ * 87-90, here reduced to every rank: quirk Q4 off) and of the RMS
+ * (store/core/check_convergence.f90:33).  Every rank holds the whole case, all
+ * planes, and updates only the planes `owner` gives it.  LU-SGS needs no
+ * exchange (Dq = 0 at plane edges).
+ *
+ * The library communicates nothing itself.  A sharded physical step is a
+ * sequence of scfd_dstep calls; each enqueues the work up to the next point
+ * where the ranks must agree and returns a request that the caller fulfils on
+ * req->buf (device memory of the context's stream on the CUDA library, host
+ * memory on the CPU restatement) before the next call:
+ *   SCFD_DREQ_REDUCE  all-reduce SUM of buf[0..nsum) and MIN of
+ *                     buf[nsum..nsum+nmin); a status travels as -status in a
+ *                     MIN slot, so the MIN is the worst status
+ *   SCFD_DREQ_HALO    all-gather: buf is nranks segments of seg doubles; this
+ *                     rank's segment is filled, the others must hold their
+ *                     ranks' segments on return
+ *   SCFD_DREQ_DONE    the step is complete; the return value is the step's
+ *                     status (the same on every rank) and stats is filled
+ * Every rank issues the same requests in the same order, whatever the status.
+ * Work on the CUDA library stays on the context's stream (scfd_get_stream);
+ * the caller orders its collectives on that stream.  In stats,
+ * chem_attempts and chem_fallback_cells count this rank's cells; dt, time,
+ * res, res1 and omega are global.  scfd_rms returns this rank's share,
+ * sqrt(sum over owned cells)/(all cells): the global RMS is the square root of
+ * the sum of the ranks' squares.  scfd_download returns all planes, of which
+ * only the owned ones are current. */
+#define SCFD_MAX_RANKS 64
+enum { SCFD_DREQ_DONE = 0, SCFD_DREQ_REDUCE = 1, SCFD_DREQ_HALO = 2 };
+typedef struct scfd_dreq {
+    int32_t kind;     /* SCFD_DREQ_* */
+    int32_t nsum;     /* REDUCE: leading slots summed */
+    int32_t nmin;     /* REDUCE: following slots minimised */
+    int32_t nranks;   /* HALO: segments */
+    int64_t seg;      /* HALO: doubles per segment */
+    double* buf;
+} scfd_dreq;
+/* Before scfd_commit: owner[p] (0-based rank, p = 0..nplane-1) of every plane,
+ * the number of ranks and this rank.  A context without a partition owns every
+ * plane and may also step through scfd_dstep (as rank 0 of 1). */
+int  scfd_set_partition(scfd_ctx* ctx, const int32_t* owner, int nranks, int rank);
+/* Begins or continues a sharded physical step.  scfd_step and scfd_run refuse
+ * a context partitioned over more than one rank (SCFD_E_STATE). */
+int  scfd_dstep(scfd_ctx* ctx, int step, scfd_dreq* req, scfd_stats* stats);
+
 /* ---- batched constant-volume 0-D reactors ---------------------------------
  * Replaces per-reactor calls of reaction_chemeq2 / reaction_one_steps
  * (store/therm_lib/chemkin/core/sub_chem.f90:1684-1713 and 1396-1504).  Each

@@ -23,6 +23,7 @@
 #include "../include/scfd_b200.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -104,6 +105,17 @@ struct orc_ctx {
     double res1 = 0.0, res = 0.0, omega_last = 0.0;
     long long chem_attempts = 0, chem_fallback = 0;
     int status = SCFD_OK;
+    // block sharding (scfd_set_partition): planes owned by this rank, the
+    // cells each rank exports to the others' ghost copies, the exchange buffers
+    // and the position of a staged step (scfd_dstep)
+    int nranks = 1, rank = 0;
+    std::vector<int> owner;
+    std::vector<std::vector<std::array<int, 3>>> exports;  // per rank: (i, j, plane)
+    long long seg = 0;
+    std::vector<double> halo, red;
+    int ds_stage = 0, ds_j = 0, ds_status = 0;
+    long long ds_att0 = 0, ds_fb0 = 0;
+    bool own(int p) const { return nranks <= 1 || owner[p - 1] == rank; }  // p 1-based
 
     int fail(int code, const std::string& m) {
         err = m;
@@ -697,6 +709,7 @@ int chemeq2(const scfd_chem& ch, double* y, double tt, double tout, double rtol,
 void set_w(orc_ctx& c) {  // store/core/scheme.f90:1-29
     const int nY = c.nY;
     for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
 #pragma omp parallel for
         for (int j = 1; j <= c.nj[p - 1]; ++j)
             for (int i = 1; i <= c.ni[p - 1]; ++i) {
@@ -716,6 +729,7 @@ int set_thermo_prop(orc_ctx& c) {
     if (c.d.thermo == SCFD_THERMO_IDEAL) {  // store/therm_lib/ideal/thermal_model.raw.f90:7-33
         const double kg = c.d.kappa, Rg = c.d.rgas, nu = c.d.nu_gas;
         for (int p = 1; p <= c.np; ++p) {
+            if (!c.own(p)) continue;
 #pragma omp parallel for
             for (int j = 1; j <= c.nj[p - 1]; ++j)
                 for (int i = 1; i <= c.ni[p - 1]; ++i) {
@@ -741,6 +755,7 @@ int set_thermo_prop(orc_ctx& c) {
     // chemkin: flow/reactive/thermal_model.f90:13-42 (cold flow is identical with ns_tocalc = ns)
     int st = 0;
     for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
 #pragma omp parallel for reduction(max : st)
         for (int j = 1; j <= c.nj[p - 1]; ++j)
             for (int i = 1; i <= c.ni[p - 1]; ++i) {
@@ -765,14 +780,14 @@ int set_thermo_prop(orc_ctx& c) {
     return st;
 }
 
-void set_dt(orc_ctx& c) {  // store/time_step/{global,local}/set_dt.f90
-    if (c.d.dt_mode == SCFD_DT_FIXED) {
-        c.dt_grbl = c.d.dt_fixed;
-        c.tt = c.tt + c.dt_grbl;
-        return;
-    }
+// store/time_step/{global,local}/set_dt.f90, in two parts: set_dt_cells fills
+// dt_mat of the owned planes and returns their smallest value, set_dt_apply
+// sets dt_grbl and the time from the (global) minimum.
+double set_dt_cells(orc_ctx& c) {
     double tmp = 1e300;
+    if (c.d.dt_mode == SCFD_DT_FIXED) return tmp;
     for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
 #pragma omp parallel for reduction(min : tmp)
         for (int j = 1; j <= c.nj[p - 1]; ++j)
             for (int i = 1; i <= c.ni[p - 1]; ++i) {
@@ -791,11 +806,20 @@ void set_dt(orc_ctx& c) {  // store/time_step/{global,local}/set_dt.f90
                 if (tmp > c.dt_mat(i, j, p)) tmp = c.dt_mat(i, j, p);
             }
     }
-    if (c.d.dt_mode == SCFD_DT_GLOBAL) {
+    return tmp;
+}
+
+void set_dt_apply(orc_ctx& c, double tmp) {
+    if (c.d.dt_mode == SCFD_DT_FIXED) {
+        c.dt_grbl = c.d.dt_fixed;
+        c.tt = c.tt + c.dt_grbl;
+    } else if (c.d.dt_mode == SCFD_DT_GLOBAL) {
         c.dt_grbl = tmp;
         c.tt = c.tt + c.dt_grbl;
     }
 }
+
+void set_dt(orc_ctx& c) { set_dt_apply(c, set_dt_cells(c)); }
 
 int proceed_reaction(orc_ctx& c) {  // flow/reactive/thermal_model.f90:45-73 + reaction_chemeq2 1684-1713
     const int ns = c.ch.ns;
@@ -803,6 +827,7 @@ int proceed_reaction(orc_ctx& c) {  // flow/reactive/thermal_model.f90:45-73 + r
     long long att = 0, fb = 0;
     const int maxsub = c.d.chem_max_substeps > 0 ? c.d.chem_max_substeps : 1000000;
     for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
 #pragma omp parallel for reduction(max : st) reduction(+ : att, fb) schedule(dynamic, 16)
         for (int j = 1; j <= c.nj[p - 1]; ++j)
             for (int i = 1; i <= c.ni[p - 1]; ++i) {
@@ -833,11 +858,15 @@ int proceed_reaction(orc_ctx& c) {  // flow/reactive/thermal_model.f90:45-73 + r
 // set_BC: section_exchange (store/cond/no-nV/condition.tail.f90:2-70), the
 // boundary descriptors in place of the user loops, set_corners (331-356).
 void copy_cell(orc_ctx& c, int id, int jd, int pd, int is, int js, int ps) {
+    if (!c.own(pd)) return;
     for (int k = 1; k <= c.W; ++k) c.w(k, id, jd, pd) = c.w(k, is, js, ps);
     for (int k = 1; k <= c.nY; ++k) c.vhi(k, id, jd, pd) = c.vhi(k, is, js, ps);
 }
 
-void section_exchange(orc_ctx& c) {
+// The copies of section_exchange in the reference's order, as
+// f(dst i, j, plane, src i, j, plane).
+template <typename F>
+void for_each_halo_copy(const orc_ctx& c, F copy_cell) {
     for (size_t n = 0; n < c.cut.size() / 11; ++n) {
         const int32_t* r = &c.cut[n * 11];
         int geo = r[0], width = r[1], order = r[2], p1 = r[3], c1 = r[4], s1 = r[5], pm1 = r[6], p2 = r[7],
@@ -846,36 +875,41 @@ void section_exchange(orc_ctx& c) {
             int a = s1 + inc, b = s2 + inc * order;
             switch (geo) {
                 case 1:  // i-i
-                    copy_cell(c, c1 + pm1, a, p1, c2, b, p2);
-                    copy_cell(c, c1 + pm1 * 2, a, p1, c2 - pm2, b, p2);
-                    copy_cell(c, c2 + pm2, b, p2, c1, a, p1);
-                    copy_cell(c, c2 + pm2 * 2, b, p2, c1 - pm1, a, p1);
+                    copy_cell(c1 + pm1, a, p1, c2, b, p2);
+                    copy_cell(c1 + pm1 * 2, a, p1, c2 - pm2, b, p2);
+                    copy_cell(c2 + pm2, b, p2, c1, a, p1);
+                    copy_cell(c2 + pm2 * 2, b, p2, c1 - pm1, a, p1);
                     break;
                 case 2:  // i-j
-                    copy_cell(c, c1 + pm1, a, p1, b, c2, p2);
-                    copy_cell(c, c1 + pm1 * 2, a, p1, b, c2 - pm2, p2);
-                    copy_cell(c, b, c2 + pm2, p2, c1, a, p1);
-                    copy_cell(c, b, c2 + pm2 * 2, p2, c1 - pm1, a, p1);
+                    copy_cell(c1 + pm1, a, p1, b, c2, p2);
+                    copy_cell(c1 + pm1 * 2, a, p1, b, c2 - pm2, p2);
+                    copy_cell(b, c2 + pm2, p2, c1, a, p1);
+                    copy_cell(b, c2 + pm2 * 2, p2, c1 - pm1, a, p1);
                     break;
                 case 3:  // j-i
-                    copy_cell(c, a, c1 + pm1, p1, c2, b, p2);
-                    copy_cell(c, a, c1 + pm1 * 2, p1, c2 - pm2, b, p2);
-                    copy_cell(c, c2 + pm2, b, p2, a, c1, p1);
-                    copy_cell(c, c2 + pm2 * 2, b, p2, a, c1 - pm1, p1);
+                    copy_cell(a, c1 + pm1, p1, c2, b, p2);
+                    copy_cell(a, c1 + pm1 * 2, p1, c2 - pm2, b, p2);
+                    copy_cell(c2 + pm2, b, p2, a, c1, p1);
+                    copy_cell(c2 + pm2 * 2, b, p2, a, c1 - pm1, p1);
                     break;
                 case 4:  // j-j
-                    copy_cell(c, a, c1 + pm1, p1, b, c2, p2);
-                    copy_cell(c, a, c1 + pm1 * 2, p1, b, c2 - pm2, p2);
-                    copy_cell(c, b, c2 + pm2, p2, a, c1, p1);
-                    copy_cell(c, b, c2 + pm2 * 2, p2, a, c1 - pm1, p1);
+                    copy_cell(a, c1 + pm1, p1, b, c2, p2);
+                    copy_cell(a, c1 + pm1 * 2, p1, b, c2 - pm2, p2);
+                    copy_cell(b, c2 + pm2, p2, a, c1, p1);
+                    copy_cell(b, c2 + pm2 * 2, p2, a, c1 - pm1, p1);
                     break;
             }
         }
     }
 }
 
+void section_exchange(orc_ctx& c) {
+    for_each_halo_copy(c, [&](int id, int jd, int pd, int is, int js, int ps) { copy_cell(c, id, jd, pd, is, js, ps); });
+}
+
 void apply_bc(orc_ctx& c, const scfd_bc& b) {
     const int p = b.plane, ni = c.ni[p - 1], nj = c.nj[p - 1];
+    if (!c.own(p)) return;
     const int W = c.W, nY = c.nY;
     for (int s = b.first; s <= b.last; ++s) {
         int ib, jb, i1, j1, i2, j2;
@@ -930,7 +964,7 @@ void apply_bc(orc_ctx& c, const scfd_bc& b) {
 
 void set_corners(orc_ctx& c) {  // condition.tail.f90:331-356
     for (int p = 1; p <= c.np; ++p)
-        for (int pi = -1; pi <= 1; pi += 2) {
+        for (int pi = -1; pi <= 1 && c.own(p); pi += 2) {
             int i = pi < 0 ? 1 : c.ni[p - 1];
             for (int pj = -1; pj <= 1; pj += 2) {
                 int j = pj < 0 ? 1 : c.nj[p - 1];
@@ -960,6 +994,7 @@ void set_HV(orc_ctx& c) {
     const double eps = 1e-300;
     const double phi = c.d.recon == SCFD_RECON_MUSCL ? c.d.phi_mus : 0.0, km = c.d.k_mus;
     for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
         int ni = c.ni[p - 1], nj = c.nj[p - 1];
         FArr dui, dli, duj, dlj;
         dui.init({{1, W}, {0, ni + 1}, {1, nj}});
@@ -1045,6 +1080,7 @@ void slau_face(const orc_ctx& c, const double* wHl, const double* wHr, const dou
 void set_TG(orc_ctx& c) {  // store/core/scheme.f90:31-259
     const int W = c.W, D = c.D;
     for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
         int ni = c.ni[p - 1], nj = c.nj[p - 1];
 #pragma omp parallel for
         for (int j = 1; j <= nj; ++j)
@@ -1077,6 +1113,7 @@ void set_TGv(orc_ctx& c) {
     }
     const double Sc = c.d.schmidt, Pr = c.d.prandtl;
     for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
         int ni = c.ni[p - 1], nj = c.nj[p - 1];
         FArr Tdeg;
         Tdeg.init({{0, ni + 1}, {0, nj + 1}});
@@ -1191,7 +1228,7 @@ void set_TGv(orc_ctx& c) {
 void set_Sq(orc_ctx& c) {  // store/dim/q2d/Sq.f90:1-18 (2d: init_Sq zeros)
     if (c.d.dim != SCFD_DIM_Q2D) return;
     for (int p = 1; p <= c.np; ++p)
-        for (int j = 1; j <= c.nj[p - 1]; ++j)
+        for (int j = 1; j <= c.nj[p - 1] && c.own(p); ++j)
             for (int i = 1; i <= c.ni[p - 1]; ++i) {
                 for (int k = 1; k <= c.D; ++k) c.Sq(k, i, j, p) = 0.0;
                 c.Sq(c.nY + 2, i, j, p) = c.w(4, i, j, p);
@@ -1208,6 +1245,7 @@ inline double rhs_k(orc_ctx& c, int k, int i, int j, int p) {  // e.g. time_lusg
 
 void calc_next_step_euler(orc_ctx& c) {  // store/time_scheme/euler/time_euler_viscous.raw.f90:1-23
     for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
 #pragma omp parallel for
         for (int j = 1; j <= c.nj[p - 1]; ++j)
             for (int i = 1; i <= c.ni[p - 1]; ++i) {
@@ -1225,6 +1263,7 @@ void set_ABpm(orc_ctx& c) {
     const bool nr = c.d.scheme == SCFD_SCHEME_NR;
     const bool q2d = c.d.dim == SCFD_DIM_Q2D;
     for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
 #pragma omp parallel for
         for (int j = 1; j <= c.nj[p - 1]; ++j)
             for (int i = 1; i <= c.ni[p - 1]; ++i) {
@@ -1298,7 +1337,8 @@ void set_ABpm(orc_ctx& c) {
 }
 
 void set_dqdt(orc_ctx& c) {  // NR/q2d/sch_NR.raw.f90:151-180
-    for (int p = 1; p <= c.np; ++p)
+    for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
 #pragma omp parallel for
         for (int j = 1; j <= c.nj[p - 1]; ++j)
             for (int i = 1; i <= c.ni[p - 1]; ++i) {
@@ -1310,19 +1350,23 @@ void set_dqdt(orc_ctx& c) {  // NR/q2d/sch_NR.raw.f90:151-180
                         c.dqdt(k, i, j, p) = (3.0 * c.q(k, i, j, p) - 4.0 * c.qp(k, i, j, p) + c.qpp(k, i, j, p)) / (2.0 * dtl);
                 }
             }
+    }
 }
 
 // calc_next_step_implicit: LU-SGS/{2d,q2d}/time_lusgs_viscous.f90 and
-// NR/{2d,q2d}/time_NR_viscous.f90:1-109.  Returns 0 or SCFD_E_OMEGA.
-int calc_next_step_implicit(orc_ctx& c, int step_internal) {
+// NR/{2d,q2d}/time_NR_viscous.f90:1-109, in two parts: lusgs_sweeps (the
+// sweeps over the owned planes; LU-SGS also updates q there) returns the
+// plane-local residual and omega candidate, nr_apply relaxes q with the
+// (global) omega.  Returns 0 or SCFD_E_OMEGA.
+void lusgs_sweeps(orc_ctx& c, double& res_out, double& omega_out) {
     const int nY = c.nY, D = c.D;
     const bool nr = c.d.scheme == SCFD_SCHEME_NR;
     const bool q2d = c.d.dim == SCFD_DIM_Q2D;
     auto& Dq = c.Dq;
     double omega = 1e300;
     double res = 0.0;
-    bool omega_fail = false;
     for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
         int ni = c.ni[p - 1], nj = c.nj[p - 1];
 #pragma omp parallel for
         for (int j = 1; j <= nj; ++j)
@@ -1366,7 +1410,7 @@ int calc_next_step_implicit(orc_ctx& c, int step_internal) {
             for (int k = 1; k <= D; ++k) Dq(k, i, nj + 1, p) = 0.0;
         for (int sm = ni + nj; sm >= 2; --sm) {
             int ilo = std::max(1, sm - nj), ihi = std::min(sm - 1, ni);
-#pragma omp parallel for reduction(min : omega) reduction(+ : res) reduction(|| : omega_fail)
+#pragma omp parallel for reduction(min : omega) reduction(+ : res)
             for (int i = ilo; i <= ihi; ++i) {
                 int j = sm - i;
                 double dqs[SCFD_MAX_SPECIES + 3];
@@ -1382,10 +1426,7 @@ int calc_next_step_implicit(orc_ctx& c, int step_internal) {
                 if (nr) {
                     res = res + sq(Dq(nY + 3, i, j, p));
                     for (int k = 1; k <= nY; ++k)
-                        if (Dq(k, i, j, p) < 0.0) {
-                            omega = std::min(omega, -c.q(k, i, j, p) / Dq(k, i, j, p) * c.d.dq_max);
-                            if (omega < c.d.omega_min) omega_fail = true;
-                        }
+                        if (Dq(k, i, j, p) < 0.0) omega = std::min(omega, -c.q(k, i, j, p) / Dq(k, i, j, p) * c.d.dq_max);
                 }
             }
         }
@@ -1396,18 +1437,34 @@ int calc_next_step_implicit(orc_ctx& c, int step_internal) {
                     for (int k = 1; k <= D; ++k) c.q(k, i, j, p) = c.q(k, i, j, p) + Dq(k, i, j, p);
         }
     }
-    if (!nr) return 0;
-    if (omega_fail) return SCFD_E_OMEGA;
+    res_out = res;
+    omega_out = omega;
+}
+
+// The omega test, residual bookkeeping and q += omega*Dq of
+// time_NR_viscous.f90:75-108.  omega is the smallest candidate (the running
+// minimum of the reference falls below omega_min exactly when it does).
+int nr_apply(orc_ctx& c, int step_internal, double res, double omega) {
+    if (omega < c.d.omega_min) return SCFD_E_OMEGA;
     if (step_internal == 1) c.res1 = res;
     c.res = res;
     omega = std::min(c.d.omega_max, omega);
     c.omega_last = omega;
-    for (int p = 1; p <= c.np; ++p)
+    for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
 #pragma omp parallel for
         for (int j = 1; j <= c.nj[p - 1]; ++j)
             for (int i = 1; i <= c.ni[p - 1]; ++i)
-                for (int k = 1; k <= D; ++k) c.q(k, i, j, p) = c.q(k, i, j, p) + omega * Dq(k, i, j, p);
+                for (int k = 1; k <= c.D; ++k) c.q(k, i, j, p) = c.q(k, i, j, p) + omega * c.Dq(k, i, j, p);
+    }
     return 0;
+}
+
+int calc_next_step_implicit(orc_ctx& c, int step_internal) {
+    double res, omega;
+    lusgs_sweeps(c, res, omega);
+    if (c.d.scheme != SCFD_SCHEME_NR) return 0;
+    return nr_apply(c, step_internal, res, omega);
 }
 
 void copy_arr(FArr& dst, const FArr& src) { dst.v = src.v; }
@@ -1499,6 +1556,176 @@ int step_body(orc_ctx& c, scfd_stats* st) {
         }
     }
     return s;
+}
+
+// ---------------------------------------------------------------------------
+// Block sharding: each rank updates the planes it owns; the ghost copies of
+// section_exchange whose source lies on another rank's plane read the values
+// that rank exported (in place of MPI_COMMUNICATIONS_*, condition.tail.f90:
+// 71-330), and dt, omega and the residual are reduced over the ranks.
+// ---------------------------------------------------------------------------
+void build_exports(orc_ctx& c) {
+    c.exports.assign(c.nranks, {});
+    for_each_halo_copy(c, [&](int, int, int pd, int is, int js, int ps) {
+        const int q = c.owner[ps - 1];
+        if (c.owner[pd - 1] != q) c.exports[q].push_back({ps, js, is});
+    });
+    size_t mx = 0;
+    for (auto& e : c.exports) {
+        std::sort(e.begin(), e.end());
+        e.erase(std::unique(e.begin(), e.end()), e.end());
+        mx = std::max(mx, e.size());
+    }
+    c.seg = (long long)mx * (c.W + c.nY);
+    c.halo.assign((size_t)std::max(1LL, c.seg * c.nranks), 0.0);
+}
+
+// this rank's segment: component-major, halo[rank*seg + k*n + t]
+void halo_pack(orc_ctx& c) {
+    const auto& e = c.exports[c.rank];
+    const size_t n = e.size();
+    double* out = c.halo.data() + (size_t)c.rank * c.seg;
+    for (size_t t = 0; t < n; ++t) {
+        const int p = e[t][0], j = e[t][1], i = e[t][2];
+        for (int k = 1; k <= c.W; ++k) out[(k - 1) * n + t] = c.w(k, i, j, p);
+        for (int k = 1; k <= c.nY; ++k) out[(c.W + k - 1) * n + t] = c.vhi(k, i, j, p);
+    }
+}
+
+void halo_unpack(orc_ctx& c) {
+    for (int q = 0; q < c.nranks; ++q) {
+        if (q == c.rank) continue;
+        const auto& e = c.exports[q];
+        const size_t n = e.size();
+        const double* in = c.halo.data() + (size_t)q * c.seg;
+        for (size_t t = 0; t < n; ++t) {
+            const int p = e[t][0], j = e[t][1], i = e[t][2];
+            for (int k = 1; k <= c.W; ++k) c.w(k, i, j, p) = in[(k - 1) * n + t];
+            for (int k = 1; k <= c.nY; ++k) c.vhi(k, i, j, p) = in[(c.W + k - 1) * n + t];
+        }
+    }
+}
+
+enum { DS_BEGIN = 0, DS_AFTER_DT, DS_INNER, DS_AFTER_HALO_NR, DS_AFTER_RES, DS_AFTER_HALO, DS_AFTER_STATUS };
+
+// The staged physical step of scfd_dstep: step_body with its reductions and
+// the halo copies turned into requests.  A status seen on any rank becomes the
+// step's status at the next reduction, where every rank stops together.
+int dstep(orc_ctx& c, scfd_dreq* req, scfd_stats* st) {
+    const bool nr = c.d.scheme == SCFD_SCHEME_NR;
+    const bool reactive = c.d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
+    auto keep = [&](int s) { c.ds_status = std::max(c.ds_status, s); };
+    auto reduce = [&](int nsum, int nmin, int next) {
+        req->kind = SCFD_DREQ_REDUCE;
+        req->nsum = nsum;
+        req->nmin = nmin;
+        req->buf = c.red.data();
+        c.ds_stage = next;
+        return 0;
+    };
+    auto exchange = [&](int next) {
+        halo_pack(c);
+        req->kind = SCFD_DREQ_HALO;
+        req->nranks = c.nranks;
+        req->seg = c.seg;
+        req->buf = c.halo.data();
+        c.ds_stage = next;
+        return 0;
+    };
+    auto finish = [&]() {
+        if (st) {
+            std::memset(st, 0, sizeof(*st));
+            st->dt_grbl = c.dt_grbl;
+            st->tt = c.tt;
+            st->res = c.res;
+            st->res1 = c.res1;
+            st->omega = c.omega_last;
+            st->chem_attempts = c.chem_attempts - c.ds_att0;
+            st->chem_fallback_cells = c.chem_fallback - c.ds_fb0;
+            st->status = c.ds_status;
+            st->inner_iters = nr ? c.ds_j - (c.ds_stage == DS_INNER ? 1 : 0) : 0;
+            st->res_warn = c.ds_stage == DS_INNER && nr && c.res / c.res1 > c.d.res_rate_warn ? 1 : 0;
+        }
+        req->kind = SCFD_DREQ_DONE;
+        req->buf = nullptr;
+        c.ds_stage = DS_BEGIN;
+        return c.ds_status;
+    };
+    for (;;) {
+        switch (c.ds_stage) {
+            case DS_BEGIN:
+                c.ds_status = 0;
+                c.ds_j = 0;
+                c.ds_att0 = c.chem_attempts;
+                c.ds_fb0 = c.chem_fallback;
+                if (!nr && !reactive) copy_arr(c.qp, c.q);
+                keep(part_primitive(c));
+                c.red[0] = set_dt_cells(c);
+                c.red[1] = -(double)c.ds_status;
+                return reduce(0, 2, DS_AFTER_DT);
+            case DS_AFTER_DT:
+                set_dt_apply(c, c.red[0]);
+                keep((int)-c.red[1]);
+                if (c.ds_status) return finish();
+                if (reactive) keep(proceed_reaction(c));
+                if (nr) {
+                    copy_arr(c.qpp, c.qp);
+                    copy_arr(c.qp, c.q);
+                    c.ds_j = 1;
+                    c.ds_stage = DS_INNER;
+                    continue;
+                }
+                if (reactive) {
+                    copy_arr(c.qp, c.q);
+                    keep(part_primitive(c));
+                }
+                return exchange(DS_AFTER_HALO);
+            case DS_INNER:
+                if (c.ds_j >= c.d.num_internal_loop) {
+                    // check_internal_loop_convergence, sch_NR.raw.f90:222-237
+                    if (c.res / c.res1 > c.d.res_rate_warn && c.res / c.res1 > c.d.res_rate_err && !c.first_dual)
+                        keep(SCFD_E_RESRATE);
+                    const int s = finish();
+                    c.first_dual = false;
+                    return s;
+                }
+                keep(part_primitive(c));
+                return exchange(DS_AFTER_HALO_NR);
+            case DS_AFTER_HALO_NR: {
+                halo_unpack(c);
+                part_main(c);
+                set_ABpm(c);
+                set_dqdt(c);
+                double res, om;
+                lusgs_sweeps(c, res, om);
+                c.red[0] = res;
+                c.red[1] = om;
+                c.red[2] = -(double)c.ds_status;
+                return reduce(1, 2, DS_AFTER_RES);
+            }
+            case DS_AFTER_RES:
+                keep((int)-c.red[2]);
+                if (!c.ds_status) keep(nr_apply(c, c.ds_j, c.red[0], c.red[1]));
+                if (c.ds_status) return finish();
+                ++c.ds_j;
+                c.ds_stage = DS_INNER;
+                continue;
+            case DS_AFTER_HALO:
+                halo_unpack(c);
+                part_main(c);
+                if (c.d.scheme == SCFD_SCHEME_EULER) {
+                    calc_next_step_euler(c);
+                } else {
+                    set_ABpm(c);
+                    calc_next_step_implicit(c, 1);
+                }
+                c.red[0] = -(double)c.ds_status;
+                return reduce(0, 1, DS_AFTER_STATUS);
+            default:  // DS_AFTER_STATUS
+                keep((int)-c.red[0]);
+                return finish();
+        }
+    }
 }
 
 // reference layout copy helpers: (k, -1:nimax+2, -1:njmax+2, plane)
@@ -1636,8 +1863,30 @@ int orc_commit(orc_ctx* c) {
         if (!c->geo_set[p]) return c->fail(SCFD_E_STATE, "geometry of a plane not set");
     if (c->d.thermo != SCFD_THERMO_IDEAL && !c->have_chem) return c->fail(SCFD_E_STATE, "chem tables not set");
     init_geometry(*c);
+    if (c->nranks > 1) build_exports(*c);
+    c->red.assign(4, 0.0);
     c->committed = true;
     return 0;
+}
+
+int orc_set_partition(orc_ctx* c, const int32_t* owner, int nranks, int rank) {
+    if (!c || !owner || nranks < 1 || nranks > SCFD_MAX_RANKS || rank < 0 || rank >= nranks) return SCFD_E_ARG;
+    if (c->committed) return c->fail(SCFD_E_STATE, "partition after commit");
+    for (int p = 0; p < c->np; ++p)
+        if (owner[p] < 0 || owner[p] >= nranks) return c->fail(SCFD_E_ARG, "plane owner out of range");
+    c->owner.assign(owner, owner + c->np);
+    c->nranks = nranks;
+    c->rank = rank;
+    return 0;
+}
+
+int orc_dstep(orc_ctx* c, int stepno, scfd_dreq* req, scfd_stats* st) {
+    if (!c || !req) return SCFD_E_ARG;
+    req->kind = SCFD_DREQ_DONE;
+    req->buf = nullptr;
+    if (!c->committed) return c->fail(SCFD_E_STATE, "dstep before commit");
+    (void)stepno;
+    return dstep(*c, req, st);
 }
 
 int orc_upload(orc_ctx* c, const double* q, const double* w, const double* vhi, double tt) {
@@ -1664,11 +1913,13 @@ int orc_prepare(orc_ctx* c, int stepno) {
 
 int orc_step(orc_ctx* c, int stepno, scfd_stats* st) {
     if (!c || !c->committed) return SCFD_E_STATE;
+    if (c->nranks > 1) return c->fail(SCFD_E_STATE, "partitioned context: step through dstep");
     return step(*c, stepno, st);
 }
 
 int orc_run(orc_ctx* c, int stepno, int nsteps, scfd_stats* st) {
     if (!c || !c->committed) return SCFD_E_STATE;
+    if (c->nranks > 1) return c->fail(SCFD_E_STATE, "partitioned context: step through dstep");
     for (int n = 0; n < nsteps; ++n) {
         int s = step(*c, stepno + n, st);
         if (s) return s;
@@ -1680,7 +1931,7 @@ int orc_rms(orc_ctx* c, double* rms) {  // store/core/check_convergence.f90:17-3
     if (!c || !rms) return SCFD_E_ARG;
     double tmp = 0.0, smc = 0.0;
     for (int p = 1; p <= c->np; ++p) {
-        for (int j = 1; j <= c->nj[p - 1]; ++j)
+        for (int j = 1; j <= c->nj[p - 1] && c->own(p); ++j)
             for (int i = 1; i <= c->ni[p - 1]; ++i) tmp = tmp + sq(c->q(c->nY + 3, i, j, p) - c->qp(c->nY + 3, i, j, p));
         smc = smc + (double)(c->ni[p - 1] * c->nj[p - 1]);
     }

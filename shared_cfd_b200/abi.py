@@ -115,6 +115,22 @@ class Stats(C.Structure):
     ]
 
 
+MAX_RANKS = 64
+DREQ_DONE, DREQ_REDUCE, DREQ_HALO = 0, 1, 2
+
+
+class DReq(C.Structure):
+    """scfd_dreq: what the caller must communicate before the next scfd_dstep."""
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("nsum", C.c_int32),
+        ("nmin", C.c_int32),
+        ("nranks", C.c_int32),
+        ("seg", C.c_int64),
+        ("buf", C.c_void_p),
+    ]
+
+
 REACTOR_QUEUE, REACTOR_PER_LAUNCH = 0, 1
 REACTOR_IGNITED, REACTOR_FELL_BACK, REACTOR_FAILED = 1, 2, 4
 
@@ -157,6 +173,8 @@ SIGNATURES = {
     "launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "profile": (C.c_int, [_P, C.c_int]),
     "kernel_stats": (C.c_int, [_P, C.c_int, _D, C.POINTER(C.c_int64), C.c_char_p, C.c_int]),
+    "set_partition": (C.c_int, [_P, C.POINTER(C.c_int32), C.c_int, C.c_int]),
+    "dstep": (C.c_int, [_P, C.c_int, C.POINTER(DReq), C.POINTER(Stats)]),
     "reactors_create": (C.c_int, [C.POINTER(Chem), C.c_int, C.POINTER(_P)]),
     "reactors_destroy": (C.c_int, [_P]),
     "reactors_upload": (C.c_int, [_P, C.c_int, _D, _D]),

@@ -57,8 +57,8 @@ __global__ void k_ghost(View v, const GhostOp* ops, int nops, const double* bcva
 
 __global__ void k_corners(View v) {
     const int t = threadIdx.x;
-    const int p = t >> 2;
-    if (p >= v.P.np) return;
+    if ((t >> 2) >= v.P.nact) return;
+    const int p = v.P.act[t >> 2];
     const int pi = (t & 1) ? 1 : -1, pj = (t & 2) ? 1 : -1;
     const int i = pi < 0 ? 1 : v.P.ni[p];
     const int j = pj < 0 ? 1 : v.P.nj[p];
@@ -77,7 +77,8 @@ int launch_ghosts(const View& v, cudaStream_t s, const GhostOp* ops, int nops, c
         k_ghost<<<(nops + 127) / 128, 128, 0, s>>>(v, ops, nops, bcval, valstride);
         ++n;
     }
-    k_corners<<<1, 4 * v.P.np, 0, s>>>(v);
+    if (v.P.nact == 0) return n;
+    k_corners<<<1, 4 * v.P.nact, 0, s>>>(v);
     return n + 1;
 }
 

@@ -20,8 +20,9 @@
 namespace scfd {
 
 __device__ __forceinline__ long long cell_of(const View& v, long long k, int& pl) {
-    // k enumerates interior cells plane by plane
-    for (int p = 0; p < v.P.np; ++p) {
+    // k enumerates the interior cells of the updated planes, plane by plane
+    for (int a = 0; a < v.P.nact; ++a) {
+        const int p = v.P.act[a];
         const long long n = (long long)v.P.ni[p] * v.P.nj[p];
         if (k < n) {
             pl = p;
@@ -105,7 +106,8 @@ __global__ void __launch_bounds__(128) k_chem(View v, long long ncells, unsigned
 
 int launch_chem_impl(const View& v, cudaStream_t s, int max_substeps, unsigned long long* counter, int nsm) {
     long long n = 0;
-    for (int p = 0; p < v.P.np; ++p) n += (long long)v.P.ni[p] * v.P.nj[p];
+    for (int a = 0; a < v.P.nact; ++a) n += (long long)v.P.ni[v.P.act[a]] * v.P.nj[v.P.act[a]];
+    if (n == 0) return 0;
     cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
     // persistent grid: a few CTAs per SM, capped by the work
     long long blocks = (long long)nsm * 8;

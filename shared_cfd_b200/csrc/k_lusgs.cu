@@ -307,7 +307,7 @@ __global__ void k_nr_update(View v, const double* partials, int nstrips, int inn
     __syncthreads();
     if (v.sc->status == SCFD_E_OMEGA) return;
     const double om = s_omega;
-    const int p = blockIdx.y;
+    const int p = v.P.act[blockIdx.y];
     const int ni = v.P.ni[p], nj = v.P.nj[p];
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= ni * nj) return;
@@ -319,8 +319,12 @@ __global__ void k_nr_update(View v, const double* partials, int nstrips, int inn
 
 int launch_nr_update(const View& v, cudaStream_t s, const double* partials, int nstrips, int inner) {
     int mx = 0;
-    for (int p = 0; p < v.P.np; ++p) mx = v.P.ni[p] * v.P.nj[p] > mx ? v.P.ni[p] * v.P.nj[p] : mx;
-    dim3 grid((mx + 255) / 256, v.P.np);
+    for (int a = 0; a < v.P.nact; ++a) {
+        const int p = v.P.act[a];
+        mx = v.P.ni[p] * v.P.nj[p] > mx ? v.P.ni[p] * v.P.nj[p] : mx;
+    }
+    if (v.P.nact == 0) return 0;
+    dim3 grid((mx + 255) / 256, v.P.nact);
     k_nr_update<<<grid, 256, 0, s>>>(v, partials, nstrips, inner);
     return 1;
 }

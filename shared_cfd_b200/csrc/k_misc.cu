@@ -13,7 +13,7 @@ __global__ void k_dt_reset(View v) {
 }
 
 __global__ void k_set_dt(View v) {
-    const int p = blockIdx.y;
+    const int p = v.P.act[blockIdx.y];
     const int ni = v.P.ni[p], nj = v.P.nj[p];
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     double dtc = 1e300;
@@ -54,32 +54,37 @@ __global__ void k_dt_final(View v) {
     }
 }
 
-int launch_set_dt(const View& v, cudaStream_t s) {
+// dt_mat of the updated planes and, for a global dt, their minimum in
+// dtmin_bits (+inf when there is no cell)
+int launch_set_dt_cells(const View& v, cudaStream_t s) {
+    if (v.dt_mode == SCFD_DT_FIXED) return 0;
     int n = 0;
-    if (v.dt_mode == SCFD_DT_FIXED) {
-        k_dt_final<<<1, 1, 0, s>>>(v);
-        return 1;
-    }
-    int mx = 0;
-    for (int p = 0; p < v.P.np; ++p) mx = v.P.ni[p] * v.P.nj[p] > mx ? v.P.ni[p] * v.P.nj[p] : mx;
     if (v.dt_mode == SCFD_DT_GLOBAL) {
         k_dt_reset<<<1, 1, 0, s>>>(v);
         ++n;
     }
-    dim3 grid((mx + 255) / 256, v.P.np);
-    k_set_dt<<<grid, 256, 0, s>>>(v);
-    ++n;
-    if (v.dt_mode == SCFD_DT_GLOBAL) {
-        k_dt_final<<<1, 1, 0, s>>>(v);
-        ++n;
+    int mx = 0;
+    for (int a = 0; a < v.P.nact; ++a) {
+        const int p = v.P.act[a];
+        mx = v.P.ni[p] * v.P.nj[p] > mx ? v.P.ni[p] * v.P.nj[p] : mx;
     }
-    return n;
+    if (v.P.nact == 0) return n;
+    dim3 grid((mx + 255) / 256, v.P.nact);
+    k_set_dt<<<grid, 256, 0, s>>>(v);
+    return n + 1;
+}
+
+int launch_set_dt(const View& v, cudaStream_t s) {
+    const int n = launch_set_dt_cells(v, s);
+    if (v.dt_mode == SCFD_DT_LOCAL) return n;
+    k_dt_final<<<1, 1, 0, s>>>(v);
+    return n + 1;
 }
 
 // Deterministic two-pass RMS of q(E) - qp(E).
 __global__ void k_rms_partial(View v, double* partial) {
     __shared__ double sh[256];
-    const int p = blockIdx.y;
+    const int p = v.P.act[blockIdx.y];
     const int ni = v.P.ni[p], nj = v.P.nj[p];
     double acc = 0.0;
     const long long N = v.ncell;
@@ -106,13 +111,18 @@ __global__ void k_rms_final(const double* partial, int n, double cells, double* 
 }
 
 int launch_rms(const View& v, cudaStream_t s, double* partial, double* out) {
+    // a sharded context sums its own planes over the cell count of all planes
     const int gx = 64;
-    dim3 grid(gx, v.P.np);
-    k_rms_partial<<<grid, 256, 0, s>>>(v, partial);
+    int n = 0;
+    if (v.P.nact > 0) {
+        dim3 grid(gx, v.P.nact);
+        k_rms_partial<<<grid, 256, 0, s>>>(v, partial);
+        ++n;
+    }
     double cells = 0.0;
     for (int p = 0; p < v.P.np; ++p) cells = cells + (double)(v.P.ni[p] * v.P.nj[p]);
-    k_rms_final<<<1, 1, 0, s>>>(partial, gx * v.P.np, cells, out);
-    return 2;
+    k_rms_final<<<1, 1, 0, s>>>(partial, gx * v.P.nact, cells, out);
+    return n + 1;
 }
 
 // FP32 copies of w and vhi (all slots, ghosts included) for the mixed path.
@@ -121,7 +131,23 @@ __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, lo
         b[k] = (float)a[k];
 }
 
+// The slots of the updated planes only, when they are not all planes (a plane's
+// slots are contiguous: base[p] .. base[p] + (nj+4)*pitch[p]).
+__global__ void k_to_f32_planes(View v) {
+    const int p = v.P.act[blockIdx.y];
+    const long long b = v.P.base[p], n = (long long)(v.P.nj[p] + 4) * v.P.pitch[p], N = v.ncell;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        for (int m = 0; m < v.W; ++m) v.w32[m * N + b + k] = (float)v.w[m * N + b + k];
+        for (int m = 0; m < v.nY; ++m) v.vhi32[m * N + b + k] = (float)v.vhi[m * N + b + k];
+    }
+}
+
 int launch_to_f32(const View& v, cudaStream_t s) {
+    if (v.P.nact < v.P.np) {
+        if (v.P.nact == 0) return 0;
+        k_to_f32_planes<<<dim3(148 * 4, v.P.nact), 256, 0, s>>>(v);
+        return 1;
+    }
     const long long nw = v.W * v.ncell, nv = v.nY * v.ncell;
     k_to_f32<<<1184, 256, 0, s>>>(v.w, v.w32, nw);
     k_to_f32<<<1184, 256, 0, s>>>(v.vhi, v.vhi32, nv);

@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(NT) k_residual(View v) {
     RT* FI = reinterpret_cast<RT*>(smraw);
     const int D = v.D, nY = v.nY;
     RT* FJ = FI + TY * (TX + 1) * D;
-    const int p = blockIdx.z;
+    const int p = v.P.act[blockIdx.z];
     const int ni = v.P.ni[p], nj = v.P.nj[p];
     const int i0 = blockIdx.x * TX + 1, j0 = blockIdx.y * TY + 1;
     if (i0 > ni || j0 > nj) return;
@@ -303,11 +303,13 @@ __global__ void __launch_bounds__(NT) k_residual(View v) {
 template <typename RT, int MODE>
 static void launch_t(const View& v, cudaStream_t s) {
     int nimax = 0, njmax = 0;
-    for (int p = 0; p < v.P.np; ++p) {
+    for (int a = 0; a < v.P.nact; ++a) {
+        const int p = v.P.act[a];
         nimax = v.P.ni[p] > nimax ? v.P.ni[p] : nimax;
         njmax = v.P.nj[p] > njmax ? v.P.nj[p] : njmax;
     }
-    dim3 grid((nimax + TX - 1) / TX, (njmax + TY - 1) / TY, v.P.np);
+    if (v.P.nact == 0) return;
+    dim3 grid((nimax + TX - 1) / TX, (njmax + TY - 1) / TY, v.P.nact);
     const size_t smem = (size_t)(TY * (TX + 1) + (TY + 1) * TX) * v.D * sizeof(RT);
     static bool attr_set = false;
     if (!attr_set) {

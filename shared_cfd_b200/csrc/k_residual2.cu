@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(NTH) k_residual2(View v) {
     S.T = S.vh + NY * HS;
     S.FI = S.T + HS;
     S.FJ = S.FI + NFI * D;
-    const int p = blockIdx.z;
+    const int p = v.P.act[blockIdx.z];
     const int ni = v.P.ni[p], nj = v.P.nj[p];
     const int i0 = blockIdx.x * TX + 1, j0 = blockIdx.y * TY + 1;
     if (i0 > ni || j0 > nj) return;
@@ -274,11 +274,13 @@ template <typename RT, int NY, int MODE>
 static void launch2(const View& v, cudaStream_t s) {
     constexpr int D = NY + 3, W = D + 5;
     int nimax = 0, njmax = 0;
-    for (int p = 0; p < v.P.np; ++p) {
+    for (int a = 0; a < v.P.nact; ++a) {
+        const int p = v.P.act[a];
         nimax = v.P.ni[p] > nimax ? v.P.ni[p] : nimax;
         njmax = v.P.nj[p] > njmax ? v.P.nj[p] : njmax;
     }
-    dim3 grid((nimax + TX - 1) / TX, (njmax + TY - 1) / TY, v.P.np);
+    if (v.P.nact == 0) return;
+    dim3 grid((nimax + TX - 1) / TX, (njmax + TY - 1) / TY, v.P.nact);
     const size_t smem = ((size_t)(W + NY + 1) * HY * HX + (size_t)(NFI + NFJ) * D) * sizeof(RT);
     static bool attr = false;
     if (!attr) {

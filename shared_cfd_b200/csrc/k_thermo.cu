@@ -118,7 +118,7 @@ __device__ int dev_calc_T(const DevChem& ch, const double* vrho, double rho, dou
 }
 
 __global__ void __launch_bounds__(128) k_thermo(View v) {
-    const int p = blockIdx.y;
+    const int p = v.P.act[blockIdx.y];
     const int ni = v.P.ni[p], nj = v.P.nj[p];
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= ni * nj) return;
@@ -178,7 +178,8 @@ __global__ void __launch_bounds__(128) k_thermo(View v) {
 }
 
 int launch_thermo(const View& v, cudaStream_t s, int cells_per_plane_max) {
-    dim3 grid((cells_per_plane_max + 127) / 128, v.P.np);
+    if (v.P.nact == 0) return 0;
+    dim3 grid((cells_per_plane_max + 127) / 128, v.P.nact);
     k_thermo<<<grid, 128, 0, s>>>(v);
     return 1;
 }

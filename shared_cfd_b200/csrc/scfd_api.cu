@@ -79,6 +79,21 @@ struct scfd_ctx {
     std::vector<std::pair<int, size_t>> ev_marks;  // kind, index of the start event
     double kind_ms[SCFD_K_COUNT] = {0};
     long long kind_n[SCFD_K_COUNT] = {0};
+    // block sharding: planes of this rank, the cells it exports to other
+    // ranks' ghost copies, the cells it imports, exchange and reduction
+    // buffers, and the position of a staged step (scfd_dstep)
+    int nranks = 1, rank = 0;
+    std::vector<int> owner;
+    long long* d_exp = nullptr;
+    int nexp = 0;
+    HaloImport* d_imp = nullptr;
+    int nimp = 0;
+    double* d_halo = nullptr;
+    long long seg = 0;
+    double* d_red = nullptr;
+    int ds_stage = 0, ds_j = 0;
+    long long ds_att0 = 0, ds_fb0 = 0;
+    bool own(int p) const { return owner.empty() || owner[p] == rank; }  // p 0-based
 
     int fail(int code, const std::string& m) {
         err = m;
@@ -385,23 +400,32 @@ void collect_events(scfd_ctx* c) {
     c->ev_used = 0;
 }
 
-// the kernel sequence of one physical step
-int enqueue_step(scfd_ctx* c) {
-    const View& v = c->v;
-    cudaStream_t s = c->stream;
+// The kernels of one physical step, stage by stage; n counts the launches.
+struct Seq {
+    scfd_ctx* c;
+    const View& v;
+    cudaStream_t s;
     long long n = 0;
-    const bool reactive = c->d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
-    const long long qbytes = sizeof(double) * (long long)c->D * c->ncell;
-    auto primitive = [&]() { n += timed(c, SCFD_K_THERMO, [&] { return launch_thermo(v, s, c->cells_max); }); };
-    auto bc = [&]() {
+    explicit Seq(scfd_ctx* ctx) : c(ctx), v(ctx->v), s(ctx->stream) {}
+
+    void primitive() { n += timed(c, SCFD_K_THERMO, [&] { return launch_thermo(v, s, c->cells_max); }); }
+    void bc() {
         n += timed(c, SCFD_K_BC, [&] { return launch_ghosts(v, s, c->d_ops, c->nops, c->d_bcval, c->valstride); });
         if (v.precision == SCFD_PREC_MIXED) n += timed(c, SCFD_K_OTHER, [&] { return launch_to_f32(v, s); });
-    };
-    auto chem = [&]() {
+    }
+    void chem() {
         n += timed(c, SCFD_K_CHEM, [&] { return launch_chem_impl(v, s, c->d.chem_max_substeps, c->d_counter, c->nsm); });
-    };
-    auto setdt = [&]() { n += timed(c, SCFD_K_DT, [&] { return launch_set_dt(v, s); }); };
-    auto sweeps = [&]() {
+    }
+    void setdt() { n += timed(c, SCFD_K_DT, [&] { return launch_set_dt(v, s); }); }
+    void copyq(double* dst, const double* src) {
+        const long long qbytes = sizeof(double) * (long long)c->D * c->ncell;
+        timed(c, SCFD_K_COPY, [&] { return (int)(cudaMemcpyAsync(dst, src, qbytes, cudaMemcpyDeviceToDevice, s) ? 0 : 0); });
+    }
+    void residual(int mode) {
+        const bool coeffs = mode != RES_EULER && !c->use_sw3 && !c->use_sw4;
+        n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, mode, coeffs); });
+    }
+    void sweeps() {
         if (c->use_sw4) {
             const Sweep4& w4 = c->sw4;
             cudaMemsetAsync(w4.progress, 0, sizeof(int) * (2 * w4.ntasks + 2), s);
@@ -410,6 +434,7 @@ int enqueue_step(scfd_ctx* c) {
             n += timed(c, SCFD_K_SWEEP_BWD, [&] { return launch_sweep4(v, s, w4, 2, 0); });
             return;
         }
+        if (c->nsf == 0) return;  // a rank without planes
         launch_sweep_reset(s, c->d_progress, c->d_tickets, c->nsf, c->nsb);
         if (c->use_sw3) {
             n += timed(c, SCFD_K_PACK, [&] { return launch_sweep3(v, s, c->sw3, 0, 0); });
@@ -425,56 +450,75 @@ int enqueue_step(scfd_ctx* c) {
             return launch_sweep(v, s, 1, c->d_xfer, c->d_progress, c->d_partials, c->d_tickets, c->nsf, c->nsb,
                                 c->d_strips_f, c->d_strips_b);
         });
-    };
-    auto copyq = [&](double* dst, const double* src) {
-        timed(c, SCFD_K_COPY, [&] { return (int)(cudaMemcpyAsync(dst, src, qbytes, cudaMemcpyDeviceToDevice, s) ? 0 : 0); });
-    };
-    if (c->d.scheme == SCFD_SCHEME_NR) {
-        primitive();
-        setdt();
-        if (reactive) chem();
-        copyq(v.qpp, v.qp);
-        copyq(v.qp, v.q);
-        for (int j = 1; j < c->d.num_internal_loop; ++j) {
-            primitive();
-            bc();
-            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_NR, !c->use_sw3 && !c->use_sw4); });
-            sweeps();
-            if (c->use_sw4)
-                n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep4(v, s, c->sw4, 3, j); });
-            else if (c->use_sw3)
-                n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, c->sw3, 3, j); });
-            else
-                n += timed(c, SCFD_K_UPDATE, [&] { return launch_nr_update(v, s, c->d_partials, c->nsb, j); });
+    }
+    // the per-strip (res, omega) partials of the last backward sweep
+    const double* partials() const { return c->use_sw4 ? c->sw4.partials : c->use_sw3 ? c->sw3.partials : c->d_partials; }
+    int nstrips() const { return c->use_sw4 ? c->sw4.nstrips : c->use_sw3 ? c->sw3.nstrips : c->nsb; }
+    // q update after the sweeps: NR relaxes with the omega reduced from
+    // `part` (nparts strip partials); LU-SGS (inner = 1) adds Dq
+    void update(int inner, const double* part, int nparts) {
+        if (c->use_sw4) {
+            Sweep4 w4 = c->sw4;
+            w4.partials = const_cast<double*>(part);
+            w4.nstrips = nparts;
+            n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep4(v, s, w4, 3, inner); });
+        } else if (c->use_sw3) {
+            if (c->nsf == 0) return;
+            Sweep3 w3 = c->sw3;
+            w3.partials = const_cast<double*>(part);
+            w3.nstrips = nparts;
+            n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, w3, 3, inner); });
+        } else if (c->d.scheme == SCFD_SCHEME_NR) {
+            n += timed(c, SCFD_K_UPDATE, [&] { return launch_nr_update(v, s, part, nparts, inner); });
         }
+    }
+    void step_end() {
         n += timed(c, SCFD_K_OTHER, [&] { return launch_step_end(v, s, c->d.res_rate_warn, c->d.res_rate_err); });
+    }
+};
+
+// the kernel sequence of one physical step
+int enqueue_step(scfd_ctx* c) {
+    Seq q(c);
+    const View& v = c->v;
+    const bool reactive = c->d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
+    if (c->d.scheme == SCFD_SCHEME_NR) {
+        q.primitive();
+        q.setdt();
+        if (reactive) q.chem();
+        q.copyq(v.qpp, v.qp);
+        q.copyq(v.qp, v.q);
+        for (int j = 1; j < c->d.num_internal_loop; ++j) {
+            q.primitive();
+            q.bc();
+            q.residual(RES_NR);
+            q.sweeps();
+            q.update(j, q.partials(), q.nstrips());
+        }
+        q.step_end();
     } else {
         if (reactive) {
-            primitive();
-            setdt();
-            chem();
-            copyq(v.qp, v.q);
-            primitive();
+            q.primitive();
+            q.setdt();
+            q.chem();
+            q.copyq(v.qp, v.q);
+            q.primitive();
         } else {
-            copyq(v.qp, v.q);
-            primitive();
-            setdt();
+            q.copyq(v.qp, v.q);
+            q.primitive();
+            q.setdt();
         }
-        bc();
+        q.bc();
         if (c->d.scheme == SCFD_SCHEME_EULER) {
-            n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, RES_EULER, false); });
+            q.residual(RES_EULER);
         } else {
-            n += timed(c, SCFD_K_RESIDUAL,
-                       [&] { return launch_residual(v, s, RES_LUSGS, !c->use_sw3 && !c->use_sw4); });
-            sweeps();
-            if (c->use_sw4)
-                n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep4(v, s, c->sw4, 3, 1); });
-            else if (c->use_sw3)
-                n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, c->sw3, 3, 1); });
+            q.residual(RES_LUSGS);
+            q.sweeps();
+            q.update(1, q.partials(), q.nstrips());
         }
     }
     CK(cudaGetLastError());
-    c->launches += n;
+    c->launches += q.n;
     return 0;
 }
 
@@ -618,10 +662,61 @@ int scfd_commit(scfd_ctx* c) {
     std::vector<GhostOp> ops;
     int st = build_ghost_ops(c, g, ops);
     if (st) return st;
+    // planes this rank updates
+    c->P.nact = 0;
+    for (int p = 0; p < c->np; ++p)
+        if (c->own(p)) c->P.act[c->P.nact++] = p;
+    // Block sharding: every rank keeps the ghost writes of its own planes.  The
+    // halo copies among them whose source cell lies on another rank's plane
+    // read that cell from the exchange buffer: rank q exports, in slot order,
+    // every cell of its planes that a halo copy onto another rank's plane
+    // reads; each rank imports the exported cells its own copies read.
+    std::vector<long long> exp_cells;
+    std::vector<HaloImport> imps;
+    if (!c->owner.empty()) {
+        auto plane_of = [&](long long slot) {
+            int p = 0;
+            while (p + 1 < c->np && c->P.base[p + 1] <= slot) ++p;
+            return p;
+        };
+        std::vector<std::vector<long long>> ex(c->nranks);
+        for (const GhostOp& o : ops) {
+            if (o.kind != -1) continue;
+            const int q = c->owner[plane_of(o.src)];
+            if (c->owner[plane_of(o.dst)] != q) ex[q].push_back(o.src);
+        }
+        size_t mx = 0;
+        for (auto& e : ex) {
+            std::sort(e.begin(), e.end());
+            e.erase(std::unique(e.begin(), e.end()), e.end());
+            mx = std::max(mx, e.size());
+        }
+        c->seg = (long long)mx * (c->W + c->nY);
+        exp_cells = ex[c->rank];
+        std::vector<GhostOp> mine;
+        std::vector<long long> reads;
+        for (const GhostOp& o : ops)
+            if (c->own(plane_of(o.dst))) {
+                mine.push_back(o);
+                reads.push_back(o.src);
+            }
+        ops.swap(mine);
+        std::sort(reads.begin(), reads.end());
+        for (int q = 0; q < c->nranks; ++q) {
+            if (q == c->rank) continue;
+            const long long n = (long long)ex[q].size();
+            for (long long t = 0; t < n; ++t)
+                if (std::binary_search(reads.begin(), reads.end(), ex[q][t]))
+                    imps.push_back(HaloImport{ex[q][t], q * c->seg + t, n});
+        }
+    }
+    c->nexp = (int)exp_cells.size();
+    c->nimp = (int)imps.size();
     c->nops = (int)ops.size();
     // strips for the sweeps
     std::vector<int> sf, sb;
     for (int p = 0; p < c->np; ++p) {
+        if (!c->own(p)) continue;
         const int ns = (c->P.nj[p] + 31) / 32;
         for (int s = 0; s < ns; ++s) {
             sf.push_back(p);
@@ -647,7 +742,7 @@ int scfd_commit(scfd_ctx* c) {
     c->use_graph = !(graph_env && std::strcmp(graph_env, "0") == 0);
     int qc4 = 0;
     const size_t blk4 = impl ? sweep4_record_elems(nY, mixed, &qc4) : 0;
-    c->use_sw4 = blk4 > 0 && !legacy && sweep_env && std::strcmp(sweep_env, "4") == 0;
+    c->use_sw4 = blk4 > 0 && !legacy && sweep_env && std::strcmp(sweep_env, "4") == 0 && c->owner.empty();
     c->use_sw3 = blk3 > 0 && !legacy && !c->use_sw4;
     // quad-per-cell sweeps: strips of R rows, tasks of up to WPC strips
     std::vector<long long> rec_off4;
@@ -680,6 +775,7 @@ int scfd_commit(scfd_ctx* c) {
     if (c->use_sw3) {
         int fs = 0;
         for (int pl = 0; pl < c->np; ++pl) {
+            if (!c->own(pl)) continue;
             const int ns = (c->P.nj[pl] + 31) / 32, steps = c->P.ni[pl] + 31;
             for (int st3 = 0; st3 < ns; ++st3, ++fs) {
                 const int pad = sweep3_pad_steps();
@@ -694,6 +790,7 @@ int scfd_commit(scfd_ctx* c) {
         }
         int base3 = 0;
         for (int pl = 0; pl < c->np; ++pl) {
+            if (!c->own(pl)) continue;
             const int ns = (c->P.nj[pl] + 31) / 32;
             for (int st3 = ns - 1; st3 >= 0; --st3) tabb3.insert(tabb3.end(), {pl, st3, base3 + st3, 0});
             base3 += ns;
@@ -712,6 +809,8 @@ int scfd_commit(scfd_ctx* c) {
     bytes += need<double>((size_t)c->nsf * (c->nimax + 8) * D);
     bytes += need<int>(c->nsf + c->nsb) + need<int>(2) + need<double>(2 * c->nsb);
     bytes += need<GhostOp>(std::max(1, c->nops)) + need<double>(std::max<size_t>(1, c->bcs.size()) * c->valstride);
+    bytes += need<long long>(std::max(1, c->nexp)) + need<HaloImport>(std::max(1, c->nimp)) +
+             need<double>(std::max<long long>(1, c->seg * c->nranks)) + need<double>(8);
     bytes += need<unsigned long long>(1) + need<double>(nrec) + need<double>(1);
     bytes += tabs.bytes();
     const size_t nref = (size_t)(c->nimax + 4) * (c->njmax + 4) * c->np;
@@ -761,6 +860,10 @@ int scfd_commit(scfd_ctx* c) {
     c->d_tickets = carve<int>(p, 2);
     c->d_partials = carve<double>(p, 2 * c->nsb);
     c->d_ops = carve<GhostOp>(p, std::max(1, c->nops));
+    c->d_exp = carve<long long>(p, std::max(1, c->nexp));
+    c->d_imp = carve<HaloImport>(p, std::max(1, c->nimp));
+    c->d_halo = carve<double>(p, std::max<long long>(1, c->seg * c->nranks));
+    c->d_red = carve<double>(p, 8);
     c->d_bcval = carve<double>(p, std::max<size_t>(1, c->bcs.size()) * c->valstride);
     c->d_counter = carve<unsigned long long>(p, 1);
     c->d_rms_partial = carve<double>(p, nrec);
@@ -835,6 +938,11 @@ int scfd_commit(scfd_ctx* c) {
     CK(cudaMemcpyAsync(c->d_strips_b, sb.data(), sb.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
     if (c->nops)
         CK(cudaMemcpyAsync(c->d_ops, ops.data(), ops.size() * sizeof(GhostOp), cudaMemcpyHostToDevice, c->stream));
+    if (c->nexp)
+        CK(cudaMemcpyAsync(c->d_exp, exp_cells.data(), exp_cells.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                           c->stream));
+    if (c->nimp)
+        CK(cudaMemcpyAsync(c->d_imp, imps.data(), imps.size() * sizeof(HaloImport), cudaMemcpyHostToDevice, c->stream));
     if (!c->bcs.empty()) {
         std::vector<double> val(c->bcs.size() * c->valstride);
         for (size_t k = 0; k < c->bcs.size(); ++k)
@@ -943,6 +1051,7 @@ int scfd_upload(scfd_ctx* c, const double* q, const double* w, const double* vhi
     CK(cudaMemcpyAsync(c->d_sc, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->uploaded = true;
+    c->ds_stage = 0;
     return 0;
 }
 
@@ -996,6 +1105,7 @@ int step_once(scfd_ctx* c) {
 
 int scfd_step(scfd_ctx* c, int step, scfd_stats* stats) {
     if (!c || !c->committed || !c->uploaded) return c ? c->fail(SCFD_E_STATE, "step before upload") : SCFD_E_ARG;
+    if (c->nranks > 1) return c->fail(SCFD_E_STATE, "partitioned context: step through scfd_dstep");
     (void)step;
     int st = sync_scalars(c);
     if (st) return st;
@@ -1009,6 +1119,7 @@ int scfd_step(scfd_ctx* c, int step, scfd_stats* stats) {
 
 int scfd_run(scfd_ctx* c, int step, int nsteps, scfd_stats* stats) {
     if (!c || !c->committed || !c->uploaded) return c ? c->fail(SCFD_E_STATE, "run before upload") : SCFD_E_ARG;
+    if (c->nranks > 1) return c->fail(SCFD_E_STATE, "partitioned context: step through scfd_dstep");
     (void)step;
     int st = sync_scalars(c);
     if (st) return st;
@@ -1021,6 +1132,137 @@ int scfd_run(scfd_ctx* c, int step, int nsteps, scfd_stats* stats) {
     if ((st = sync_scalars(c))) return st;
     collect_events(c);
     return fill_stats(c, stats, att0, fb0);
+}
+
+int scfd_set_partition(scfd_ctx* c, const int32_t* owner, int nranks, int rank) {
+    if (!c || !owner || nranks < 1 || nranks > SCFD_MAX_RANKS || rank < 0 || rank >= nranks) return SCFD_E_ARG;
+    if (c->committed) return c->fail(SCFD_E_STATE, "partition after commit");
+    for (int p = 0; p < c->np; ++p)
+        if (owner[p] < 0 || owner[p] >= nranks) return c->fail(SCFD_E_ARG, "plane owner out of range");
+    c->owner.assign(owner, owner + c->np);
+    c->nranks = nranks;
+    c->rank = rank;
+    return 0;
+}
+
+// Stages of scfd_dstep: the kernel sequence of enqueue_step cut at the points
+// where the ranks exchange halo cells or reduce scalars.  The device carries
+// on whatever the status; every rank issues the same requests.
+enum { DS_BEGIN = 0, DS_AFTER_DT, DS_INNER, DS_AFTER_HALO_NR, DS_AFTER_RES, DS_AFTER_HALO, DS_AFTER_STATUS };
+
+int scfd_dstep(scfd_ctx* c, int step, scfd_dreq* req, scfd_stats* stats) {
+    if (!c || !req) return SCFD_E_ARG;
+    req->kind = SCFD_DREQ_DONE;
+    req->buf = nullptr;
+    if (!c->committed || !c->uploaded) return c->fail(SCFD_E_STATE, "dstep before upload");
+    (void)step;
+    const bool nr = c->d.scheme == SCFD_SCHEME_NR;
+    const bool reactive = c->d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
+    const View& v = c->v;
+    cudaStream_t s = c->stream;
+    Seq q(c);
+    auto reduce = [&](int nsum, int nmin, int next) {
+        req->kind = SCFD_DREQ_REDUCE;
+        req->nsum = nsum;
+        req->nmin = nmin;
+        req->buf = c->d_red;
+        c->ds_stage = next;
+    };
+    auto exchange = [&](int next) {
+        q.n += launch_halo_pack(v, s, c->d_exp, c->nexp, c->d_halo + (long long)c->rank * c->seg);
+        req->kind = SCFD_DREQ_HALO;
+        req->nranks = c->nranks;
+        req->seg = c->seg;
+        req->buf = c->d_halo;
+        c->ds_stage = next;
+    };
+    bool finished = false;
+    for (bool more = true; more;) {
+        more = false;
+        switch (c->ds_stage) {
+            case DS_BEGIN: {
+                const int st = sync_scalars(c);
+                if (st) return st;
+                c->ds_att0 = c->h_sc->chem_attempts;
+                c->ds_fb0 = c->h_sc->chem_fallback;
+                c->launches = 0;
+                if (!nr && !reactive) q.copyq(v.qp, v.q);
+                q.primitive();
+                q.n += timed(c, SCFD_K_DT, [&] { return launch_set_dt_cells(v, s); });
+                q.n += launch_dt_export(v, s, c->d_red);
+                reduce(0, 2, DS_AFTER_DT);
+                break;
+            }
+            case DS_AFTER_DT:
+                q.n += launch_dt_import(v, s, c->d_red);
+                if (reactive) q.chem();
+                if (nr) {
+                    q.copyq(v.qpp, v.qp);
+                    q.copyq(v.qp, v.q);
+                    c->ds_j = 1;
+                    c->ds_stage = DS_INNER;
+                    more = true;
+                    break;
+                }
+                if (reactive) {
+                    q.copyq(v.qp, v.q);
+                    q.primitive();
+                }
+                exchange(DS_AFTER_HALO);
+                break;
+            case DS_INNER:
+                if (c->ds_j >= c->d.num_internal_loop) {
+                    q.step_end();
+                    finished = true;
+                    break;
+                }
+                q.primitive();
+                exchange(DS_AFTER_HALO_NR);
+                break;
+            case DS_AFTER_HALO_NR:
+                q.n += launch_halo_unpack(v, s, c->d_imp, c->nimp, c->d_halo);
+                q.bc();
+                q.residual(RES_NR);
+                q.sweeps();
+                q.n += launch_res_export(v, s, q.partials(), c->nsf == 0 ? 0 : q.nstrips(), c->d_red);
+                reduce(1, 2, DS_AFTER_RES);
+                break;
+            case DS_AFTER_RES:
+                q.n += launch_res_import(v, s, c->d_red, c->ds_j);
+                q.update(c->ds_j, c->d_red, 1);
+                ++c->ds_j;
+                c->ds_stage = DS_INNER;
+                more = true;
+                break;
+            case DS_AFTER_HALO:
+                q.n += launch_halo_unpack(v, s, c->d_imp, c->nimp, c->d_halo);
+                q.bc();
+                if (c->d.scheme == SCFD_SCHEME_EULER) {
+                    q.residual(RES_EULER);
+                } else {
+                    q.residual(RES_LUSGS);
+                    q.sweeps();
+                    q.update(1, q.partials(), q.nstrips());
+                }
+                q.n += launch_status_export(v, s, c->d_red);
+                reduce(0, 1, DS_AFTER_STATUS);
+                break;
+            default:  // DS_AFTER_STATUS
+                q.n += launch_status_import(v, s, c->d_red);
+                finished = true;
+                break;
+        }
+    }
+    CK(cudaGetLastError());
+    c->launches += q.n;
+    if (!finished) return 0;
+    c->ds_stage = DS_BEGIN;
+    req->kind = SCFD_DREQ_DONE;
+    req->buf = nullptr;
+    const int st = sync_scalars(c);
+    if (st) return st;
+    collect_events(c);
+    return fill_stats(c, stats, c->ds_att0, c->ds_fb0);
 }
 
 int scfd_rms(scfd_ctx* c, double* rms) {

@@ -29,6 +29,10 @@ struct Planes {
     int nj[kMaxPlanes];
     int pitch[kMaxPlanes];
     long long base[kMaxPlanes];
+    // planes this context updates (all of them unless the case is sharded over
+    // ranks); kernels with one grid row per plane run over act[0..nact)
+    int nact;
+    int act[kMaxPlanes];
 };
 
 __host__ __device__ inline long long cidx(const Planes& P, int p, int i, int j) {
@@ -110,6 +114,7 @@ struct GhostOp {
 int launch_thermo(const View& v, cudaStream_t s, int cells_per_plane_max);
 int launch_ghosts(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride);
 int launch_set_dt(const View& v, cudaStream_t s);
+int launch_set_dt_cells(const View& v, cudaStream_t s);  // dt_mat and the local minimum only
 int launch_residual(const View& v, cudaStream_t s, int mode, bool need_coeffs);
 bool launch_residual2(const View& v, cudaStream_t s, int mode);
 int launch_sweep_reset(cudaStream_t s, int* progress, int* tickets, int nstrips_fwd, int nstrips_bwd);
@@ -168,6 +173,22 @@ int launch_to_f32(const View& v, cudaStream_t s);
 // reference layout <-> SoA slots (dir 0: ref -> soa, dir 1: soa -> ref_out)
 int launch_ref_soa(const View& v, cudaStream_t s, int nk, int IX, int JX, const double* ref, double* soa,
                    double* ref_out, int dir);
+
+// block sharding (k_shard.cu): exchange of the cells other ranks' ghost
+// copies read, and the device halves of the cross-rank reductions
+struct HaloImport {
+    long long slot;  // cell written
+    long long off;   // buffer index of component 0
+    long long n;     // buffer stride between components
+};
+int launch_halo_pack(const View& v, cudaStream_t s, const long long* cells, int n, double* out);
+int launch_halo_unpack(const View& v, cudaStream_t s, const HaloImport* imp, int n, const double* buf);
+int launch_dt_export(const View& v, cudaStream_t s, double* red);        // red = [dt_min, -status]
+int launch_dt_import(const View& v, cudaStream_t s, const double* red);
+int launch_res_export(const View& v, cudaStream_t s, const double* partials, int nstrips, double* red);
+int launch_res_import(const View& v, cudaStream_t s, const double* red, int inner);  // red = [res, omega, -status]
+int launch_status_export(const View& v, cudaStream_t s, double* red);    // red = [-status]
+int launch_status_import(const View& v, cudaStream_t s, const double* red);
 
 // residual modes
 enum { RES_EULER = 0, RES_LUSGS = 1, RES_NR = 2 };

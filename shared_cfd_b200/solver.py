@@ -92,12 +92,19 @@ class Case:
 class Solver:
     """Runs a Case through one library (the CUDA library by default)."""
 
-    def __init__(self, case, lib=None):
+    def __init__(self, case, lib=None, partition=None):
+        """partition: optional (owner, nranks, rank) of a block-sharded run,
+        owner[p] the 0-based rank of plane p (scfd_set_partition)."""
         self.case = case
         self.lib = lib if lib is not None else load_library()
         self.ctx = C.c_void_p()
         self._check(self.lib.create(C.byref(case.desc), C.byref(self.ctx)), "create")
         try:
+            if partition is not None:
+                owner, nranks, rank = partition
+                own = np.ascontiguousarray(owner, dtype=np.int32)
+                self._check(self.lib.set_partition(self.ctx, own.ctypes.data_as(C.POINTER(C.c_int32)), nranks,
+                                                   rank), "set_partition")
             for p, (xh, rh) in enumerate(case.planes):
                 xf = np.asfortranarray(xh, dtype=np.float64).reshape(-1, order="F").copy()
                 rf = np.asfortranarray(rh, dtype=np.float64).reshape(-1, order="F").copy()
