@@ -13,9 +13,15 @@ C ABI with host buffers copied in and the result copied out every step.
 --config reactors measures the batched 0-D reactors instead: reactors/s for
 one batch of 8192 H2/air reactors integrated to 2 ms (a step is one batch).
 
-One JSON line is printed by rank 0.  Under torchrun every rank runs its own
-replica of the workload on its own GPU (weak scaling, no data exchange) and
-the time is the maximum over ranks.
+One JSON line is printed by rank 0.  Under torchrun (N > 1) the flow
+configurations are block-sharded over the ranks (strong scaling: the same
+workload; each block is cut along i into ceil(N/2) pieces for the four-block
+reacting step, N pieces for a single-block case, and the pieces are spread
+evenly by cell count): halo cells travel by NCCL all-gather, dt, the inner
+residual, omega and the status by NCCL all-reduce, all on the library's
+stream.  --sharded takes that path also at N = 1.  The reactors are
+independent units: each rank integrates its own batch (weak scaling, no data
+exchange).  Times are the maximum over ranks.
 """
 import argparse
 import ctypes as C
@@ -45,6 +51,13 @@ def make_case(config, scale, precision):
     if config == "flat_plate":
         return cases.flat_plate(int(round(256 * scale)), int(round(128 * scale)), precision=precision)
     return cases.sod(int(round(400 * scale)), 4, precision=precision)
+
+
+def shard_pieces(config, world):
+    """Pieces per block along i for a run over `world` ranks."""
+    if world <= 1:
+        return 1
+    return (world + 1) // 2 if config == "reacting_step" else world
 
 
 def iters_per_step(case):
@@ -175,7 +188,8 @@ def time_resident(solver, steps, warmup, torch, dev, sampler_dev, barrier):
     return e0.elapsed_time(e1), st, solver.launch_count(), cs.summary()
 
 
-def kernel_profile(solver, steps, case, mixed):
+def kernel_profile(solver, steps, case, mixed, ncells=None):
+    ncells = case.ncells if ncells is None else ncells
     lib = solver.lib
     lib.profile(solver.ctx, 1)
     solver.run(100, steps)
@@ -188,7 +202,7 @@ def kernel_profile(solver, steps, case, mixed):
         if n.value:
             out[name.value.decode()] = {"kind": k, "total_ms": ms.value, "launches": n.value,
                                         "avg_ms": ms.value / n.value,
-                                        "bytes_per_launch": algo_bytes(k, case, mixed) * case.ncells}
+                                        "bytes_per_launch": algo_bytes(k, case, mixed) * ncells}
     lib.profile(solver.ctx, 0)
     return out
 
@@ -380,6 +394,7 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sharded", action="store_true", help="block-sharded path also at N = 1 (needs torchrun)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -412,7 +427,8 @@ def main():
     dev = local if torch.cuda.device_count() > 1 else 0
     torch.cuda.set_device(dev)
     dist = None
-    if world > 1:
+    sharded = world > 1 or args.sharded
+    if sharded:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", dev))
@@ -429,6 +445,7 @@ def main():
         return float(t.item())
 
     from shared_cfd_b200 import build
+    from shared_cfd_b200.sharded import ShardedSolver, partition_planes
     from shared_cfd_b200.solver import Solver
     if rank == 0:
         build.build()
@@ -436,14 +453,21 @@ def main():
 
     res = {}
     solvers = {}
+    pieces = shard_pieces(args.config, world)
     for prec, tag in ((abi.PREC_MIXED, "mixed"), (abi.PREC_FP64, "fp64")):
         case = make_case(args.config, args.scale, prec)
-        s = Solver(case)
+        if sharded:
+            case = cases.split_planes_i(case, pieces)
+            owner = partition_planes([a * b for a, b in zip(case.ni, case.nj)], world)
+            s = ShardedSolver(case, owner)
+        else:
+            s = Solver(case)
         s.upload()
         s.prepare(1)
         ms, st, nl, clk = time_resident(s, args.steps, args.warmup, torch, dev, dev, barrier)
         ms = max_over_ranks(ms)
-        units = case.ncells * iters_per_step(case) * args.steps * world
+        # strong scaling under sharding: the ranks share one workload
+        units = case.ncells * iters_per_step(case) * args.steps * (1 if sharded else world)
         res[tag] = {"ms": ms, "value": units / (ms * 1e-3) / 1e6, "launches": nl, "clocks": clk,
                     "status": st.status, "res_warn": st.res_warn, "omega": st.omega,
                     "chem_attempts": st.chem_attempts, "chem_fallback": st.chem_fallback_cells}
@@ -451,8 +475,8 @@ def main():
         log("%s: %.2f ms/step  %.1f Mcell-iter/s  status %d" % (tag, ms / args.steps, res[tag]["value"], st.status))
 
     # accuracy of the mixed path against the FP64 path after the same steps
-    qm, _, _, _ = solvers["mixed"][0].download()
-    qd, _, _, _ = solvers["fp64"][0].download()
+    qm, _, _, _ = solvers["mixed"][0].gather() if sharded else solvers["mixed"][0].download()
+    qd, _, _, _ = solvers["fp64"][0].gather() if sharded else solvers["fp64"][0].download()
     case = solvers["fp64"][1]
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from helpers import rel_l2
@@ -460,8 +484,9 @@ def main():
 
     # per-kernel device times (separate, profiled pass of the mixed path)
     s_m, case_m = solvers["mixed"]
-    prof = kernel_profile(s_m, args.steps, case_m, True)
-    prof64 = kernel_profile(solvers["fp64"][0], args.steps, case, False)
+    cells_here = s_m.owned_cells if sharded else case_m.ncells
+    prof = kernel_profile(s_m, args.steps, case_m, True, cells_here)
+    prof64 = kernel_profile(solvers["fp64"][0], args.steps, case, False, cells_here)
     peak, peak_kind = measured_peaks()
     hbm = {k: v for k, v in prof.items() if v["bytes_per_launch"] > 0 and v["kind"] != abi.K_CHEM}
     top = max(prof.items(), key=lambda kv: kv[1]["total_ms"])
@@ -469,7 +494,7 @@ def main():
     ach = dom[1]["bytes_per_launch"] / (dom[1]["avg_ms"] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "peak_source": peak_kind,
-                "traffic": traffic_per_launch(args.config, True, dom[1]["kind"], case_m.ncells),
+                "traffic": traffic_per_launch(args.config, True, dom[1]["kind"], cells_here),
                 "traffic_source": NCU_TRAFFIC_NOTE,
                 "algorithmic_bytes_per_launch": dom[1]["bytes_per_launch"],
                 "avg_launch_ms": dom[1]["avg_ms"], "top_kernel_by_time": top[0]}
@@ -478,7 +503,7 @@ def main():
         r = prof["residual"]
         ach_r = r["bytes_per_launch"] / (r["avg_ms"] * 1e-3) / 1e9
         roofline["flux_kernel"] = {"kernel": "residual", "achieved": ach_r, "frac": ach_r / peak,
-                                   "traffic": traffic_per_launch(args.config, True, abi.K_RESIDUAL, case_m.ncells),
+                                   "traffic": traffic_per_launch(args.config, True, abi.K_RESIDUAL, cells_here),
                                    "avg_launch_ms": r["avg_ms"]}
     for v in list(prof.values()) + list(prof64.values()):
         if v["bytes_per_launch"]:
@@ -497,11 +522,14 @@ def main():
     t0 = time.perf_counter()
     for k in range(args.steps):
         s_e._check(lib.upload(s_e.ctx, abi.dptr(q), abi.dptr(w), abi.dptr(vhi), 0.0), "upload")
-        st = abi.Stats()
-        lib.step(s_e.ctx, k + 1, C.byref(st))
+        if sharded:
+            s_e.dstep(k + 1)
+        else:
+            st = abi.Stats()
+            lib.step(s_e.ctx, k + 1, C.byref(st))
         s_e._check(lib.download(s_e.ctx, abi.dptr(qout), None, None, C.byref(ttc)), "download")
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    units = case_e.ncells * iters_per_step(case_e) * args.steps * world
+    units = case_e.ncells * iters_per_step(case_e) * args.steps * (1 if sharded else world)
     e2e = {"value": units / e2e_s / 1e6, "unit": "Mcell-iter/s",
            "h2d_bytes_per_step": int(q.nbytes + w.nbytes + vhi.nbytes), "d2h_bytes_per_step": int(qout.nbytes)}
 
@@ -521,9 +549,12 @@ def main():
             "metric": "Mcell-iter/s (mixed FP32/FP64; plain FP64 in fp64_value)",
             "value": m["value"], "unit": "Mcell-iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": m["ms"] / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic (seeded)",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic (seeded)",
             "config": {"workload": workload_name(args.config, args.scale), "cells": case.ncells,
-                       "inner_iterations": iters_per_step(case), "parallelism": "replica per GPU" if world > 1 else "1 GPU",
+                       "inner_iterations": iters_per_step(case),
+                       "parallelism": ("%d GPU(s), block-sharded: %d planes (blocks cut along i into %d), "
+                                       "NCCL all-gather of halo cells and all-reduce of dt/res/omega/status"
+                                       % (world, len(case.planes), pieces)) if sharded else "1 GPU",
                        "l2": l2_note(case)},
             "fp64_value": res["fp64"]["value"], "fp64_ms_per_step": res["fp64"]["ms"] / args.steps,
             "mixed_over_fp64": m["value"] / res["fp64"]["value"],

@@ -374,6 +374,53 @@ def forward_step(orientation=0, n=12, scheme=abi.SCHEME_EULER, dt_mode=abi.DT_GL
     return case
 
 
+def split_planes_i(case, k):
+    """The same case with every plane cut along i into k pieces of (nearly)
+    equal width, joined again by i-i block interfaces that the connectivity
+    generator finds (the pieces share their cut node columns exactly).  The
+    boundary descriptors, the initial state (ghost layers included) and the
+    chemistry carry over; the LU-SGS sweeps then stop at the cuts, as they do
+    at the sub-domain edges of the reference's MPI decomposition."""
+    if k <= 1:
+        return case
+    planes, origin = [], []  # origin[n] = (plane, a, b): interior columns a+1..b
+    for p, (xh, rh) in enumerate(case.planes):
+        ni = xh.shape[0] - 1
+        cuts = [int(round(m * ni / k)) for m in range(k + 1)]
+        if min(b - a for a, b in zip(cuts, cuts[1:])) < 2:
+            raise ValueError("plane %d (ni=%d) is too narrow for %d pieces" % (p + 1, ni, k))
+        for a, b in zip(cuts, cuts[1:]):
+            planes.append((xh[a:b + 1].copy(), rh[a:b + 1].copy()))
+            origin.append((p, a, b))
+    if len(planes) > abi.MAX_PLANES:
+        raise ValueError("%d planes exceed the %d of the ABI" % (len(planes), abi.MAX_PLANES))
+    desc = abi.Desc.from_buffer_copy(case.desc)
+    cut, _ = F.connectivity(planes)
+    new = Case(planes, desc, cut=cut, chem=case.chem)
+    for b in case.bcs:
+        pieces = [(n, a, e) for n, (p, a, e) in enumerate(origin) if p == b.plane - 1]
+        if b.side == abi.SIDE_ILO:
+            targets = [(pieces[0][0], b.first, b.last)]
+        elif b.side == abi.SIDE_IHI:
+            targets = [(pieces[-1][0], b.first, b.last)]
+        else:
+            targets = [(n, max(b.first, a + 1) - a, min(b.last, e) - a) for n, a, e in pieces]
+            targets = [t for t in targets if t[1] <= t[2]]
+        for n, lo, hi in targets:
+            nb = abi.BC.from_buffer_copy(b)
+            nb.plane, nb.first, nb.last = n + 1, lo, hi
+            new.bcs.append(nb)
+    for n, (p, a, b) in enumerate(origin):
+        nj, ni = case.nj[p], b - a
+        for dst, src in ((new.q, case.q), (new.w, case.w), (new.vhi, case.vhi)):
+            dst[n, :nj + 4, :ni + 4] = src[p, :nj + 4, a:b + 4]
+    for attr in ("mech", "steps", "states"):
+        if hasattr(case, attr):
+            setattr(new, attr, getattr(case, attr))
+    new.name = "%s_i%d" % (getattr(case, "name", "case"), k)
+    return new
+
+
 def perturb(case, seed=1, amp=0.05):
     """Seeded smooth perturbation of the initial state (density, velocity,
     pressure for the ideal gas; temperature and mixing for chemistry) so that

@@ -64,6 +64,11 @@ class ShardedSolver(Solver):
         super().__init__(case, lib=lib, partition=(self.owner, nranks, rank))
         self._device = self.stream() is not None
         self._views = {}
+        self._run_launches = 0
+
+    @property
+    def owned_cells(self):
+        return sum(a * b for a, b, o in zip(self.case.ni, self.case.nj, self.owner) if o == self.rank)
 
     # -- request buffers ---------------------------------------------------
     def buffer(self, addr, n):
@@ -123,11 +128,17 @@ class ShardedSolver(Solver):
 
     def run(self, step, nsteps, check=True):
         st = None
+        self._run_launches = 0
         for n in range(nsteps):
             st = self.dstep(step + n, check)
+            self._run_launches += Solver.launch_count(self)
             if st.status:
                 break
         return st
+
+    def launch_count(self):
+        """Kernels launched by the last run() (scfd_launch_count covers one step)."""
+        return self._run_launches
 
     def rms(self):
         """The global RMS: the library returns this rank's share."""

@@ -243,3 +243,33 @@ def test_gloo_two_processes_match_unsharded(orc, tmp_path):
         assert int(got["status"]) == 0
         assert float(got["res"]) == pytest.approx(st.res, rel=1e-12)
         assert float(got["rms"]) == pytest.approx(rms, rel=1e-12)
+
+
+@pytest.mark.parametrize("orientation", [0, 1, 2, 3])
+def test_split_planes_explicit_equals_unsplit(orc, orientation):
+    """Cutting the blocks along i (the decomposition of multi-GPU runs) leaves
+    an explicit inviscid step bit-identical: the two-layer halo copies give
+    every face the neighbours it had in the whole block."""
+    whole = cases.perturb(cases.forward_step(orientation, n=8), seed=4)
+    cut = cases.split_planes_i(whole, 2)
+    assert len(cut.planes) == 4
+    r0 = run_case(whole, orc, 5)
+    r2 = run_case(cut, orc, 5)
+    for p in range(2):
+        joined = np.concatenate([cut.interior(r2["q"], 2 * p), cut.interior(r2["q"], 2 * p + 1)], axis=1)
+        assert np.array_equal(joined, whole.interior(r0["q"], p))
+    assert r0["tt"] == r2["tt"]
+
+
+def test_split_reacting_step_sharded_over_four_ranks(orc):
+    """The decomposition bench.py uses on 4 GPUs: each block cut in two along
+    i, one large and one small piece per rank."""
+    case = cases.split_planes_i(cases.reacting_step(scale=0.0625, inner=3), 2)
+    owner = partition_planes([a * b for a, b in zip(case.ni, case.nj)], 4)
+    loads = [sum(a * b for a, b, o in zip(case.ni, case.nj, owner) if o == r) for r in range(4)]
+    assert max(loads) == min(loads)
+    ref = run_case(case, orc, 2)
+    got, stats = _lockstep_run(case, orc, owner, 4, 2)
+    for r in range(4):
+        _owned_planes_equal(case, ref, got[r], owner, r, "q")
+        assert stats[r].status == 0
