@@ -60,7 +60,10 @@ enum {
 /* ---- option enums (values follow checkout.inp where one exists) ------- */
 enum { SCFD_DIM_2D = 0, SCFD_DIM_Q2D = 1 };                   /* checkout_flow.py:105-118 */
 enum { SCFD_DT_GLOBAL = 0, SCFD_DT_LOCAL = 1, SCFD_DT_FIXED = 2 }; /* checkout_flow.py:120-132; FIXED: dt given */
-enum { SCFD_SCHEME_EULER = 0, SCFD_SCHEME_LUSGS = 2, SCFD_SCHEME_NR = 3 }; /* checkout_flow.py:134-181 */
+/* checkout_flow.py:134-181 (the values of its time-scheme line); DUAL is the
+ * Weiss-Smith preconditioned dual time of store/time_scheme/dual/2d (2d, global
+ * or fixed dt, non-reacting: checkout_flow.py:159-168) */
+enum { SCFD_SCHEME_EULER = 0, SCFD_SCHEME_LUSGS = 2, SCFD_SCHEME_NR = 3, SCFD_SCHEME_DUAL = 5 };
 enum { SCFD_RECON_UPWIND = 0, SCFD_RECON_MUSCL = 1 };           /* checkout_flow.py:183-194 */
 enum { SCFD_THERMO_IDEAL = 0, SCFD_THERMO_CHEMKIN_COLD = 1, SCFD_THERMO_CHEMKIN_REACTIVE = 2 };
 enum { SCFD_MU_REFERENCE = 0, SCFD_MU_SUTHERLAND = 1 };        /* ideal gas viscosity law */
@@ -110,7 +113,9 @@ typedef struct scfd_desc {
     double  dt_fixed;              /* dt for SCFD_DT_FIXED                        */
     double  omega_max, omega_min, dq_max, res_rate_warn, res_rate_err; /* NR control */
     int32_t chem_max_substeps;     /* device cap on chemistry substeps per cell   */
-    int32_t reserved[15];
+    int32_t pad0;
+    double  cfl_tau;               /* DUAL: control.inp "InternalLoop CFL tau" (> 0) */
+    int32_t reserved[12];
 } scfd_desc;
 
 typedef struct scfd_bc {
@@ -210,6 +215,18 @@ int  scfd_rms(scfd_ctx* ctx, double* rms);
 int  scfd_download(scfd_ctx* ctx, double* q, double* w, double* vhi, double* tt);
 /* Same as download but for qp (the previous step's q). */
 int  scfd_download_qp(scfd_ctx* ctx, double* qp);
+/* restart.bin / result/result<step>.bin of out_bin (store/core/inout.f90:1-75):
+ * three Fortran sequential-unformatted big-endian records, the step (int32),
+ * tt (float64) and, for every plane, j = 0..nj+1, i = 0..ni+1 (i fastest),
+ * q(1:dimq), w(indxR), w(indxg), w(4).  Before the field is taken the first
+ * ghost layer of q is recomputed from w as set_bc_q does (inout.f90:144-200),
+ * in the written copy only.  SCFD_E_IO if the file cannot be written. */
+int  scfd_write_restart(scfd_ctx* ctx, const char* path, int step);
+/* restart_bin (inout.f90:77-100): reads such a file into q and w(indxR),
+ * w(indxg), w(4) of cells i = 0..ni+1, j = 0..nj+1 (the rest of the state is
+ * kept), sets tt and qp = qpp = q as scfd_upload does, and returns the step.
+ * SCFD_E_IO for a missing, truncated or mis-sized file.  After commit. */
+int  scfd_read_restart(scfd_ctx* ctx, const char* path, int* step, double* tt);
 /* The context's CUDA stream (cudaStream_t as void*), for event timing. */
 int  scfd_get_stream(scfd_ctx* ctx, void** stream);
 /* Number of device kernel launches issued by the last scfd_step/scfd_run. */

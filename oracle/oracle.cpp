@@ -101,6 +101,7 @@ struct orc_ctx {
     double dt_grbl = 0.0, tt = 0.0;
     // store/time_scheme/NR/q2d/var_NR.f90 (superset of var_lusgs)
     FArr Ap, Am, Bp, Bm, alpha, dsci, dscj, vnci, vncj, dpdq, dqdt, Dq;
+    FArr pre1, pre2, pre_sca, phi;  // store/time_scheme/dual/2d/var_dual.f90
     bool first_dual = true;
     double res1 = 0.0, res = 0.0, omega_last = 0.0;
     long long chem_attempts = 0, chem_fallback = 0;
@@ -1353,6 +1354,200 @@ void set_dqdt(orc_ctx& c) {  // NR/q2d/sch_NR.raw.f90:151-180
     }
 }
 
+// set_ABpm of the preconditioned dual time, store/time_scheme/dual/2d/
+// sch_dual.raw.f90:1-209: low-Mach reference velocity, preconditioned spectral
+// radii, pseudo time step from cfl_tau, the scalars and vectors of Gamma^-1,
+// S and S^-1 (pre_sca, pre1, pre2) and the split Jacobians multiplied by
+// Gamma^-1 (a rank-one update, 156-181).
+void set_ABpm_dual(orc_ctx& c) {
+    const int nY = c.nY, D = c.D;
+    for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
+#pragma omp parallel for
+        for (int j = 1; j <= c.nj[p - 1]; ++j)
+            for (int i = 1; i <= c.ni[p - 1]; ++i) {
+                std::vector<double> A(D * D), B(D * D), tA(D), tB(D), At(D * D), Bt(D * D);
+                auto a = [&](int r, int cc) -> double& { return A[(r - 1) + D * (cc - 1)]; };
+                auto b = [&](int r, int cc) -> double& { return B[(r - 1) + D * (cc - 1)]; };
+                const double rho = c.w(1, i, j, p), u = c.w(2, i, j, p), v = c.w(3, i, j, p), pr = c.w(4, i, j, p);
+                const double gamm = c.w(c.indxg, i, j, p), H = c.w(c.indxht, i, j, p);
+                const double cs = std::sqrt(gamm * pr / rho), gmmad = gamm - 1.0, Vs = sq(u) + sq(v);
+                const double unA = c.vnci(1, i, j, p) * u + c.vnci(2, i, j, p) * v;
+                const double unB = c.vncj(1, i, j, p) * u + c.vncj(2, i, j, p) * v;
+                const double Vv = c.w(c.indxMu, i, j, p) / rho / std::min(c.dsci(i, j, p), c.dscj(i, j, p));
+                const double Ur = std::min(std::max(Vv, std::sqrt(Vs)), cs);
+                c.phi(i, j, p) = 1.0 / sq(Ur) - 1.0 / sq(cs);
+                const double alp = 0.5 * (1.0 - sq(Ur / cs));
+                double ud = unA * (1.0 - alp), cd = std::sqrt(sq(alp) * sq(unA) + sq(Ur));
+                const double nuA = std::fabs(ud) + cd;
+                ud = unB * (1.0 - alp);
+                cd = std::sqrt(sq(alp) * sq(unB) + sq(Ur));
+                const double nuB = std::fabs(ud) + cd;
+                const double uds = nuA * (c.dsi(i, j, p) + c.dsi(i - 1, j, p)) + nuB * (c.dsj(i, j, p) + c.dsj(i, j - 1, p));
+                const double dtau = c.d.cfl_tau * c.Vol(i, j, p) / std::max(uds, c.w(c.indxMu, i, j, p) / rho);
+                c.alpha(i, j, p) = 1.0 / (c.Vol(i, j, p) / dtau + c.dsci(i, j, p) * nuA + c.dscj(i, j, p) * nuB);
+                const double beta = 3.0 * c.Vol(i, j, p) / (2.0 * c.DTLG(i, j, p)) * c.alpha(i, j, p);
+                const double ph = c.phi(i, j, p);
+                c.pre_sca(1, i, j, p) = 1.0 + beta;
+                c.pre_sca(2, i, j, p) = -1.0 / (1.0 / ph + sq(cs));
+                c.pre_sca(3, i, j, p) = -1.0 / (1.0 / ph + sq(cs)) / (1.0 / beta + 1.0);
+                c.pre_sca(4, i, j, p) = beta / ((1.0 + beta) / ph + sq(cs));
+                for (int k = 1; k <= nY; ++k) c.pre1(k, i, j, p) = c.w(4 + k, i, j, p);
+                c.pre1(nY + 1, i, j, p) = u;
+                c.pre1(nY + 2, i, j, p) = v;
+                c.pre1(nY + 3, i, j, p) = H;
+                for (int k = 1; k <= nY; ++k) c.pre2(k, i, j, p) = 0.5 * gmmad * Vs + c.DHi(k, i, j, p);
+                c.pre2(nY + 1, i, j, p) = -gmmad * u;
+                c.pre2(nY + 2, i, j, p) = -gmmad * v;
+                c.pre2(nY + 3, i, j, p) = gmmad;
+                // pure A and B, as set_ABpm of LU-SGS (sch_dual.raw.f90:85-154)
+                a(nY + 1, nY + 1) = u * (3.0 - gamm); a(nY + 2, nY + 1) = v; a(nY + 3, nY + 1) = H - sq(u) * gmmad;
+                a(nY + 1, nY + 2) = -v * gmmad; a(nY + 2, nY + 2) = u; a(nY + 3, nY + 2) = -u * v * gmmad;
+                a(nY + 1, nY + 3) = gmmad; a(nY + 2, nY + 3) = 0.0; a(nY + 3, nY + 3) = u * gamm;
+                for (int k = 1; k <= nY; ++k) {
+                    tA[k - 1] = -c.w(4 + k, i, j, p) * u;
+                    a(k, nY + 1) = c.w(4 + k, i, j, p); a(k, nY + 2) = 0.0; a(k, nY + 3) = 0.0;
+                }
+                tA[nY] = -sq(u) + 0.5 * gmmad * Vs;
+                tA[nY + 1] = -u * v;
+                tA[nY + 2] = u * (-H + 0.5 * gmmad * Vs);
+                b(nY + 1, nY + 1) = v; b(nY + 2, nY + 1) = -u * gmmad; b(nY + 3, nY + 1) = -u * v * gmmad;
+                b(nY + 1, nY + 2) = u; b(nY + 2, nY + 2) = v * (3.0 - gamm); b(nY + 3, nY + 2) = H - sq(v) * gmmad;
+                b(nY + 1, nY + 3) = 0.0; b(nY + 2, nY + 3) = gmmad; b(nY + 3, nY + 3) = v * gamm;
+                for (int k = 1; k <= nY; ++k) {
+                    tB[k - 1] = -c.w(4 + k, i, j, p) * v;
+                    b(k, nY + 1) = 0.0; b(k, nY + 2) = c.w(4 + k, i, j, p); b(k, nY + 3) = 0.0;
+                }
+                tB[nY] = -v * u;
+                tB[nY + 1] = -sq(v) + 0.5 * gmmad * Vs;
+                tB[nY + 2] = v * (-H + 0.5 * gmmad * Vs);
+                for (int k = 1; k <= nY; ++k) {
+                    for (int l = 1; l <= nY; ++l) { a(l, k) = tA[l - 1]; b(l, k) = tB[l - 1]; }
+                    a(k, k) = tA[k - 1] + u;
+                    a(nY + 1, k) = tA[nY] + c.DHi(k, i, j, p);
+                    a(nY + 2, k) = tA[nY + 1];
+                    a(nY + 3, k) = tA[nY + 2] + c.DHi(k, i, j, p) * u;
+                    b(k, k) = tB[k - 1] + v;
+                    b(nY + 1, k) = tB[nY];
+                    b(nY + 2, k) = tB[nY + 1] + c.DHi(k, i, j, p);
+                    b(nY + 3, k) = tB[nY + 2] + c.DHi(k, i, j, p) * v;
+                }
+                // multiply Gamma^-1 (156-181)
+                for (int k = 1; k <= D; ++k) {
+                    double ta = 0.0, tb = 0.0;
+                    for (int l = 1; l <= D; ++l) {
+                        ta = ta + c.pre2(l, i, j, p) * a(l, k);
+                        tb = tb + c.pre2(l, i, j, p) * b(l, k);
+                    }
+                    ta = c.pre_sca(2, i, j, p) * ta;
+                    tb = c.pre_sca(2, i, j, p) * tb;
+                    for (int l = 1; l <= D; ++l) {
+                        a(l, k) = a(l, k) + c.pre1(l, i, j, p) * ta;
+                        b(l, k) = b(l, k) + c.pre1(l, i, j, p) * tb;
+                    }
+                }
+                for (int cc = 1; cc <= D; ++cc)
+                    for (int rr = 1; rr <= D; ++rr) {
+                        const double at = c.vnci(1, i, j, p) * a(rr, cc) + c.vnci(2, i, j, p) * b(rr, cc);
+                        c.Ap(rr, cc, i, j, p) = at * 0.5;
+                        c.Am(rr, cc, i, j, p) = at * 0.5;
+                        const double bt = c.vncj(1, i, j, p) * a(rr, cc) + c.vncj(2, i, j, p) * b(rr, cc);
+                        c.Bp(rr, cc, i, j, p) = bt * 0.5;
+                        c.Bm(rr, cc, i, j, p) = bt * 0.5;
+                    }
+                for (int k = 1; k <= D; ++k) {
+                    c.Ap(k, k, i, j, p) = c.Ap(k, k, i, j, p) + nuA * 0.5;
+                    c.Am(k, k, i, j, p) = c.Am(k, k, i, j, p) - nuA * 0.5;
+                    c.Bp(k, k, i, j, p) = c.Bp(k, k, i, j, p) + nuB * 0.5;
+                    c.Bm(k, k, i, j, p) = c.Bm(k, k, i, j, p) - nuB * 0.5;
+                }
+            }
+    }
+}
+
+// The sweeps of time_dual_viscous.f90:1-95 on the owned planes: the RHS
+// multiplied by Gamma^-1, forward sweep with S^-1, the S step, backward sweep
+// with S^-1; returns the plane-local residual and omega candidate (the omega
+// test, relaxation and q update are nr_apply, 96-125).
+void dual_sweeps(orc_ctx& c, double& res_out, double& omega_out) {
+    const int nY = c.nY, D = c.D;
+    auto& Dq = c.Dq;
+    double omega = 1e300, res = 0.0;
+    // Dq += s * (pre2 . Dq) * pre1 at cell (i, j, p)
+    auto rank1 = [&](int s, int i, int j, int p) {
+        double t = 0.0;
+        for (int l = 1; l <= D; ++l) t = t + c.pre2(l, i, j, p) * Dq(l, i, j, p);
+        for (int l = 1; l <= D; ++l) Dq(l, i, j, p) = Dq(l, i, j, p) + c.pre_sca(s, i, j, p) * t * c.pre1(l, i, j, p);
+    };
+    for (int p = 1; p <= c.np; ++p) {
+        if (!c.own(p)) continue;
+        const int ni = c.ni[p - 1], nj = c.nj[p - 1];
+#pragma omp parallel for
+        for (int j = 1; j <= nj; ++j)
+            for (int i = 1; i <= ni; ++i) {
+                for (int k = 1; k <= D; ++k) Dq(k, i, j, p) = rhs_k(c, k, i, j, p) - c.Vol(i, j, p) * c.dqdt(k, i, j, p);
+                rank1(2, i, j, p);
+            }
+        for (int j = 0; j <= nj; ++j)
+            for (int k = 1; k <= D; ++k) Dq(k, 0, j, p) = 0.0;
+        for (int i = 0; i <= ni; ++i)
+            for (int k = 1; k <= D; ++k) Dq(k, i, 0, p) = 0.0;
+        for (int sm = 2; sm <= ni + nj; ++sm) {
+            const int ilo = std::max(1, sm - nj), ihi = std::min(sm - 1, ni);
+#pragma omp parallel for
+            for (int i = ilo; i <= ihi; ++i) {
+                const int j = sm - i;
+                double dqs[SCFD_MAX_SPECIES + 3];
+                for (int k = 1; k <= D; ++k) {
+                    double s1 = 0.0, s2 = 0.0;
+                    for (int l = 1; l <= D; ++l) {
+                        s1 += c.Ap(k, l, i - 1, j, p) * Dq(l, i - 1, j, p);
+                        s2 += c.Bp(k, l, i, j - 1, p) * Dq(l, i, j - 1, p);
+                    }
+                    dqs[k - 1] = c.dsci(i - 1, j, p) * s1 + c.dscj(i, j - 1, p) * s2;
+                }
+                for (int k = 1; k <= D; ++k) Dq(k, i, j, p) = c.alpha(i, j, p) * (Dq(k, i, j, p) + dqs[k - 1]);
+                rank1(4, i, j, p);
+                for (int k = 1; k <= D; ++k) Dq(k, i, j, p) = 1.0 / c.pre_sca(1, i, j, p) * Dq(k, i, j, p);
+            }
+        }
+#pragma omp parallel for
+        for (int j = 1; j <= nj; ++j)
+            for (int i = 1; i <= ni; ++i) {
+                rank1(3, i, j, p);
+                for (int k = 1; k <= D; ++k) Dq(k, i, j, p) = c.pre_sca(1, i, j, p) * Dq(k, i, j, p);
+            }
+        for (int j = 1; j <= nj + 1; ++j)
+            for (int k = 1; k <= D; ++k) Dq(k, ni + 1, j, p) = 0.0;
+        for (int i = 1; i <= ni + 1; ++i)
+            for (int k = 1; k <= D; ++k) Dq(k, i, nj + 1, p) = 0.0;
+        for (int sm = ni + nj; sm >= 2; --sm) {
+            const int ilo = std::max(1, sm - nj), ihi = std::min(sm - 1, ni);
+#pragma omp parallel for reduction(min : omega) reduction(+ : res)
+            for (int i = ilo; i <= ihi; ++i) {
+                const int j = sm - i;
+                double dqs[SCFD_MAX_SPECIES + 3];
+                for (int k = 1; k <= D; ++k) {
+                    double s1 = 0.0, s2 = 0.0;
+                    for (int l = 1; l <= D; ++l) {
+                        s1 += c.Am(k, l, i + 1, j, p) * Dq(l, i + 1, j, p);
+                        s2 += c.Bm(k, l, i, j + 1, p) * Dq(l, i, j + 1, p);
+                    }
+                    dqs[k - 1] = c.dsci(i + 1, j, p) * s1 + c.dscj(i, j + 1, p) * s2;
+                }
+                for (int k = 1; k <= D; ++k) Dq(k, i, j, p) = Dq(k, i, j, p) - c.alpha(i, j, p) * dqs[k - 1];
+                rank1(4, i, j, p);
+                for (int k = 1; k <= D; ++k) Dq(k, i, j, p) = 1.0 / c.pre_sca(1, i, j, p) * Dq(k, i, j, p);
+                res = res + sq(Dq(nY + 3, i, j, p));
+                for (int k = 1; k <= nY; ++k)
+                    if (Dq(k, i, j, p) < 0.0) omega = std::min(omega, -c.q(k, i, j, p) / Dq(k, i, j, p) * c.d.dq_max);
+            }
+        }
+    }
+    res_out = res;
+    omega_out = omega;
+}
+
 // calc_next_step_implicit: LU-SGS/{2d,q2d}/time_lusgs_viscous.f90 and
 // NR/{2d,q2d}/time_NR_viscous.f90:1-109, in two parts: lusgs_sweeps (the
 // sweeps over the owned planes; LU-SGS also updates q there) returns the
@@ -1462,10 +1657,26 @@ int nr_apply(orc_ctx& c, int step_internal, double res, double omega) {
 
 int calc_next_step_implicit(orc_ctx& c, int step_internal) {
     double res, omega;
+    if (c.d.scheme == SCFD_SCHEME_DUAL) {
+        dual_sweeps(c, res, omega);
+        return nr_apply(c, step_internal, res, omega);
+    }
     lusgs_sweeps(c, res, omega);
     if (c.d.scheme != SCFD_SCHEME_NR) return 0;
     return nr_apply(c, step_internal, res, omega);
 }
+
+// the set_ABpm of the configured implicit scheme
+void set_ABpm_scheme(orc_ctx& c) {
+    if (c.d.scheme == SCFD_SCHEME_DUAL)
+        set_ABpm_dual(c);
+    else
+        set_ABpm(c);
+}
+
+// dual time (NR and the preconditioned dual) share the main loop of
+// NR/q2d/main.main.raw.f90 and dual/2d/main.main.raw.f90
+bool dual_time(const orc_ctx& c) { return c.d.scheme == SCFD_SCHEME_NR || c.d.scheme == SCFD_SCHEME_DUAL; }
 
 void copy_arr(FArr& dst, const FArr& src) { dst.v = src.v; }
 
@@ -1508,8 +1719,8 @@ int step(orc_ctx& c, int stepno, scfd_stats* st) {
 int step_body(orc_ctx& c, scfd_stats* st) {
     int s = 0;
     const bool reactive = c.d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
-    if (c.d.scheme == SCFD_SCHEME_NR) {
-        // NR/q2d/main.main.raw.f90:1-20, with proceed_reaction after set_dt as in
+    if (dual_time(c)) {
+        // NR/q2d/main.main.raw.f90:1-20 (dual/2d/main.main.raw.f90:1-20 alike), with proceed_reaction after set_dt as in
         // LU-SGS/q2d/main.main.point_implicit.f90:1-3 when the model is reactive.
         if ((s = part_primitive(c))) return s;
         set_dt(c);
@@ -1521,7 +1732,7 @@ int step_body(orc_ctx& c, scfd_stats* st) {
             if (st) st->inner_iters = j;
             if ((s = part_primitive(c))) return s;
             part_main(c);
-            set_ABpm(c);
+            set_ABpm_scheme(c);
             set_dqdt(c);
             if ((s = calc_next_step_implicit(c, j))) return s;
             ++j;
@@ -1612,7 +1823,7 @@ enum { DS_BEGIN = 0, DS_AFTER_DT, DS_INNER, DS_AFTER_HALO_NR, DS_AFTER_RES, DS_A
 // the halo copies turned into requests.  A status seen on any rank becomes the
 // step's status at the next reduction, where every rank stops together.
 int dstep(orc_ctx& c, scfd_dreq* req, scfd_stats* st) {
-    const bool nr = c.d.scheme == SCFD_SCHEME_NR;
+    const bool nr = dual_time(c);
     const bool reactive = c.d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
     auto keep = [&](int s) { c.ds_status = std::max(c.ds_status, s); };
     auto reduce = [&](int nsum, int nmin, int next) {
@@ -1694,10 +1905,13 @@ int dstep(orc_ctx& c, scfd_dreq* req, scfd_stats* st) {
             case DS_AFTER_HALO_NR: {
                 halo_unpack(c);
                 part_main(c);
-                set_ABpm(c);
+                set_ABpm_scheme(c);
                 set_dqdt(c);
                 double res, om;
-                lusgs_sweeps(c, res, om);
+                if (c.d.scheme == SCFD_SCHEME_DUAL)
+                    dual_sweeps(c, res, om);
+                else
+                    lusgs_sweeps(c, res, om);
                 c.red[0] = res;
                 c.red[1] = om;
                 c.red[2] = -(double)c.ds_status;
@@ -1747,6 +1961,14 @@ int orc_create(const scfd_desc* d, orc_ctx** out) {
     if (!d || !out) return SCFD_E_ARG;
     if (d->abi_version != SCFD_ABI_VERSION) return SCFD_E_ARG;
     if (d->nplane < 1 || d->nplane > SCFD_MAX_PLANES || d->ny < 1 || d->ny > SCFD_MAX_SPECIES) return SCFD_E_ARG;
+    if (d->scheme != SCFD_SCHEME_EULER && d->scheme != SCFD_SCHEME_LUSGS && d->scheme != SCFD_SCHEME_NR &&
+        d->scheme != SCFD_SCHEME_DUAL)
+        return SCFD_E_UNSUPPORTED;
+    if (d->scheme == SCFD_SCHEME_DUAL) {  // checkout_flow.py:159-168; no reacting variant of dual
+        if (d->dim != SCFD_DIM_2D || d->dt_mode == SCFD_DT_LOCAL || d->thermo == SCFD_THERMO_CHEMKIN_REACTIVE)
+            return SCFD_E_UNSUPPORTED;
+        if (!(d->cfl_tau > 0.0)) return SCFD_E_ARG;
+    }
     auto* c = new orc_ctx();
     c->d = *d;
     c->np = d->nplane;
@@ -1796,7 +2018,13 @@ int orc_create(const scfd_desc* d, orc_ctx** out) {
     c->x.init({{0, NI + 1}, {0, NJ + 1}, {1, np}});
     c->r.init({{0, NI + 1}, {0, NJ + 1}, {1, np}});
     c->dt_mat.init({{1, NI}, {1, NJ}, {1, np}});
-    bool impl = d->scheme == SCFD_SCHEME_LUSGS || d->scheme == SCFD_SCHEME_NR;
+    bool impl = d->scheme == SCFD_SCHEME_LUSGS || d->scheme == SCFD_SCHEME_NR || d->scheme == SCFD_SCHEME_DUAL;
+    if (d->scheme == SCFD_SCHEME_DUAL) {
+        c->pre1.init({{1, D}, {1, NI}, {1, NJ}, {1, np}});
+        c->pre2.init({{1, D}, {1, NI}, {1, NJ}, {1, np}});
+        c->pre_sca.init({{1, 4}, {1, NI}, {1, NJ}, {1, np}});
+        c->phi.init({{1, NI}, {1, NJ}, {1, np}});
+    }
     if (impl) {
         c->Ap.init({{1, D}, {1, D}, {0, NI + 1}, {0, NJ + 1}, {1, np}});
         c->Am.init({{1, D}, {1, D}, {0, NI + 1}, {0, NJ + 1}, {1, np}});
@@ -1944,6 +2172,114 @@ int orc_download(orc_ctx* c, double* q, double* w, double* vhi, double* tt) {
     if (q) std::memcpy(q, c->q.v.data(), sizeof(double) * c->q.v.size());
     if (w) std::memcpy(w, c->w.v.data(), sizeof(double) * c->w.v.size());
     if (vhi) std::memcpy(vhi, c->vhi.v.data(), sizeof(double) * c->vhi.v.size());
+    if (tt) *tt = c->tt;
+    return 0;
+}
+
+// out_bin / restart_bin / set_bc_q (store/core/inout.f90:1-200) on the
+// single-process (PC) path: Fortran unformatted sequential records, big-endian.
+static void be_put(std::string& o, const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t k = n; k-- > 0;) o.push_back((char)b[k]);
+}
+static void be_get(const char* in, void* p, size_t n) {
+    unsigned char* b = static_cast<unsigned char*>(p);
+    for (size_t k = 0; k < n; ++k) b[n - 1 - k] = (unsigned char)in[k];
+}
+
+int orc_write_restart(orc_ctx* c, const char* path, int step) {
+    if (!c || !path) return SCFD_E_ARG;
+    if (!c->committed) return SCFD_E_STATE;
+    const int nY = c->nY;
+    FArr q = c->q;  // set_bc_q writes the copy that is written
+    auto bcq = [&](int i, int j, int plane) {  // inout.f90:155-161
+        double tmp = c->w(1, i, j, plane);
+        for (int k = 1; k <= nY; ++k) q(k, i, j, plane) = tmp * c->w(k + 4, i, j, plane);
+        q(nY + 1, i, j, plane) = tmp * c->w(2, i, j, plane);
+        q(nY + 2, i, j, plane) = tmp * c->w(3, i, j, plane);
+        q(nY + 3, i, j, plane) = tmp * c->w(c->indxht, i, j, plane) - c->w(4, i, j, plane);
+    };
+    for (int plane = 1; plane <= c->np; ++plane) {
+        const int ni = c->ni[plane - 1], nj = c->nj[plane - 1];
+        for (int j = 1; j <= nj; ++j) {
+            bcq(0, j, plane);
+            bcq(ni + 1, j, plane);
+        }
+        for (int i = 0; i <= ni + 1; ++i) {
+            bcq(i, 0, plane);
+            bcq(i, nj + 1, plane);
+        }
+    }
+    std::string out, rec;
+    auto record = [&]() {
+        const int32_t n = (int32_t)rec.size();
+        be_put(out, &n, 4);
+        out += rec;
+        be_put(out, &n, 4);
+        rec.clear();
+    };
+    const int32_t s32 = step;
+    be_put(rec, &s32, 4);
+    record();
+    be_put(rec, &c->tt, 8);
+    record();
+    for (int plane = 1; plane <= c->np; ++plane)  // inout.f90:49-51
+        for (int k = 0; k <= c->nj[plane - 1] + 1; ++k)
+            for (int j = 0; j <= c->ni[plane - 1] + 1; ++j) {
+                for (int i = 1; i <= c->D; ++i) be_put(rec, &q(i, j, k, plane), 8);
+                be_put(rec, &c->w(c->indxR, j, k, plane), 8);
+                be_put(rec, &c->w(c->indxg, j, k, plane), 8);
+                be_put(rec, &c->w(4, j, k, plane), 8);
+            }
+    record();
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return SCFD_E_IO;
+    const bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+    return (std::fclose(f) == 0 && ok) ? 0 : SCFD_E_IO;
+}
+
+int orc_read_restart(orc_ctx* c, const char* path, int* step, double* tt) {
+    if (!c || !path || !step) return SCFD_E_ARG;
+    if (!c->committed) return SCFD_E_STATE;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return SCFD_E_IO;
+    std::string buf;
+    char tmp[1 << 16];
+    size_t n;
+    while ((n = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.append(tmp, n);
+    std::fclose(f);
+    std::vector<std::string> recs;
+    for (size_t pos = 0; pos < buf.size();) {
+        int32_t a = 0, b = 0;
+        if (pos + 4 > buf.size()) return SCFD_E_IO;
+        be_get(&buf[pos], &a, 4);
+        if (a < 0 || pos + 8 + (size_t)a > buf.size()) return SCFD_E_IO;
+        be_get(&buf[pos + 4 + a], &b, 4);
+        if (a != b) return SCFD_E_IO;
+        recs.push_back(buf.substr(pos + 4, (size_t)a));
+        pos += 8 + (size_t)a;
+    }
+    size_t need = 0;
+    for (int p = 0; p < c->np; ++p) need += (size_t)(c->ni[p] + 2) * (c->nj[p] + 2) * (c->D + 3) * 8;
+    if (recs.size() != 3 || recs[0].size() != 4 || recs[1].size() != 8 || recs[2].size() != need) return SCFD_E_IO;
+    int32_t s32;
+    be_get(recs[0].data(), &s32, 4);
+    be_get(recs[1].data(), &c->tt, 8);
+    const char* fp = recs[2].data();
+    for (int plane = 1; plane <= c->np; ++plane)  // inout.f90:96-98
+        for (int k = 0; k <= c->nj[plane - 1] + 1; ++k)
+            for (int j = 0; j <= c->ni[plane - 1] + 1; ++j) {
+                for (int i = 1; i <= c->D; ++i, fp += 8) be_get(fp, &c->q(i, j, k, plane), 8);
+                be_get(fp, &c->w(c->indxR, j, k, plane), 8);
+                be_get(fp + 8, &c->w(c->indxg, j, k, plane), 8);
+                be_get(fp + 16, &c->w(4, j, k, plane), 8);
+                fp += 24;
+            }
+    c->qp.v = c->q.v;
+    c->qpp.v = c->q.v;
+    c->first_dual = true;
+    c->ds_stage = 0;
+    *step = s32;
     if (tt) *tt = c->tt;
     return 0;
 }

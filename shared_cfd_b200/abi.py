@@ -22,7 +22,7 @@ STATUS_NAMES = {
 
 DIM_2D, DIM_Q2D = 0, 1
 DT_GLOBAL, DT_LOCAL, DT_FIXED = 0, 1, 2
-SCHEME_EULER, SCHEME_LUSGS, SCHEME_NR = 0, 2, 3
+SCHEME_EULER, SCHEME_LUSGS, SCHEME_NR, SCHEME_DUAL = 0, 2, 3, 5
 RECON_UPWIND, RECON_MUSCL = 0, 1
 THERMO_IDEAL, THERMO_CHEMKIN_COLD, THERMO_CHEMKIN_REACTIVE = 0, 1, 2
 MU_REFERENCE, MU_SUTHERLAND = 0, 1
@@ -59,7 +59,9 @@ class Desc(C.Structure):
         ("omega_max", C.c_double), ("omega_min", C.c_double), ("dq_max", C.c_double),
         ("res_rate_warn", C.c_double), ("res_rate_err", C.c_double),
         ("chem_max_substeps", C.c_int32),
-        ("reserved", C.c_int32 * 15),
+        ("pad0", C.c_int32),
+        ("cfl_tau", C.c_double),
+        ("reserved", C.c_int32 * 12),
     ]
 
 
@@ -169,6 +171,8 @@ SIGNATURES = {
     "rms": (C.c_int, [_P, _D]),
     "download": (C.c_int, [_P, _D, _D, _D, _D]),
     "download_qp": (C.c_int, [_P, _D]),
+    "write_restart": (C.c_int, [_P, C.c_char_p, C.c_int]),
+    "read_restart": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_int), _D]),
     "get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "profile": (C.c_int, [_P, C.c_int]),

@@ -54,6 +54,7 @@ def base_desc(ny=1, dim=abi.DIM_2D, dt_mode=abi.DT_GLOBAL, scheme=abi.SCHEME_EUL
     d.omega_max, d.omega_min, d.dq_max = 1e-1, 1e-3, 1e-2   # NR/q2d/control.part.inp
     d.res_rate_warn, d.res_rate_err = 1e-5, 1e-3
     d.chem_max_substeps = 100000
+    d.cfl_tau = 1e-2                                        # dual/2d/control.part.inp
     return d
 
 

@@ -79,6 +79,55 @@ __device__ __forceinline__ void jac_out(int nY, const CellJ<RT>& cj, const RT* Y
     }
 }
 
+// The preconditioned dual time (dual/2d/sch_dual.raw.f90:156-209): the split
+// Jacobians are (I + s2 p1 p2^T)(n1 A + n2 B)/2 +/- nu/2 with p1 = (Y, u, v, H)
+// and p2 . x = P(x) of the cell (pre1, pre2), so with z = (n1 A + n2 B) x
+// formed as above, A(+/-) x = (z + s2 P(z) p1 +/- nu x) / 2.
+template <typename RT>
+__device__ __forceinline__ RT pfun(int nY, const CellJ<RT>& cj, const RT* DH, const RT* x) {
+    RT P = RT(0);
+    for (int k = 0; k < nY; ++k) P += (cj.hvs + DH[k]) * x[k];
+    return P - cj.g1 * cj.u * x[nY] - cj.g1 * cj.v * x[nY + 1] + cj.g1 * x[nY + 2];
+}
+
+template <typename RT, int D, bool PLUS>
+__device__ __forceinline__ void jac_out_dual(int nY, const CellJ<RT>& cj, RT s2, const RT* Y, const RT* DH,
+                                             const RT* x, RT* oa, RT* ob) {
+    RT S = RT(0);
+    for (int k = 0; k < nY; ++k) S += x[k];
+    const RT P = pfun(nY, cj, DH, x);
+    const RT xmx = x[nY], xmy = x[nY + 1], xE = x[nY + 2];
+    const RT half = RT(0.5);
+    for (int dir = 0; dir < 2; ++dir) {
+        const RT n1 = dir == 0 ? cj.a1 : cj.b1, n2 = dir == 0 ? cj.a2 : cj.b2;
+        const RT nu = dir == 0 ? cj.nuA : cj.nuB, f = half * (dir == 0 ? cj.dsa : cj.dsb);
+        RT* o = dir == 0 ? oa : ob;
+        const RT un = n1 * cj.u + n2 * cj.v;
+        const RT base = n1 * xmx + n2 * xmy - un * S;
+        RT z[D];
+        for (int k = 0; k < nY; ++k) z[k] = Y[k] * base + un * x[k];
+        z[nY] = cj.u * base + un * xmx + n1 * P;
+        z[nY + 1] = cj.v * base + un * xmy + n2 * P;
+        z[nY + 2] = cj.H * base + un * xE + un * P;
+        const RT g = s2 * pfun(nY, cj, DH, z);
+        const RT lam = PLUS ? nu : -nu;
+        for (int k = 0; k < nY; ++k) o[k] = f * (z[k] + g * Y[k] + lam * x[k]);
+        o[nY] = f * (z[nY] + g * cj.u + lam * xmx);
+        o[nY + 1] = f * (z[nY + 1] + g * cj.v + lam * xmy);
+        o[nY + 2] = f * (z[nY + 2] + g * cj.H + lam * xE);
+    }
+}
+
+// x += s * P(x) * p1
+template <typename RT>
+__device__ __forceinline__ void dual_rank1(int nY, const CellJ<RT>& cj, RT s, const RT* Y, const RT* DH, RT* x) {
+    const RT g = s * pfun(nY, cj, DH, x);
+    for (int k = 0; k < nY; ++k) x[k] += g * Y[k];
+    x[nY] += g * cj.u;
+    x[nY + 1] += g * cj.v;
+    x[nY + 2] += g * cj.H;
+}
+
 struct StripList {
     const int2* strips;  // (plane, strip index in plane)
     int n;
@@ -93,7 +142,8 @@ __global__ void __launch_bounds__(128) k_sweep(View v, StripList sl, double* xfe
     const int nY = v.nY, D = v.D;
     const long long N = v.ncell;
     const bool q2d = v.dim == SCFD_DIM_Q2D;
-    const bool nr = v.scheme == SCFD_SCHEME_NR;
+    const bool nr = dual_time_scheme(v.scheme);
+    const bool dual = v.scheme == SCFD_SCHEME_DUAL;
     for (;;) {
         int sid = 0;
         if (lane == 0) sid = atomicAdd(ticket, 1);
@@ -154,12 +204,6 @@ __global__ void __launch_bounds__(128) k_sweep(View v, StripList sl, double* xfe
 #pragma unroll
                     for (int k = 0; k < DMAX; ++k) outA[k] = RT(0);
                 }
-#pragma unroll
-                for (int k = 0; k < DMAX; ++k)
-                    if (k < D) {
-                        const RT rk = RT(v.Dq[k * N + c]);
-                        x[k] = DIR == 0 ? al * (rk + (outA[k] + inB[k])) : rk - al * (outA[k] + inB[k]);
-                    }
                 CellJ<RT> cj;
                 cj.u = RT(v.w[N + c]);
                 cj.v = RT(v.w[2 * N + c]);
@@ -173,6 +217,30 @@ __global__ void __launch_bounds__(128) k_sweep(View v, StripList sl, double* xfe
                         Y[k] = RT(v.w[(4 + k) * N + c]);
                         DH[k] = RT(v.DHi[k * N + c]);
                     }
+                RT s1 = RT(1), s2 = RT(0), s4 = RT(0);
+                if (dual) {
+                    s1 = RT(v.pre[c]);
+                    s2 = RT(v.pre[N + c]);
+                    s4 = RT(v.pre[3 * N + c]);
+                }
+                RT rv[DMAX];
+#pragma unroll
+                for (int k = 0; k < DMAX; ++k) rv[k] = k < D ? RT(v.Dq[k * N + c]) : RT(0);
+                if (DIR == 1 && dual) {
+                    // second step of time_dual_viscous.f90:62-68 (S): Dq += s3 P(Dq) p1, Dq *= s1
+                    dual_rank1(nY, cj, RT(v.pre[2 * N + c]), Y, DH, rv);
+#pragma unroll
+                    for (int k = 0; k < DMAX; ++k) rv[k] = s1 * rv[k];
+                }
+#pragma unroll
+                for (int k = 0; k < DMAX; ++k)
+                    if (k < D) x[k] = DIR == 0 ? al * (rv[k] + (outA[k] + inB[k])) : rv[k] - al * (outA[k] + inB[k]);
+                if (dual) {
+                    // S^-1 after each sweep (time_dual_viscous.f90:50-51, 84-85)
+                    dual_rank1(nY, cj, s4, Y, DH, x);
+#pragma unroll
+                    for (int k = 0; k < DMAX; ++k) x[k] = RT(1) / s1 * x[k];
+                }
                 if (DIR == 0 && q2d) {
                     // semi-implicit axisymmetric pressure source (q2d time_lusgs_viscous.f90:38-44)
                     RT tmp = RT(0);
@@ -190,7 +258,10 @@ __global__ void __launch_bounds__(128) k_sweep(View v, StripList sl, double* xfe
                 cj.a1 = RT(v.vnci[c]); cj.a2 = RT(v.vnci[N + c]);
                 cj.b1 = RT(v.vncj[c]); cj.b2 = RT(v.vncj[N + c]);
                 cj.dsa = RT(v.dsci[c]); cj.dsb = RT(v.dscj[c]);
-                jac_out<RT, DMAX, DIR == 0>(nY, cj, Y, DH, x, outA, outB);
+                if (dual)
+                    jac_out_dual<RT, DMAX, DIR == 0>(nY, cj, s2, Y, DH, x, outA, outB);
+                else
+                    jac_out<RT, DMAX, DIR == 0>(nY, cj, Y, DH, x, outA, outB);
                 if (DIR == 0 || nr || !lusgs_update) {
                     for (int k = 0; k < D; ++k) v.Dq[k * N + c] = double(x[k]);
                 }
@@ -271,9 +342,11 @@ int launch_sweep(const View& v, cudaStream_t s, int dir, double* xfer, int* prog
                  int nstrips_fwd, int nstrips_bwd, const int* strip_tab_f, const int* strip_tab_b) {
     StripList f{(const int2*)strip_tab_f, nstrips_fwd}, b{(const int2*)strip_tab_b, nstrips_bwd};
     const bool mixed = v.precision == SCFD_PREC_MIXED;
-    const int upd = v.scheme == SCFD_SCHEME_NR ? 0 : 1;
-    if (dir == 0 && launch_sweep2(v, s, 0, f.strips, f.n, xfer, progress, tickets, partials, upd)) return 1;
-    if (dir == 1 && launch_sweep2(v, s, 1, b.strips, b.n, xfer, progress + nstrips_fwd, tickets + 1, partials, upd))
+    const int upd = dual_time_scheme(v.scheme) ? 0 : 1;
+    const bool dual = v.scheme == SCFD_SCHEME_DUAL;
+    if (!dual && dir == 0 && launch_sweep2(v, s, 0, f.strips, f.n, xfer, progress, tickets, partials, upd)) return 1;
+    if (!dual && dir == 1 &&
+        launch_sweep2(v, s, 1, b.strips, b.n, xfer, progress + nstrips_fwd, tickets + 1, partials, upd))
         return 1;
     if (dir == 0) {
         if (mixed) launch_rt<float>(v, s, 0, f, xfer, progress, tickets, partials, upd);

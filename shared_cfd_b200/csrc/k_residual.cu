@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(NT) k_residual(View v) {
     for (int k = 0; k < D; ++k) {
         const double src = k == nY + 1 ? area * (sq_my + svq_my) : area * 0.0;
         double rhs = (double)fim[k] - (double)fip[k] + (double)fjm[k] - (double)fjp[k] + src;
-        if (MODE == RES_NR) {
+        if (MODE == RES_NR || MODE == RES_DUAL) {
             const double qk = v.q[k * N + c], qpk = v.qp[k * N + c];
             const double dqdt = first ? (qk - qpk) / dtl : (3.0 * qk - 4.0 * qpk + v.qpp[k * N + c]) / (2.0 * dtl);
             rhs = rhs - vol * dqdt;
@@ -292,6 +292,49 @@ __global__ void __launch_bounds__(NT) k_residual(View v) {
     const double cs = sqrt(gamm * pr / rho);
     const double unA = v.vnci[c] * u + v.vnci[N + c] * vv;
     const double unB = v.vncj[c] * u + v.vncj[N + c] * vv;
+    if (MODE == RES_DUAL) {
+        // set_ABpm of the preconditioned dual time (dual/2d/sch_dual.raw.f90:38-83):
+        // low-Mach reference velocity, preconditioned spectral radii, pseudo time
+        // step from cfl_tau, and the scalars of Gamma^-1, S, S^-1
+        const double mu = v.w[(D + 4) * N + c], dsa = v.dsci[c], dsb = v.dscj[c];
+        const double Vs = u * u + vv * vv;
+        const double Vv = mu / rho / fmin(dsa, dsb);
+        const double Ur = fmin(fmax(Vv, sqrt(Vs)), cs);
+        const double phi = 1.0 / (Ur * Ur) - 1.0 / (cs * cs);
+        const double alp = 0.5 * (1.0 - (Ur / cs) * (Ur / cs));
+        double ud = unA * (1.0 - alp), cd = sqrt(alp * alp * (unA * unA) + Ur * Ur);
+        const double nuA = fabs(ud) + cd;
+        ud = unB * (1.0 - alp);
+        cd = sqrt(alp * alp * (unB * unB) + Ur * Ur);
+        const double nuB = fabs(ud) + cd;
+        const long long cim = cidx(v.P, p, i - 1, j), cjm = cidx(v.P, p, i, j - 1);
+        const double uds = nuA * (v.dsi[c] + v.dsi[cim]) + nuB * (v.dsj[c] + v.dsj[cjm]);
+        const double dtau = v.cfl_tau * vol / fmax(uds, mu / rho);
+        const double al = 1.0 / (vol / dtau + dsa * nuA + dsb * nuB);
+        const double beta = 3.0 * vol / (2.0 * dtl) * al;
+        const double c2 = cs * cs;
+        const double s2 = -1.0 / (1.0 / phi + c2);
+        v.alpha[c] = al;
+        v.nuA[c] = nuA;
+        v.nuB[c] = nuB;
+        v.pre[c] = 1.0 + beta;
+        v.pre[N + c] = s2;
+        v.pre[2 * N + c] = -1.0 / (1.0 / phi + c2) / (1.0 / beta + 1.0);
+        v.pre[3 * N + c] = beta / ((1.0 + beta) / phi + c2);
+        // Dq += pre_sca(2) * (pre2 . Dq) * pre1 (time_dual_viscous.f90:29), pre1 =
+        // (Y, u, v, H), pre2 = (g1 Vs/2 + DHi, -g1 u, -g1 v, g1)
+        const double g1 = gamm - 1.0, H = v.w[(D + 2) * N + c];
+        double t = 0.0;
+        for (int k = 0; k < nY; ++k) t = t + (0.5 * g1 * Vs + v.DHi[k * N + c]) * v.Dq[k * N + c];
+        t = t + (-g1 * u) * v.Dq[nY * N + c];
+        t = t + (-g1 * vv) * v.Dq[(nY + 1) * N + c];
+        t = t + g1 * v.Dq[(nY + 2) * N + c];
+        for (int k = 0; k < nY; ++k) v.Dq[k * N + c] = v.Dq[k * N + c] + s2 * t * v.w[(4 + k) * N + c];
+        v.Dq[nY * N + c] = v.Dq[nY * N + c] + s2 * t * u;
+        v.Dq[(nY + 1) * N + c] = v.Dq[(nY + 1) * N + c] + s2 * t * vv;
+        v.Dq[(nY + 2) * N + c] = v.Dq[(nY + 2) * N + c] + s2 * t * H;
+        return;
+    }
     const double nuA = fabs(unA) + cs, nuB = fabs(unB) + cs;
     const double tmp = MODE == RES_NR ? 3.0 * vol / (2.0 * dtl) + v.dsci[c] * nuA + v.dscj[c] * nuB
                                       : vol / dtl + v.dsci[c] * nuA + v.dscj[c] * nuB;
@@ -322,12 +365,14 @@ static void launch_t(const View& v, cudaStream_t s) {
 // need_coeffs: the caller's sweep reads alpha/nuA/nuB from the cell arrays,
 // which only this generic kernel writes.
 int launch_residual(const View& v, cudaStream_t s, int mode, bool need_coeffs) {
-    if (!need_coeffs && launch_residual2(v, s, mode)) return 1;
+    if (mode != RES_DUAL && !need_coeffs && launch_residual2(v, s, mode)) return 1;
     const bool mixed = v.precision == SCFD_PREC_MIXED;
     if (mode == RES_EULER) {
         if (mixed) launch_t<float, RES_EULER>(v, s); else launch_t<double, RES_EULER>(v, s);
     } else if (mode == RES_LUSGS) {
         if (mixed) launch_t<float, RES_LUSGS>(v, s); else launch_t<double, RES_LUSGS>(v, s);
+    } else if (mode == RES_DUAL) {
+        if (mixed) launch_t<float, RES_DUAL>(v, s); else launch_t<double, RES_DUAL>(v, s);
     } else {
         if (mixed) launch_t<float, RES_NR>(v, s); else launch_t<double, RES_NR>(v, s);
     }

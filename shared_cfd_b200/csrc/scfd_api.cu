@@ -422,6 +422,7 @@ struct Seq {
         timed(c, SCFD_K_COPY, [&] { return (int)(cudaMemcpyAsync(dst, src, qbytes, cudaMemcpyDeviceToDevice, s) ? 0 : 0); });
     }
     void residual(int mode) {
+        if (mode == RES_NR && c->d.scheme == SCFD_SCHEME_DUAL) mode = RES_DUAL;
         const bool coeffs = mode != RES_EULER && !c->use_sw3 && !c->use_sw4;
         n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, mode, coeffs); });
     }
@@ -468,7 +469,7 @@ struct Seq {
             w3.partials = const_cast<double*>(part);
             w3.nstrips = nparts;
             n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, w3, 3, inner); });
-        } else if (c->d.scheme == SCFD_SCHEME_NR) {
+        } else if (dual_time_scheme(c->d.scheme)) {
             n += timed(c, SCFD_K_UPDATE, [&] { return launch_nr_update(v, s, part, nparts, inner); });
         }
     }
@@ -482,7 +483,7 @@ int enqueue_step(scfd_ctx* c) {
     Seq q(c);
     const View& v = c->v;
     const bool reactive = c->d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
-    if (c->d.scheme == SCFD_SCHEME_NR) {
+    if (dual_time_scheme(c->d.scheme)) {
         q.primitive();
         q.setdt();
         if (reactive) q.chem();
@@ -532,10 +533,10 @@ int fill_stats(scfd_ctx* c, scfd_stats* st, long long att0, long long fb0) {
         st->res1 = h.res1;
         st->omega = h.omega;
         st->status = h.status;
-        st->inner_iters = c->d.scheme == SCFD_SCHEME_NR ? std::max(0, c->d.num_internal_loop - 1) : 0;
+        st->inner_iters = dual_time_scheme(c->d.scheme) ? std::max(0, c->d.num_internal_loop - 1) : 0;
         st->chem_attempts = h.chem_attempts - att0;
         st->chem_fallback_cells = h.chem_fallback - fb0;
-        st->res_warn = (c->d.scheme == SCFD_SCHEME_NR && h.res / h.res1 > c->d.res_rate_warn) ? 1 : 0;
+        st->res_warn = (dual_time_scheme(c->d.scheme) && h.res / h.res1 > c->d.res_rate_warn) ? 1 : 0;
     }
     return h.status;
 }
@@ -550,8 +551,14 @@ int scfd_create(const scfd_desc* d, scfd_ctx** out) {
     if (!d || !out) return SCFD_E_ARG;
     if (d->abi_version != SCFD_ABI_VERSION) return SCFD_E_ARG;
     if (d->nplane < 1 || d->nplane > SCFD_MAX_PLANES || d->ny < 1 || d->ny > SCFD_MAX_SPECIES) return SCFD_E_ARG;
-    if (d->scheme != SCFD_SCHEME_EULER && d->scheme != SCFD_SCHEME_LUSGS && d->scheme != SCFD_SCHEME_NR)
+    if (d->scheme != SCFD_SCHEME_EULER && d->scheme != SCFD_SCHEME_LUSGS && d->scheme != SCFD_SCHEME_NR &&
+        d->scheme != SCFD_SCHEME_DUAL)
         return SCFD_E_UNSUPPORTED;
+    if (d->scheme == SCFD_SCHEME_DUAL) {  // checkout_flow.py:159-168; no reacting variant of dual
+        if (d->dim != SCFD_DIM_2D || d->dt_mode == SCFD_DT_LOCAL || d->thermo == SCFD_THERMO_CHEMKIN_REACTIVE)
+            return SCFD_E_UNSUPPORTED;
+        if (!(d->cfl_tau > 0.0)) return SCFD_E_ARG;
+    }
     if (d->thermo == SCFD_THERMO_IDEAL && d->ny != 1) return SCFD_E_ARG;
     if (d->thermo == SCFD_THERMO_CHEMKIN_REACTIVE && d->dt_mode == SCFD_DT_LOCAL) return SCFD_E_UNSUPPORTED;
     auto* c = new scfd_ctx();
@@ -734,14 +741,15 @@ int scfd_commit(scfd_ctx* c) {
     const ChemTables tabs = c->have_chem ? ChemTables(c->chem) : ChemTables();
     const int nrec = 64 * c->np;
     // strip records for the TMA-streamed sweeps
-    const size_t blk3 = impl ? sweep3_record_elems(nY, mixed) : 0;
+    const bool dual = c->d.scheme == SCFD_SCHEME_DUAL;
+    const size_t blk3 = impl && !dual ? sweep3_record_elems(nY, mixed) : 0;
     const size_t esz3 = mixed ? sizeof(float) : sizeof(double);
     const char* sweep_env = std::getenv("SCFD_SWEEP");
     const bool legacy = std::getenv("SCFD_SWEEP_LEGACY") != nullptr;
     const char* graph_env = std::getenv("SCFD_GRAPH");
     c->use_graph = !(graph_env && std::strcmp(graph_env, "0") == 0);
     int qc4 = 0;
-    const size_t blk4 = impl ? sweep4_record_elems(nY, mixed, &qc4) : 0;
+    const size_t blk4 = impl && !dual ? sweep4_record_elems(nY, mixed, &qc4) : 0;
     c->use_sw4 = blk4 > 0 && !legacy && sweep_env && std::strcmp(sweep_env, "4") == 0 && c->owner.empty();
     c->use_sw3 = blk3 > 0 && !legacy && !c->use_sw4;
     // quad-per-cell sweeps: strips of R rows, tasks of up to WPC strips
@@ -802,6 +810,7 @@ int scfd_commit(scfd_ctx* c) {
     bytes += need<double>(W * N) + 2 * need<double>(nY * N);  // w, vhi, DHi
     bytes += need<double>(D * N);                             // Dq
     bytes += 4 * need<double>(N);                             // dt_mat, alpha, nuA, nuB
+    if (dual) bytes += need<double>(4 * N);                   // pre_sca
     bytes += 8 * need<double>(N) + 4 * need<double>(2 * N) + 3 * need<double>(4 * N);  // geometry
     if (mixed) bytes += need<float>(W * N) + need<float>(nY * N);
     bytes += need<DevScalars>(1);
@@ -843,6 +852,8 @@ int scfd_commit(scfd_ctx* c) {
     v.w = carve<double>(p, W * N); v.vhi = carve<double>(p, nY * N); v.DHi = carve<double>(p, nY * N);
     v.Dq = carve<double>(p, D * N);
     v.dt_mat = carve<double>(p, N); v.alpha = carve<double>(p, N); v.nuA = carve<double>(p, N); v.nuB = carve<double>(p, N);
+    v.pre = dual ? carve<double>(p, 4 * N) : nullptr;
+    v.cfl_tau = c->d.cfl_tau;
     v.Vol = carve<double>(p, N); v.Area = carve<double>(p, N); v.dsi = carve<double>(p, N); v.dsj = carve<double>(p, N);
     v.x = carve<double>(p, N); v.r = carve<double>(p, N); v.dsci = carve<double>(p, N); v.dscj = carve<double>(p, N);
     v.vni = carve<double>(p, 2 * N); v.vnj = carve<double>(p, 2 * N); v.vnci = carve<double>(p, 2 * N); v.vncj = carve<double>(p, 2 * N);
@@ -1156,7 +1167,7 @@ int scfd_dstep(scfd_ctx* c, int step, scfd_dreq* req, scfd_stats* stats) {
     req->buf = nullptr;
     if (!c->committed || !c->uploaded) return c->fail(SCFD_E_STATE, "dstep before upload");
     (void)step;
-    const bool nr = c->d.scheme == SCFD_SCHEME_NR;
+    const bool nr = dual_time_scheme(c->d.scheme);
     const bool reactive = c->d.thermo == SCFD_THERMO_CHEMKIN_REACTIVE;
     const View& v = c->v;
     cudaStream_t s = c->stream;
@@ -1283,6 +1294,135 @@ int scfd_download(scfd_ctx* c, double* q, double* w, double* vhi, double* tt) {
         if ((st = sync_scalars(c))) return st;
         *tt = c->h_sc->tt;
     }
+    return 0;
+}
+
+// ---- restart.bin (store/core/inout.f90) -----------------------------------
+// Fortran sequential unformatted, big-endian (the reference compiles with
+// -fconvert=big-endian): every record is [int32 n][n bytes][int32 n].
+static void put_be(std::string& out, const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    for (size_t k = 0; k < n; ++k) out.push_back((char)b[n - 1 - k]);
+}
+static void get_be(const char* in, void* p, size_t n) {
+    unsigned char* b = static_cast<unsigned char*>(p);
+    for (size_t k = 0; k < n; ++k) b[n - 1 - k] = (unsigned char)in[k];
+}
+static void put_record(std::string& out, const std::string& payload) {
+    const int32_t n = (int32_t)payload.size();
+    put_be(out, &n, 4);
+    out += payload;
+    put_be(out, &n, 4);
+}
+
+int scfd_write_restart(scfd_ctx* c, const char* path, int step) {
+    if (!c || !path) return SCFD_E_ARG;
+    if (!c->committed) return c->fail(SCFD_E_STATE, "write_restart before commit");
+    const int D = c->D, W = c->W, nY = c->nY, IX = c->nimax + 4, JX = c->njmax + 4;
+    const size_t cells = (size_t)IX * JX * c->np;
+    std::vector<double> q(cells * D), w(cells * W);
+    double tt = 0.0;
+    int st = scfd_download(c, q.data(), w.data(), nullptr, &tt);
+    if (st) return st;
+    auto at = [&](int p, int i, int j) { return (size_t)(i + 1) + (size_t)IX * ((size_t)(j + 1) + (size_t)JX * p); };
+    const int ig = D + 1, iht = D + 2, iR = D + 3;  // 0-based indxg, indxht, indxR
+    // set_bc_q: the first ghost layer of q from w (inout.f90:151-198)
+    auto bc_q = [&](int p, int i, int j) {
+        const size_t c0 = at(p, i, j);
+        const double* wc = &w[c0 * W];
+        double* qc = &q[c0 * D];
+        const double tmp = wc[0];
+        for (int k = 0; k < nY; ++k) qc[k] = tmp * wc[k + 4];
+        qc[nY] = tmp * wc[1];
+        qc[nY + 1] = tmp * wc[2];
+        qc[nY + 2] = tmp * wc[iht] - wc[3];
+    };
+    for (int p = 0; p < c->np; ++p) {
+        const int ni = c->P.ni[p], nj = c->P.nj[p];
+        for (int j = 1; j <= nj; ++j) {
+            bc_q(p, 0, j);
+            bc_q(p, ni + 1, j);
+        }
+        for (int i = 0; i <= ni + 1; ++i) {
+            bc_q(p, i, 0);
+            bc_q(p, i, nj + 1);
+        }
+    }
+    std::string field;
+    for (int p = 0; p < c->np; ++p)
+        for (int j = 0; j <= c->P.nj[p] + 1; ++j)
+            for (int i = 0; i <= c->P.ni[p] + 1; ++i) {
+                const size_t c0 = at(p, i, j);
+                for (int k = 0; k < D; ++k) put_be(field, &q[c0 * D + k], 8);
+                put_be(field, &w[c0 * W + iR], 8);
+                put_be(field, &w[c0 * W + ig], 8);
+                put_be(field, &w[c0 * W + 3], 8);
+            }
+    std::string out, rec;
+    const int32_t s32 = step;
+    put_be(rec, &s32, 4);
+    put_record(out, rec);
+    rec.clear();
+    put_be(rec, &tt, 8);
+    put_record(out, rec);
+    put_record(out, field);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return c->fail(SCFD_E_IO, std::string("cannot open ") + path);
+    const size_t wr = std::fwrite(out.data(), 1, out.size(), f);
+    const int cl = std::fclose(f);
+    if (wr != out.size() || cl != 0) return c->fail(SCFD_E_IO, std::string("cannot write ") + path);
+    return 0;
+}
+
+int scfd_read_restart(scfd_ctx* c, const char* path, int* step, double* tt) {
+    if (!c || !path || !step) return SCFD_E_ARG;
+    if (!c->committed) return c->fail(SCFD_E_STATE, "read_restart before commit");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return c->fail(SCFD_E_IO, std::string("cannot open ") + path);
+    std::string buf;
+    char tmp[1 << 16];
+    size_t n;
+    while ((n = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.append(tmp, n);
+    std::fclose(f);
+    std::vector<std::pair<size_t, size_t>> recs;  // offset, length
+    for (size_t pos = 0; pos < buf.size();) {
+        int32_t a = 0, b = 0;
+        if (pos + 4 > buf.size()) return c->fail(SCFD_E_IO, "truncated record marker");
+        get_be(&buf[pos], &a, 4);
+        if (a < 0 || pos + 8 + (size_t)a > buf.size()) return c->fail(SCFD_E_IO, "truncated record");
+        get_be(&buf[pos + 4 + a], &b, 4);
+        if (a != b) return c->fail(SCFD_E_IO, "record markers disagree");
+        recs.push_back({pos + 4, (size_t)a});
+        pos += 8 + (size_t)a;
+    }
+    const int D = c->D, W = c->W, IX = c->nimax + 4, JX = c->njmax + 4;
+    size_t need = 0;
+    for (int p = 0; p < c->np; ++p) need += (size_t)(c->P.ni[p] + 2) * (c->P.nj[p] + 2) * (D + 3) * 8;
+    if (recs.size() != 3 || recs[0].second != 4 || recs[1].second != 8 || recs[2].second != need)
+        return c->fail(SCFD_E_IO, "restart file does not match the case");
+    int32_t s32 = 0;
+    double t = 0.0;
+    get_be(&buf[recs[0].first], &s32, 4);
+    get_be(&buf[recs[1].first], &t, 8);
+    const size_t cells = (size_t)IX * JX * c->np;
+    std::vector<double> q(cells * D), w(cells * W);
+    int st = scfd_download(c, q.data(), w.data(), nullptr, nullptr);
+    if (st) return st;
+    const char* fp = &buf[recs[2].first];
+    const int ig = D + 1, iR = D + 3;
+    for (int p = 0; p < c->np; ++p)
+        for (int j = 0; j <= c->P.nj[p] + 1; ++j)
+            for (int i = 0; i <= c->P.ni[p] + 1; ++i) {
+                const size_t c0 = (size_t)(i + 1) + (size_t)IX * ((size_t)(j + 1) + (size_t)JX * p);
+                for (int k = 0; k < D; ++k, fp += 8) get_be(fp, &q[c0 * D + k], 8);
+                get_be(fp, &w[c0 * W + iR], 8);
+                get_be(fp + 8, &w[c0 * W + ig], 8);
+                get_be(fp + 16, &w[c0 * W + 3], 8);
+                fp += 24;
+            }
+    if ((st = scfd_upload(c, q.data(), w.data(), nullptr, t))) return st;
+    *step = s32;
+    if (tt) *tt = t;
     return 0;
 }
 

@@ -89,9 +89,11 @@ struct View {
     int dim, viscous, recon, thermo, mu_model, scheme, dt_mode, precision;
     double phi_mus, k_mus, kappa, rgas, nu_gas, suth_mu0, suth_t0, suth_s, prandtl, schmidt, cfl, dt_fixed;
     double omega_max, omega_min, dq_max;
+    double cfl_tau;              // DUAL: pseudo-time CFL
     // state
     double *q, *qp, *qpp, *w, *vhi, *DHi, *Dq, *dt_mat;
     double *alpha, *nuA, *nuB;   // LU-SGS coefficients per cell
+    double* pre;                 // DUAL: pre_sca(1..4) per cell, pre[k * ncell + c]
     // geometry
     double *Vol, *Area, *dsi, *dsj, *vni, *vnj, *x, *r, *gjc, *gji, *gjj, *dsci, *dscj, *vnci, *vncj;
     // mixed-precision copies used by the FP32 residual / sweeps
@@ -190,7 +192,13 @@ int launch_res_import(const View& v, cudaStream_t s, const double* red, int inne
 int launch_status_export(const View& v, cudaStream_t s, double* red);    // red = [-status]
 int launch_status_import(const View& v, cudaStream_t s, const double* red);
 
-// residual modes
-enum { RES_EULER = 0, RES_LUSGS = 1, RES_NR = 2 };
+// residual modes (RES_DUAL: NR's right-hand side multiplied by Gamma^-1 and the
+// coefficients of the preconditioned dual time)
+enum { RES_EULER = 0, RES_LUSGS = 1, RES_NR = 2, RES_DUAL = 3 };
+
+// NR and the preconditioned dual time share the dual-time main loop
+__host__ __device__ inline bool dual_time_scheme(int scheme) {
+    return scheme == SCFD_SCHEME_NR || scheme == SCFD_SCHEME_DUAL;
+}
 
 }  // namespace scfd

@@ -184,6 +184,16 @@ class Solver:
         self._check(self.lib.download_qp(self.ctx, abi.dptr(qp)), "download_qp")
         return qp
 
+    def write_restart(self, path, step):
+        """restart.bin / result file of out_bin (store/core/inout.f90:1-75)."""
+        self._check(self.lib.write_restart(self.ctx, os.fsencode(path), step), "write_restart")
+
+    def read_restart(self, path):
+        """restart_bin (inout.f90:77-100); returns (step, tt)."""
+        step, tt = C.c_int(), C.c_double()
+        self._check(self.lib.read_restart(self.ctx, os.fsencode(path), C.byref(step), C.byref(tt)), "read_restart")
+        return step.value, tt.value
+
     def stream(self):
         s = C.c_void_p()
         self._check(self.lib.get_stream(self.ctx, C.byref(s)), "get_stream")
