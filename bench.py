@@ -217,14 +217,18 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def cpu_reference(config, scale, steps, cores):
-    """The CPU restatement of the reference (OpenMP on the host cores)."""
+def cpu_reference(config, scale, steps, cores, threads=None):
+    """The CPU restatement of the reference (OpenMP on the host cores; `threads`
+    caps the OpenMP team of this and later runs)."""
     from shared_cfd_b200.solver import Solver
     so = os.path.join(ROOT, "oracle", "_build", "liborc.so")
     if not os.path.exists(so):
         subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
     os.environ["OMP_NUM_THREADS"] = str(cores)
     orc = abi.Bound(C.CDLL(so), "orc_")
+    if threads is not None:
+        import ctypes.util
+        C.CDLL(ctypes.util.find_library("gomp") or "libgomp.so.1").omp_set_num_threads(threads)
     case = make_case(config, scale, abi.PREC_FP64)
     s = Solver(case, lib=orc)
     s.upload()
@@ -540,6 +544,11 @@ def main():
             cpu = {"value": v, "unit": "Mcell-iter/s", "cores": cores, "kind": "port",
                    "sample": "%d physical step(s) of the full workload (%.1f s) on %d OpenMP threads, "
                              "C++ FP64 restatement" % (args.cpu_steps, dt, cores)}
+            # one core, on a quarter-resolution sample of the same case (1/16 of the cells)
+            v1, dt1, c1 = cpu_reference(args.config, args.scale * 0.25, 1, cores, threads=1)
+            cpu["single_core"] = {"value": v1, "unit": "Mcell-iter/s", "cores": 1,
+                                  "sample": "1 physical step of the workload at quarter resolution per "
+                                            "direction (%d cells, %.1f s) on 1 thread" % (c1.ncells, dt1)}
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "Mcell-iter/s", "cores": cores, "kind": "port", "sample": "failed: %s" % e}
 

@@ -227,6 +227,10 @@ int  scfd_write_restart(scfd_ctx* ctx, const char* path, int step);
  * kept), sets tt and qp = qpp = q as scfd_upload does, and returns the step.
  * SCFD_E_IO for a missing, truncated or mis-sized file.  After commit. */
 int  scfd_read_restart(scfd_ctx* ctx, const char* path, int* step, double* tt);
+/* geometry.bin of out_geo_bin (store/dim/2d/geometry.f90:182-193): per plane
+ * the records ni, nj (int32) and (xh, rh) of nodes i = 0..ni, j = 0..nj
+ * (i fastest), big-endian.  After scfd_set_geometry of every plane. */
+int  scfd_write_geometry(scfd_ctx* ctx, const char* path);
 /* The context's CUDA stream (cudaStream_t as void*), for event timing. */
 int  scfd_get_stream(scfd_ctx* ctx, void** stream);
 /* Number of device kernel launches issued by the last scfd_step/scfd_run. */

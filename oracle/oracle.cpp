@@ -2238,6 +2238,37 @@ int orc_write_restart(orc_ctx* c, const char* path, int step) {
     return (std::fclose(f) == 0 && ok) ? 0 : SCFD_E_IO;
 }
 
+int orc_write_geometry(orc_ctx* c, const char* path) {  // out_geo_bin, geometry.f90:182-193
+    if (!c || !path) return SCFD_E_ARG;
+    for (int p = 0; p < c->np; ++p)
+        if (!c->geo_set[p]) return SCFD_E_STATE;
+    std::string out, rec;
+    auto record = [&]() {
+        const int32_t n = (int32_t)rec.size();
+        be_put(out, &n, 4);
+        out += rec;
+        be_put(out, &n, 4);
+        rec.clear();
+    };
+    for (int plane = 1; plane <= c->np; ++plane) {
+        const int32_t ni = c->ni[plane - 1], nj = c->nj[plane - 1];
+        be_put(rec, &ni, 4);
+        record();
+        be_put(rec, &nj, 4);
+        record();
+        for (int j = 0; j <= nj; ++j)
+            for (int i = 0; i <= ni; ++i) {
+                be_put(rec, &c->xh(i, j, plane), 8);
+                be_put(rec, &c->rh(i, j, plane), 8);
+            }
+        record();
+    }
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return SCFD_E_IO;
+    const bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+    return (std::fclose(f) == 0 && ok) ? 0 : SCFD_E_IO;
+}
+
 int orc_read_restart(orc_ctx* c, const char* path, int* step, double* tt) {
     if (!c || !path || !step) return SCFD_E_ARG;
     if (!c->committed) return SCFD_E_STATE;

@@ -173,6 +173,7 @@ SIGNATURES = {
     "download_qp": (C.c_int, [_P, _D]),
     "write_restart": (C.c_int, [_P, C.c_char_p, C.c_int]),
     "read_restart": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_int), _D]),
+    "write_geometry": (C.c_int, [_P, C.c_char_p]),
     "get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "profile": (C.c_int, [_P, C.c_int]),

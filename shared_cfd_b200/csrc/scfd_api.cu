@@ -1374,6 +1374,35 @@ int scfd_write_restart(scfd_ctx* c, const char* path, int step) {
     return 0;
 }
 
+int scfd_write_geometry(scfd_ctx* c, const char* path) {
+    if (!c || !path) return SCFD_E_ARG;
+    for (int p = 0; p < c->np; ++p)
+        if (!c->geo_set[p]) return c->fail(SCFD_E_STATE, "geometry of plane " + std::to_string(p + 1) + " not set");
+    std::string out, rec;
+    for (int p = 0; p < c->np; ++p) {
+        const int32_t ni = c->P.ni[p], nj = c->P.nj[p];
+        for (const int32_t n : {ni, nj}) {
+            rec.clear();
+            put_be(rec, &n, 4);
+            put_record(out, rec);
+        }
+        rec.clear();
+        for (int j = 0; j <= nj; ++j)
+            for (int i = 0; i <= ni; ++i) {
+                const size_t k = (size_t)i + (size_t)(ni + 1) * j;
+                put_be(rec, &c->xh[p][k], 8);
+                put_be(rec, &c->rh[p][k], 8);
+            }
+        put_record(out, rec);
+    }
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return c->fail(SCFD_E_IO, std::string("cannot open ") + path);
+    const size_t wr = std::fwrite(out.data(), 1, out.size(), f);
+    const int cl = std::fclose(f);
+    if (wr != out.size() || cl != 0) return c->fail(SCFD_E_IO, std::string("cannot write ") + path);
+    return 0;
+}
+
 int scfd_read_restart(scfd_ctx* c, const char* path, int* step, double* tt) {
     if (!c || !path || !step) return SCFD_E_ARG;
     if (!c->committed) return c->fail(SCFD_E_STATE, "read_restart before commit");

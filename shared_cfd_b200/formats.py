@@ -152,6 +152,25 @@ def restart_bytes(step, tt, cells):
     return _record(struct.pack(">i", step)) + _record(struct.pack(">d", tt)) + _record(field)
 
 
+def read_geometry_bin(path):
+    """geometry.bin of out_geo_bin (store/dim/2d/geometry.f90:182-193): a list
+    of (xh, rh) node arrays of shape (ni+1, nj+1)."""
+    with open(path, "rb") as f:
+        recs = _read_records(f.read())
+    if len(recs) % 3:
+        raise ValueError("geometry.bin holds %d records, not three per plane" % len(recs))
+    planes = []
+    for k in range(0, len(recs), 3):
+        (ni,) = struct.unpack(">i", recs[k])
+        (nj,) = struct.unpack(">i", recs[k + 1])
+        arr = np.frombuffer(recs[k + 2], dtype=">f8").astype(np.float64)
+        if arr.size != 2 * (ni + 1) * (nj + 1):
+            raise ValueError("plane %d: node record size" % (k // 3 + 1))
+        xr = arr.reshape(nj + 1, ni + 1, 2)
+        planes.append((xr[..., 0].T.copy(), xr[..., 1].T.copy()))
+    return planes
+
+
 def write_restart(path, step, tt, cells):
     with open(path, "wb") as f:
         f.write(restart_bytes(step, tt, cells))

@@ -194,6 +194,10 @@ class Solver:
         self._check(self.lib.read_restart(self.ctx, os.fsencode(path), C.byref(step), C.byref(tt)), "read_restart")
         return step.value, tt.value
 
+    def write_geometry(self, path):
+        """geometry.bin of out_geo_bin (store/dim/2d/geometry.f90:182-193)."""
+        self._check(self.lib.write_geometry(self.ctx, os.fsencode(path)), "write_geometry")
+
     def stream(self):
         s = C.c_void_p()
         self._check(self.lib.get_stream(self.ctx, C.byref(s)), "get_stream")

@@ -58,3 +58,14 @@ def test_restart_after_gpu_steps(gpu, tmp_path):
             t.close()
     finally:
         s.close()
+
+
+def test_geometry_bin_equals_restatement(gpu, orc, tmp_path):
+    case = cases.reacting_step(scale=0.0625)
+    for lib, tag in ((gpu, "gpu"), (orc, "orc")):
+        s = Solver(case, lib=lib)
+        try:
+            s.write_geometry(str(tmp_path / ("%s.bin" % tag)))
+        finally:
+            s.close()
+    assert (tmp_path / "gpu.bin").read_bytes() == (tmp_path / "orc.bin").read_bytes()

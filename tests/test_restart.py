@@ -106,3 +106,18 @@ def test_restart_errors(stepped, orc, tmp_path):
         s.write_restart(str(tmp_path / "no" / "such" / "dir.bin"), 1)
     assert e.value.code == abi.E_IO
     assert s.lib.read_restart(s.ctx, b"x", None, None) == abi.E_ARG
+
+
+def test_write_geometry_bin(orc, tmp_path):
+    case = cases.reacting_step(scale=0.03)
+    s = Solver(case, lib=orc)
+    try:
+        s.write_geometry(str(tmp_path / "geometry.bin"))
+    finally:
+        s.close()
+    back = F.read_geometry_bin(str(tmp_path / "geometry.bin"))
+    assert len(back) == 4
+    for (xh, rh), (x2, r2) in zip(case.planes, back):
+        assert np.array_equal(xh, x2) and np.array_equal(rh, r2)
+    raw = (tmp_path / "geometry.bin").read_bytes()
+    assert raw[:12] == (4).to_bytes(4, "big") + case.ni[0].to_bytes(4, "big") + (4).to_bytes(4, "big")
