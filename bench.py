@@ -473,6 +473,7 @@ def main():
         # strong scaling under sharding: the ranks share one workload
         units = case.ncells * iters_per_step(case) * args.steps * (1 if sharded else world)
         res[tag] = {"ms": ms, "value": units / (ms * 1e-3) / 1e6, "launches": nl, "clocks": clk,
+                    "autotune": s.tuning(),
                     "status": st.status, "res_warn": st.res_warn, "omega": st.omega,
                     "chem_attempts": st.chem_attempts, "chem_fallback": st.chem_fallback_cells}
         solvers[tag] = (s, case)
@@ -569,6 +570,7 @@ def main():
             "mixed_over_fp64": m["value"] / res["fp64"]["value"],
             "l2_mixed_vs_fp64": l2_mixed,
             "e2e": e2e, "gpu_launches": m["launches"],
+            "autotune": {"mixed": m["autotune"], "fp64": res["fp64"]["autotune"]},
             "clocks": m["clocks"], "roofline": roofline, "cpu_baseline": cpu,
             "status": {"mixed": m["status"], "fp64": res["fp64"]["status"], "res_warn": m["res_warn"],
                        "omega": m["omega"], "chem_attempts": m["chem_attempts"], "chem_fallback_cells": m["chem_fallback"]},

@@ -245,6 +245,13 @@ enum {
     SCFD_K_COUNT
 };
 int  scfd_profile(scfd_ctx* ctx, int enable);
+/* The launch shapes the autotuner picked for this context, as a JSON object
+ * (residual tile shape, thermo CTA size, the device time of every candidate).
+ * The tuner runs once per context, before its first step: each candidate is
+ * timed with CUDA events on the context's own state (saved before and
+ * restored after) and the fastest is kept; the candidates compute the same
+ * values.  SCFD_AUTOTUNE=0 in the environment keeps the default shapes. */
+int  scfd_tuning(scfd_ctx* ctx, char* json, int len);
 int  scfd_kernel_stats(scfd_ctx* ctx, int kind, double* total_ms, int64_t* launches, char* name, int namelen);
 
 /* ---- block-sharded step over several processes (one GPU each) -------------

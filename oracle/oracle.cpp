@@ -2333,6 +2333,12 @@ int orc_launch_count(const orc_ctx* c, int64_t* n) {
     return 0;
 }
 
+int orc_tuning(orc_ctx* c, char* json, int len) {  // no launch shapes on the CPU
+    if (!c || !json || len <= 0) return SCFD_E_ARG;
+    std::snprintf(json, (size_t)len, "{\"enabled\": false}");
+    return 0;
+}
+
 int orc_profile(orc_ctx* c, int enable) {
     (void)enable;
     return c ? 0 : SCFD_E_ARG;

@@ -177,6 +177,7 @@ SIGNATURES = {
     "get_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "profile": (C.c_int, [_P, C.c_int]),
+    "tuning": (C.c_int, [_P, C.c_char_p, C.c_int]),
     "kernel_stats": (C.c_int, [_P, C.c_int, _D, C.POINTER(C.c_int64), C.c_char_p, C.c_int]),
     "set_partition": (C.c_int, [_P, C.POINTER(C.c_int32), C.c_int, C.c_int]),
     "dstep": (C.c_int, [_P, C.c_int, C.POINTER(DReq), C.POINTER(Stats)]),

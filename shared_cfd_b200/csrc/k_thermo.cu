@@ -117,7 +117,7 @@ __device__ int dev_calc_T(const DevChem& ch, const double* vrho, double rho, dou
     return 0;
 }
 
-__global__ void __launch_bounds__(128) k_thermo(View v) {
+__global__ void __launch_bounds__(256) k_thermo(View v) {
     const int p = v.P.act[blockIdx.y];
     const int ni = v.P.ni[p], nj = v.P.nj[p];
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -179,8 +179,9 @@ __global__ void __launch_bounds__(128) k_thermo(View v) {
 
 int launch_thermo(const View& v, cudaStream_t s, int cells_per_plane_max) {
     if (v.P.nact == 0) return 0;
-    dim3 grid((cells_per_plane_max + 127) / 128, v.P.nact);
-    k_thermo<<<grid, 128, 0, s>>>(v);
+    const int bs = v.thermo_block == 64 || v.thermo_block == 256 ? v.thermo_block : 128;
+    dim3 grid((cells_per_plane_max + bs - 1) / bs, v.P.nact);
+    k_thermo<<<grid, bs, 0, s>>>(v);
     return 1;
 }
 

@@ -94,6 +94,9 @@ struct scfd_ctx {
     int ds_stage = 0, ds_j = 0;
     long long ds_att0 = 0, ds_fb0 = 0;
     bool own(int p) const { return owner.empty() || owner[p] == rank; }  // p 0-based
+    // autotuner (launch shapes of the residual and thermo kernels)
+    bool tuned = false;
+    std::string tune_report = "{}";
 
     int fail(int code, const std::string& m) {
         err = m;
@@ -854,6 +857,8 @@ int scfd_commit(scfd_ctx* c) {
     v.dt_mat = carve<double>(p, N); v.alpha = carve<double>(p, N); v.nuA = carve<double>(p, N); v.nuB = carve<double>(p, N);
     v.pre = dual ? carve<double>(p, 4 * N) : nullptr;
     v.cfl_tau = c->d.cfl_tau;
+    v.res_tile = 0;
+    v.thermo_block = 128;
     v.Vol = carve<double>(p, N); v.Area = carve<double>(p, N); v.dsi = carve<double>(p, N); v.dsj = carve<double>(p, N);
     v.x = carve<double>(p, N); v.r = carve<double>(p, N); v.dsci = carve<double>(p, N); v.dscj = carve<double>(p, N);
     v.vni = carve<double>(p, 2 * N); v.vnj = carve<double>(p, 2 * N); v.vnci = carve<double>(p, 2 * N); v.vncj = carve<double>(p, 2 * N);
@@ -1078,6 +1083,104 @@ int scfd_prepare(scfd_ctx* c, int step) {
     return c->h_sc->status;
 }
 
+// ---------------------------------------------------------------------------
+// Autotuner: picks the residual tile shape and the thermo CTA size for this
+// context by timing every candidate (CUDA events, 1 warm-up + 3 timed launches)
+// on the context's state.  The kernels under test overwrite q..nuB and the
+// scalars, which are saved first and restored after.  Runs once, before the
+// first step is enqueued (so a captured graph holds the chosen shapes).
+// ---------------------------------------------------------------------------
+static int autotune(scfd_ctx* c) {
+    c->tuned = true;
+    View& v = c->v;
+    v.res_tile = 0;
+    v.thermo_block = 128;
+    const char* env = std::getenv("SCFD_AUTOTUNE");
+    if (env && std::strcmp(env, "0") == 0) {
+        c->tune_report = "{\"enabled\": false, \"residual_tile\": \"32x8\", \"thermo_block\": 128}";
+        return 0;
+    }
+    cudaStream_t s = c->stream;
+    const size_t bytes = (size_t)((char*)v.Vol - (char*)v.q);
+    char* save = nullptr;
+    if (cudaMalloc(&save, bytes + sizeof(DevScalars)) != cudaSuccess) {
+        cudaGetLastError();
+        c->tune_report = "{\"enabled\": false, \"reason\": \"no memory for the state copy\"}";
+        return 0;
+    }
+    CK(cudaMemcpyAsync(save, v.q, bytes, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(save + bytes, v.sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, s));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto time3 = [&](auto launch) {
+        launch();
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 3; ++r) launch();
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return ms / 3.0f;
+    };
+    char buf[512];
+    std::string rep = "{\"enabled\": true";
+    // residual: the fused kernel of the strip-record path (not the generic one)
+    const int mode = c->d.scheme == SCFD_SCHEME_EULER ? RES_EULER : c->d.scheme == SCFD_SCHEME_LUSGS ? RES_LUSGS : RES_NR;
+    const bool fused = c->d.scheme != SCFD_SCHEME_DUAL && (mode == RES_EULER || c->use_sw3 || c->use_sw4) &&
+                       (c->nY == 1 || c->nY == 8 || c->nY == 9) && c->P.nact > 0;
+    if (fused) {
+        if (v.precision == SCFD_PREC_MIXED) launch_to_f32(v, s);
+        int tx[8], ty[8];
+        const int nt = residual2_tiles(tx, ty);
+        float best = 1e30f;
+        int pick = 0;
+        rep += ", \"residual_ms\": {";
+        for (int k = 0; k < nt; ++k) {
+            v.res_tile = k;
+            const float ms = time3([&] { launch_residual2(v, s, mode); });
+            std::snprintf(buf, sizeof(buf), "%s\"%dx%d\": %.4f", k ? ", " : "", tx[k], ty[k], ms);
+            rep += buf;
+            if (ms < best) {
+                best = ms;
+                pick = k;
+            }
+        }
+        v.res_tile = pick;
+        std::snprintf(buf, sizeof(buf), "}, \"residual_tile\": \"%dx%d\"", tx[pick], ty[pick]);
+        rep += buf;
+    }
+    if (c->P.nact > 0) {
+        const int cand[3] = {64, 128, 256};
+        float best = 1e30f;
+        int pick = 128;
+        rep += ", \"thermo_ms\": {";
+        for (int k = 0; k < 3; ++k) {
+            v.thermo_block = cand[k];
+            const float ms = time3([&] { launch_thermo(v, s, c->cells_max); });
+            std::snprintf(buf, sizeof(buf), "%s\"%d\": %.4f", k ? ", " : "", cand[k], ms);
+            rep += buf;
+            if (ms < best) {
+                best = ms;
+                pick = cand[k];
+            }
+        }
+        v.thermo_block = pick;
+        std::snprintf(buf, sizeof(buf), "}, \"thermo_block\": %d", pick);
+        rep += buf;
+    }
+    rep += "}";
+    CK(cudaMemcpyAsync(v.q, save, bytes, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(v.sc, save + bytes, sizeof(DevScalars), cudaMemcpyDeviceToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(save);
+    CK(cudaGetLastError());
+    c->tune_report = rep;
+    return 0;
+}
+
 // One physical step.  The first step of a context runs eagerly (it also sets
 // the kernels' shared-memory attributes); the second is captured into a CUDA
 // graph, which every later step replays with one launch.  The graph holds
@@ -1085,6 +1188,10 @@ int scfd_prepare(scfd_ctx* c, int step) {
 // live on the device.  Profiled steps run eagerly (their events are recorded
 // between the kernels).
 int step_once(scfd_ctx* c) {
+    if (!c->tuned) {
+        const int st = autotune(c);
+        if (st) return st;
+    }
     if (c->profiling || !c->use_graph || c->eager_steps < 1) {
         ++c->eager_steps;
         return enqueue_step(c);
@@ -1192,6 +1299,10 @@ int scfd_dstep(scfd_ctx* c, int step, scfd_dreq* req, scfd_stats* stats) {
         more = false;
         switch (c->ds_stage) {
             case DS_BEGIN: {
+                if (!c->tuned) {
+                    const int st0 = autotune(c);
+                    if (st0) return st0;
+                }
                 const int st = sync_scalars(c);
                 if (st) return st;
                 c->ds_att0 = c->h_sc->chem_attempts;
@@ -1274,6 +1385,12 @@ int scfd_dstep(scfd_ctx* c, int step, scfd_dreq* req, scfd_stats* stats) {
     if (st) return st;
     collect_events(c);
     return fill_stats(c, stats, c->ds_att0, c->ds_fb0);
+}
+
+int scfd_tuning(scfd_ctx* c, char* json, int len) {
+    if (!c || !json || len <= 0) return SCFD_E_ARG;
+    std::snprintf(json, (size_t)len, "%s", c->tune_report.c_str());
+    return (int)c->tune_report.size() < len ? 0 : SCFD_E_ARG;
 }
 
 int scfd_rms(scfd_ctx* c, double* rms) {

@@ -90,6 +90,9 @@ struct View {
     double phi_mus, k_mus, kappa, rgas, nu_gas, suth_mu0, suth_t0, suth_s, prandtl, schmidt, cfl, dt_fixed;
     double omega_max, omega_min, dq_max;
     double cfl_tau;              // DUAL: pseudo-time CFL
+    // launch shapes chosen by the autotuner (scfd_api.cu::autotune)
+    int res_tile;                // index into residual2_tiles()
+    int thermo_block;            // threads per CTA of k_thermo (64, 128 or 256)
     // state
     double *q, *qp, *qpp, *w, *vhi, *DHi, *Dq, *dt_mat;
     double *alpha, *nuA, *nuB;   // LU-SGS coefficients per cell
@@ -119,6 +122,7 @@ int launch_set_dt(const View& v, cudaStream_t s);
 int launch_set_dt_cells(const View& v, cudaStream_t s);  // dt_mat and the local minimum only
 int launch_residual(const View& v, cudaStream_t s, int mode, bool need_coeffs);
 bool launch_residual2(const View& v, cudaStream_t s, int mode);
+int residual2_tiles(int* tx, int* ty);  // the tile shapes of k_residual2 (count; tx, ty may be null)
 int launch_sweep_reset(cudaStream_t s, int* progress, int* tickets, int nstrips_fwd, int nstrips_bwd);
 int launch_sweep(const View& v, cudaStream_t s, int dir, double* xfer, int* progress, double* partials,
                  int* tickets, int nstrips_fwd, int nstrips_bwd, const int* strip_tab_f, const int* strip_tab_b);

@@ -198,6 +198,13 @@ class Solver:
         """geometry.bin of out_geo_bin (store/dim/2d/geometry.f90:182-193)."""
         self._check(self.lib.write_geometry(self.ctx, os.fsencode(path)), "write_geometry")
 
+    def tuning(self):
+        """The autotuner's choices and candidate times for this context (dict)."""
+        import json
+        buf = C.create_string_buffer(4096)
+        self._check(self.lib.tuning(self.ctx, buf, 4096), "tuning")
+        return json.loads(buf.value.decode())
+
     def stream(self):
         s = C.c_void_p()
         self._check(self.lib.get_stream(self.ctx, C.byref(s)), "get_stream")
