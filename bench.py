@@ -573,7 +573,8 @@ def main():
             "autotune": {"mixed": m["autotune"], "fp64": res["fp64"]["autotune"]},
             "clocks": m["clocks"], "roofline": roofline, "cpu_baseline": cpu,
             "status": {"mixed": m["status"], "fp64": res["fp64"]["status"], "res_warn": m["res_warn"],
-                       "omega": m["omega"], "chem_attempts": m["chem_attempts"], "chem_fallback_cells": m["chem_fallback"]},
+                       "omega": m["omega"], "omega_fp64": res["fp64"]["omega"],
+                       "chem_attempts": m["chem_attempts"], "chem_fallback_cells": m["chem_fallback"]},
             "kernels_mixed": {k: {kk: v[kk] for kk in ("avg_ms", "launches", "total_ms", "gbs") if kk in v}
                               for k, v in prof.items()},
             "kernels_fp64": {k: {kk: v[kk] for kk in ("avg_ms", "launches", "total_ms", "gbs") if kk in v}

@@ -266,7 +266,11 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
 #pragma unroll
         for (int k = 0; k < D; ++k) { outA[k] = RT(0); outB[k] = RT(0); }
         double res = 0.0;
-        // omega candidate q / (-Dq), kept as the pair (q, -Dq) in the record precision
+        // smallest omega candidate q / (-Dq) of the lane.  FP64 keeps it as the pair
+        // (q, -Dq), compared by cross-multiplication; FP32 keeps the ratio (fast
+        // divide), since species held at the density floor (~1e-37) would
+        // underflow an FP32 cross product.
+        constexpr bool f32 = sizeof(RT) == 4;
         RT on = RT(__longlong_as_double(0x7FF0000000000000ll)), od = RT(1);
         RT* gblk = const_cast<RT*>(rd) + lf * G;
         for (int tb = 0; tb < nblk8 && !bail; ++tb) {
@@ -374,12 +378,16 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
                     res = res + dE * dE;
 #pragma unroll
                     for (int k = 0; k < NY; ++k) {
-                        // smallest q_k/(-Dq_k) over Dq_k < 0, compared by cross-multiplication
+                        // smallest q_k/(-Dq_k) over Dq_k < 0
                         const RT dk = x[k];
                         const RT qn = f[R::QS + k], qd = -dk;
-                        if (dk < RT(0) && qn * od < on * qd) {
-                            on = qn;
-                            od = qd;
+                        if constexpr (f32) {
+                            if (dk < RT(0)) on = fminf(on, __fdividef(qn, qd));
+                        } else {
+                            if (dk < RT(0) && qn * od < on * qd) {
+                                on = qn;
+                                od = qd;
+                            }
                         }
                     }
                 }
@@ -410,7 +418,7 @@ __global__ void __launch_bounds__(32) k_sweep3(View v, StripRec sl, RT* rec, dou
             for (int o = 16; o > 0; o >>= 1) {
                 res += __shfl_xor_sync(0xffffffffu, res, o);
                 const RT on2 = __shfl_xor_sync(0xffffffffu, on, o), od2 = __shfl_xor_sync(0xffffffffu, od, o);
-                if (on2 * od < on * od2) {
+                if (on2 * od < on * od2) {  // FP32: od = 1, a plain minimum of the ratios
                     on = on2;
                     od = od2;
                 }
