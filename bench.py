@@ -73,20 +73,17 @@ def workload_name(config, scale):
 
 
 # algorithmic HBM bytes per interior cell and launch, FP64 storage
-# DRAM bytes (read + write) per interior cell and launch, from ncu captures of
+# DRAM bytes (read + write) per interior cell and launch, from an ncu capture of
 # the reacting step at scale 0.5 (196 608 cells; ncu flushes the caches before each
-# launch, so these are cold-cache figures).  Residual and sweeps:
-#   ncu --set full --clock-control none -k regex:"k_sweep3|k_residual2" -c 3
-#       -o prof_full python bench.py --scale 0.5 --steps 1 --warmup 1 --no-cpu-baseline
-# thermo, pack and unpack:
-#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
-#       --clock-control none -k regex:"k_thermo|k_pack|k_unpack" -c 12 --csv
+# launch, so these are cold-cache figures), residual tile pinned to 16x16:
+#   SCFD_RES_TILE=1 ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#       --clock-control none -k regex:"k_residual2|k_thermo|k_pack|k_unpack|k_sweep3" -c 80 --csv
 #       python bench.py --scale 0.5 --steps 1 --warmup 1 --no-cpu-baseline
 # None of these kernels reuses data across launches, so the traffic of a launch
 # grows with the cell count and is scaled to the workload by cells.
 NCU_DRAM_BYTES_PER_CELL = {
-    ("reacting_step", True): {abi.K_THERMO: 434.7, abi.K_RESIDUAL: 565.7, abi.K_PACK: 538.8,
-                              abi.K_SWEEP_FWD: 286.0, abi.K_SWEEP_BWD: 286.2, abi.K_UPDATE: 155.9},
+    ("reacting_step", True): {abi.K_THERMO: 494.2, abi.K_RESIDUAL: 549.5, abi.K_PACK: 540.2,
+                              abi.K_SWEEP_FWD: 285.2, abi.K_SWEEP_BWD: 285.3, abi.K_UPDATE: 155.9},
 }
 NCU_TRAFFIC_NOTE = "ncu dram__bytes_read+write per cell at scale 0.5 (cold cache), scaled by cells"
 

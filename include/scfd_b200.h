@@ -250,7 +250,9 @@ int  scfd_profile(scfd_ctx* ctx, int enable);
  * The tuner runs once per context, before its first step: each candidate is
  * timed with CUDA events on the context's own state (saved before and
  * restored after) and the fastest is kept; the candidates compute the same
- * values.  SCFD_AUTOTUNE=0 in the environment keeps the default shapes. */
+ * values.  SCFD_AUTOTUNE=0 in the environment keeps the default shapes;
+ * SCFD_RES_TILE=<k> pins the residual to tile k of the list (e.g. to profile
+ * one shape). */
 int  scfd_tuning(scfd_ctx* ctx, char* json, int len);
 int  scfd_kernel_stats(scfd_ctx* ctx, int kind, double* total_ms, int64_t* launches, char* name, int namelen);
 

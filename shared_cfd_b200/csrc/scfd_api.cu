@@ -1129,10 +1129,16 @@ static int autotune(scfd_ctx* c) {
     const int mode = c->d.scheme == SCFD_SCHEME_EULER ? RES_EULER : c->d.scheme == SCFD_SCHEME_LUSGS ? RES_LUSGS : RES_NR;
     const bool fused = c->d.scheme != SCFD_SCHEME_DUAL && (mode == RES_EULER || c->use_sw3 || c->use_sw4) &&
                        (c->nY == 1 || c->nY == 8 || c->nY == 9) && c->P.nact > 0;
-    if (fused) {
+    const char* force = std::getenv("SCFD_RES_TILE");  // pins the tile (index), e.g. for profiling
+    int tx[8], ty[8];
+    const int nt = residual2_tiles(tx, ty);
+    if (fused && force && std::atoi(force) >= 0 && std::atoi(force) < nt) {
+        v.res_tile = std::atoi(force);
+        std::snprintf(buf, sizeof(buf), ", \"residual_tile\": \"%dx%d\", \"residual_forced\": true", tx[v.res_tile],
+                      ty[v.res_tile]);
+        rep += buf;
+    } else if (fused) {
         if (v.precision == SCFD_PREC_MIXED) launch_to_f32(v, s);
-        int tx[8], ty[8];
-        const int nt = residual2_tiles(tx, ty);
         float best = 1e30f;
         int pick = 0;
         rep += ", \"residual_ms\": {";
