@@ -256,6 +256,36 @@ int  scfd_profile(scfd_ctx* ctx, int enable);
 int  scfd_tuning(scfd_ctx* ctx, char* json, int len);
 int  scfd_kernel_stats(scfd_ctx* ctx, int kind, double* total_ms, int64_t* launches, char* name, int namelen);
 
+/* ---- discrete adjoint of the explicit ideal-gas step ------------------------
+ * The reference has no adjoint.  For a 2d inviscid ideal-gas case on the
+ * explicit Euler scheme with a fixed dt (FP64), scfd_adjoint_run runs nsteps
+ * physical steps from the uploaded state and returns
+ *   J = sum over steps n in [win_first, win_last] of
+ *       sum over the boundary cells of descriptor obj_bc of ds * p(q^n)
+ * (the pressure force on that boundary: p of the first interior cell times the
+ * boundary face length) and dJ/dvalue of descriptor param_bc's values (the
+ * inflow state of a SCFD_BC_FIXED descriptor, for instance), by the reverse of
+ * every step: the MUSCL + SLAU residual, the ghost writes and the primitive
+ * map, hand-differentiated (the branches of SLAU's min / max / abs as taken
+ * forward).  States are recomputed from at most `snapshots` stored ones by
+ * binomial checkpointing.  counts (may be NULL) receives the forward and the
+ * reverse steps taken.  On return the context holds the uploaded state again.
+ * Other configurations return SCFD_E_UNSUPPORTED. */
+typedef struct scfd_adj_desc {
+    int32_t abi_version;
+    int32_t nsteps;              /* physical steps, >= 1                           */
+    int32_t snapshots;           /* stored states besides the initial one, >= 0  */
+    int32_t obj_bc;              /* 0-based descriptor index of the objective     */
+    int32_t win_first, win_last; /* 0 <= win_first <= win_last < nsteps           */
+    int32_t param_bc;            /* 0-based descriptor of the gradient, -1: none  */
+    int32_t forward_only;        /* 1: J only                                     */
+    int32_t reserved[8];
+} scfd_adj_desc;
+/* grad: SCFD_BC_MAXVAL + 2 doubles, one per value[] entry of param_bc. */
+int  scfd_adjoint_run(scfd_ctx* ctx, const scfd_adj_desc* desc, double* J, double* grad, int64_t* counts);
+/* Replaces the value[] of boundary descriptor bc (0-based) after commit. */
+int  scfd_set_bc_values(scfd_ctx* ctx, int bc, const double* value);
+
 /* ---- block-sharded step over several processes (one GPU each) -------------
  * Replaces the MPI decomposition of the reference: the cross-rank halo copies
  * of set_BC (store/cond/no-nV/condition.tail.f90:71-330, MPI_Isend/Recv of w

@@ -2333,6 +2333,66 @@ int orc_launch_count(const orc_ctx* c, int64_t* n) {
     return 0;
 }
 
+int orc_set_bc_values(orc_ctx* c, int bc, const double* value) {
+    if (!c || !value || bc < 0 || bc >= (int)c->bcs.size()) return SCFD_E_ARG;
+    std::memcpy(c->bcs[bc].value, value, sizeof(c->bcs[bc].value));
+    return 0;
+}
+
+// The objective of scfd_adjoint_run on the restatement (forward only: the
+// reference has no adjoint): J = sum over the window's states of
+// sum_cells ds * p, p = (kappa-1)(E - |rho u|^2 / (2 rho)) of the first interior
+// cells along the descriptor, ds the boundary face length.
+int orc_adjoint_run(orc_ctx* c, const scfd_adj_desc* d, double* J, double* grad, int64_t* counts) {
+    if (!c || !d || !J) return SCFD_E_ARG;
+    if (!c->committed) return SCFD_E_STATE;
+    if (!d->forward_only) return SCFD_E_UNSUPPORTED;
+    if (d->nsteps < 1 || d->win_first < 0 || d->win_first > d->win_last || d->win_last >= d->nsteps ||
+        d->obj_bc < 0 || d->obj_bc >= (int)c->bcs.size())
+        return SCFD_E_ARG;
+    const scfd_bc& b = c->bcs[d->obj_bc];
+    const int p = b.plane, ni = c->ni[p - 1], nj = c->nj[p - 1], nY = c->nY;
+    auto term = [&]() {
+        double t = 0.0;
+        for (int s = b.first; s <= b.last; ++s) {
+            int i, j;
+            double ds;
+            switch (b.side) {
+                case SCFD_SIDE_ILO: i = 1; j = s; ds = c->dsi(0, s, p); break;
+                case SCFD_SIDE_IHI: i = ni; j = s; ds = c->dsi(ni, s, p); break;
+                case SCFD_SIDE_JLO: i = s; j = 1; ds = c->dsj(s, 0, p); break;
+                default: i = s; j = nj; ds = c->dsj(s, nj, p); break;
+            }
+            double rho = 0.0;
+            for (int k = 1; k <= nY; ++k) rho = rho + c->q(k, i, j, p);
+            const double mx = c->q(nY + 1, i, j, p), my = c->q(nY + 2, i, j, p);
+            t = t + ds * (c->d.kappa - 1.0) * (c->q(nY + 3, i, j, p) - 0.5 * (mx * mx + my * my) / rho);
+        }
+        return t;
+    };
+    const std::vector<double> q0 = c->q.v;
+    const double tt0 = c->tt;
+    double sum = 0.0;
+    for (int n = 0; n <= d->win_last; ++n) {
+        if (n >= d->win_first) sum = sum + term();
+        if (n < d->win_last) {
+            const int s = step(*c, n + 1, nullptr);
+            if (s) return s;
+        }
+    }
+    c->q.v = q0;
+    c->qp.v = q0;
+    c->qpp.v = q0;
+    c->tt = tt0;
+    *J = sum;
+    (void)grad;
+    if (counts) {
+        counts[0] = d->win_last;
+        counts[1] = 0;
+    }
+    return 0;
+}
+
 int orc_tuning(orc_ctx* c, char* json, int len) {  // no launch shapes on the CPU
     if (!c || !json || len <= 0) return SCFD_E_ARG;
     std::snprintf(json, (size_t)len, "{\"enabled\": false}");

@@ -117,6 +117,21 @@ class Stats(C.Structure):
     ]
 
 
+class AdjDesc(C.Structure):
+    """scfd_adj_desc: the discrete adjoint run of scfd_adjoint_run."""
+    _fields_ = [
+        ("abi_version", C.c_int32),
+        ("nsteps", C.c_int32),
+        ("snapshots", C.c_int32),
+        ("obj_bc", C.c_int32),
+        ("win_first", C.c_int32),
+        ("win_last", C.c_int32),
+        ("param_bc", C.c_int32),
+        ("forward_only", C.c_int32),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
 MAX_RANKS = 64
 DREQ_DONE, DREQ_REDUCE, DREQ_HALO = 0, 1, 2
 
@@ -179,6 +194,8 @@ SIGNATURES = {
     "profile": (C.c_int, [_P, C.c_int]),
     "tuning": (C.c_int, [_P, C.c_char_p, C.c_int]),
     "kernel_stats": (C.c_int, [_P, C.c_int, _D, C.POINTER(C.c_int64), C.c_char_p, C.c_int]),
+    "adjoint_run": (C.c_int, [_P, C.POINTER(AdjDesc), _D, _D, C.POINTER(C.c_int64)]),
+    "set_bc_values": (C.c_int, [_P, C.c_int, _D]),
     "set_partition": (C.c_int, [_P, C.POINTER(C.c_int32), C.c_int, C.c_int]),
     "dstep": (C.c_int, [_P, C.c_int, C.POINTER(DReq), C.POINTER(Stats)]),
     "reactors_create": (C.c_int, [C.POINTER(Chem), C.c_int, C.POINTER(_P)]),

@@ -375,6 +375,39 @@ def forward_step(orientation=0, n=12, scheme=abi.SCHEME_EULER, dt_mode=abi.DT_GL
     return case
 
 
+def adjoint_channel(n=24, steps=60, mach=0.5, seed=3, cfl=0.25):
+    """Two ideal-gas blocks joined i-i (the first forward-step layout): a fixed
+    inflow (descriptor 0, plane 1 i-lo) slightly off the initial state, slip walls
+    at j-lo and j-hi, zero-gradient outflow (plane 2 i-hi); a seeded smooth
+    perturbation of the initial state; explicit Euler, inviscid, fixed dt at
+    acoustic CFL 0.25 (forward Euler with MUSCL lets this perturbed flow grow
+    unboundedly at 0.4 within 60 steps).  The case of the discrete adjoint
+    (scfd_adjoint_run)."""
+    L = 1.0
+    a = np.linspace(0.0, L, n + 1)
+    b = np.linspace(L, 2 * L, 2 * n + 1)
+    c = np.linspace(0.2, 0.2 + L, n + 1)
+    planes = F.roundtrip_plot3d_values([rect_plane(a, c), rect_plane(b, c)])
+    d = base_desc(dt_mode=abi.DT_FIXED, scheme=abi.SCHEME_EULER, viscous=0)
+    cut, _ = F.connectivity(planes)
+    case = Case(planes, d, cut=cut)
+    rho, p = 1.2, 1e5
+    snd = math.sqrt(1.4 * p / rho)
+    d.dt_fixed = cfl * (L / n) / (snd * (1.0 + mach))
+    for pl in range(2):
+        q, w, vhi = ideal_state(case, rho, mach * snd, 0.0, p)
+        fill_all(case, pl, q, w, vhi)
+    perturb(case, seed=seed, amp=0.02)
+    qi, wi, vi = ideal_state(case, 1.02 * rho, 1.05 * mach * snd, 0.02 * snd, 1.01 * p)
+    case.bcs = [bc(1, abi.SIDE_ILO, 1, n, abi.BC_FIXED, list(wi) + list(vi)),
+                bc(2, abi.SIDE_IHI, 1, n, abi.BC_EXTRAP),
+                bc(1, abi.SIDE_JLO, 1, n, abi.BC_SLIP), bc(1, abi.SIDE_JHI, 1, n, abi.BC_SLIP),
+                bc(2, abi.SIDE_JLO, 1, 2 * n, abi.BC_SLIP), bc(2, abi.SIDE_JHI, 1, 2 * n, abi.BC_SLIP)]
+    case.steps = steps
+    case.name = "adjoint_channel_%d" % n
+    return case
+
+
 def split_planes_i(case, k):
     """The same case with every plane cut along i into k pieces of (nearly)
     equal width, joined again by i-i block interfaces that the connectivity

@@ -1393,6 +1393,204 @@ int scfd_dstep(scfd_ctx* c, int step, scfd_dreq* req, scfd_stats* stats) {
     return fill_stats(c, stats, c->ds_att0, c->ds_fb0);
 }
 
+int scfd_set_bc_values(scfd_ctx* c, int bc, const double* value) {
+    if (!c || !value || bc < 0 || bc >= (int)c->bcs.size()) return SCFD_E_ARG;
+    if (!c->committed) return c->fail(SCFD_E_STATE, "set_bc_values before commit");
+    std::memcpy(c->bcs[bc].value, value, sizeof(double) * c->valstride);
+    CK(cudaMemcpyAsync(c->d_bcval + (size_t)bc * c->valstride, value, sizeof(double) * c->valstride,
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint of the explicit ideal-gas step with binomial checkpointing.
+// ---------------------------------------------------------------------------
+namespace {
+
+// binomial(s + t, t): steps reversible with s stored states and t sweeps
+long long binom_steps(int s, int t) {
+    long double r = 1.0L;
+    for (int k = 1; k <= t; ++k) r = r * (long double)(s + k) / (long double)k;
+    return r > 4e18L ? (long long)4e18 : (long long)(r + 0.5L);
+}
+
+struct AdjRun {
+    scfd_ctx* c;
+    const scfd_adj_desc* d;
+    double dt = 0.0;
+    size_t qsz = 0;            // doubles per stored state (q, all slots)
+    double* slots = nullptr;   // [snapshots + 1][qsz]
+    int nslots = 0;
+    std::vector<int> free_slot;
+    double* lam = nullptr;     // dJ/dq, D components per slot
+    double* wbar = nullptr;    // adjoint of w, W components per slot
+    double* dgrad = nullptr;   // [valstride]
+    double* dJ = nullptr;
+    long long* ocells = nullptr;
+    double* owt = nullptr;
+    int nobj = 0;
+    long long fwd = 0, rev = 0;
+    int visited = 0;           // highest step index whose state has been formed
+
+    bool in_window(int n) const { return n >= d->win_first && n <= d->win_last; }
+    int save(int slot) {
+        CK(cudaMemcpyAsync(slots + (size_t)slot * qsz, c->v.q, qsz * sizeof(double), cudaMemcpyDeviceToDevice,
+                           c->stream));
+        return 0;
+    }
+    int restore(int slot) {
+        CK(cudaMemcpyAsync(c->v.q, slots + (size_t)slot * qsz, qsz * sizeof(double), cudaMemcpyDeviceToDevice,
+                           c->stream));
+        return 0;
+    }
+    // q^a in the context -> q^b; adds the objective of states formed for the first time
+    int advance(int a, int b) {
+        for (int k = a; k < b; ++k) {
+            int st = step_once(c);
+            if (st) return st;
+            ++fwd;
+            if (k + 1 > visited) {
+                visited = k + 1;
+                if (in_window(k + 1)) launch_adj_objective(c->v, c->stream, ocells, owt, nobj, dJ, nullptr, 0);
+            }
+        }
+        return 0;
+    }
+    // q^n in the context; lam = dJ/dq^{n+1} -> dJ/dq^n
+    int step_back(int n) {
+        const View& v = c->v;
+        cudaStream_t s = c->stream;
+        launch_thermo(v, s, c->cells_max);
+        launch_ghosts(v, s, c->d_ops, c->nops, c->d_bcval, c->valstride);
+        CK(cudaMemsetAsync(wbar, 0, sizeof(double) * (size_t)c->W * c->ncell, s));
+        launch_adj_faces(v, s, lam, wbar, dt);
+        launch_adj_ghost(v, s, c->d_ops, c->nops, c->d_bcval, c->valstride, wbar, dgrad, d->param_bc);
+        launch_adj_prim(v, s, wbar, lam);
+        if (in_window(n)) launch_adj_objective(v, s, ocells, owt, nobj, nullptr, lam, 1);
+        CK(cudaGetLastError());
+        ++rev;
+        return 0;
+    }
+    int split(int a, int b, int sfree) const {
+        const int n = b - a;
+        int t = 1;
+        while (binom_steps(sfree, t) < n) ++t;
+        const long long tail = binom_steps(sfree - 1, t);
+        const int m = b - (int)std::min<long long>(tail, n - 1);
+        return std::max(m, a + 1);
+    }
+    // precondition: the context holds q^a, stored in slot sa; lam = dJ/dq^b
+    int revolve(int a, int b, int sa) {
+        int st;
+        if (b - a == 1) return step_back(a);
+        if (free_slot.empty()) {
+            for (int k = b - 1; k >= a; --k) {
+                if ((st = restore(sa)) || (st = advance(a, k)) || (st = step_back(k))) return st;
+            }
+            return 0;
+        }
+        const int m = split(a, b, (int)free_slot.size());
+        if ((st = advance(a, m))) return st;
+        const int sm = free_slot.back();
+        free_slot.pop_back();
+        if ((st = save(sm))) return st;
+        if ((st = revolve(m, b, sm))) return st;
+        free_slot.push_back(sm);
+        if ((st = restore(sa))) return st;
+        return revolve(a, m, sa);
+    }
+};
+
+}  // namespace
+
+int scfd_adjoint_run(scfd_ctx* c, const scfd_adj_desc* d, double* J, double* grad, int64_t* counts) {
+    if (!c || !d || !J) return SCFD_E_ARG;
+    if (!c->committed || !c->uploaded) return c->fail(SCFD_E_STATE, "adjoint before upload");
+    if (d->abi_version != SCFD_ABI_VERSION || d->nsteps < 1 || d->snapshots < 0 || d->win_first < 0 ||
+        d->win_first > d->win_last || d->win_last >= d->nsteps || d->obj_bc < 0 || d->obj_bc >= (int)c->bcs.size() ||
+        d->param_bc < -1 || d->param_bc >= (int)c->bcs.size() || (!d->forward_only && d->param_bc >= 0 && !grad))
+        return c->fail(SCFD_E_ARG, "bad adjoint descriptor");
+    const scfd_desc& cd = c->d;
+    if (cd.scheme != SCFD_SCHEME_EULER || cd.thermo != SCFD_THERMO_IDEAL || cd.dim != SCFD_DIM_2D || cd.viscous ||
+        cd.dt_mode != SCFD_DT_FIXED || cd.precision != SCFD_PREC_FP64 || c->nranks > 1 || c->nY != 1)
+        return c->fail(SCFD_E_UNSUPPORTED, "the adjoint covers the 2d inviscid ideal-gas explicit step (FP64, fixed dt)");
+    AdjRun r;
+    r.c = c;
+    r.d = d;
+    r.dt = cd.dt_fixed;
+    r.qsz = (size_t)c->D * c->ncell;
+    // objective cells: the first interior cells along the descriptor's range, weighted by the face length
+    {
+        const scfd_bc& b = c->bcs[d->obj_bc];
+        const int p = b.plane - 1, ni = c->P.ni[p], nj = c->P.nj[p];
+        std::vector<long long> cells, faces;
+        for (int sx = b.first; sx <= b.last; ++sx) {
+            switch (b.side) {
+                case SCFD_SIDE_ILO: cells.push_back(cidx(c->P, p, 1, sx)); faces.push_back(cidx(c->P, p, 0, sx)); break;
+                case SCFD_SIDE_IHI: cells.push_back(cidx(c->P, p, ni, sx)); faces.push_back(cidx(c->P, p, ni, sx)); break;
+                case SCFD_SIDE_JLO: cells.push_back(cidx(c->P, p, sx, 1)); faces.push_back(cidx(c->P, p, sx, 0)); break;
+                default: cells.push_back(cidx(c->P, p, sx, nj)); faces.push_back(cidx(c->P, p, sx, nj)); break;
+            }
+        }
+        const double* ds = (b.side == SCFD_SIDE_ILO || b.side == SCFD_SIDE_IHI) ? c->v.dsi : c->v.dsj;
+        std::vector<double> wt(cells.size());
+        for (size_t k = 0; k < cells.size(); ++k)
+            CK(cudaMemcpy(&wt[k], ds + faces[k], sizeof(double), cudaMemcpyDeviceToHost));
+        r.nobj = (int)cells.size();
+        CK(cudaMalloc(&r.ocells, sizeof(long long) * std::max(1, r.nobj)));
+        CK(cudaMalloc(&r.owt, sizeof(double) * std::max(1, r.nobj)));
+        CK(cudaMemcpy(r.ocells, cells.data(), sizeof(long long) * cells.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(r.owt, wt.data(), sizeof(double) * wt.size(), cudaMemcpyHostToDevice));
+    }
+    const int S = d->forward_only ? 0 : std::min(d->snapshots, d->nsteps);
+    r.nslots = S + 1;
+    int st = 0;
+    auto fail_free = [&](int code) {
+        cudaFree(r.slots); cudaFree(r.lam); cudaFree(r.wbar); cudaFree(r.dgrad); cudaFree(r.dJ);
+        cudaFree(r.ocells); cudaFree(r.owt);
+        return code;
+    };
+    if (cudaMalloc(&r.slots, sizeof(double) * r.qsz * r.nslots) != cudaSuccess ||
+        cudaMalloc(&r.dgrad, sizeof(double) * c->valstride) != cudaSuccess ||
+        cudaMalloc(&r.dJ, sizeof(double)) != cudaSuccess ||
+        (!d->forward_only && (cudaMalloc(&r.lam, sizeof(double) * r.qsz) != cudaSuccess ||
+                              cudaMalloc(&r.wbar, sizeof(double) * (size_t)c->W * c->ncell) != cudaSuccess))) {
+        cudaGetLastError();
+        return fail_free(c->fail(SCFD_E_CUDA, "no device memory for the adjoint's states"));
+    }
+    for (int k = S; k >= 1; --k) r.free_slot.push_back(k);
+    DevScalars sc0;
+    if ((st = sync_scalars(c))) return fail_free(st);
+    sc0 = *c->h_sc;
+    CK(cudaMemsetAsync(r.dJ, 0, sizeof(double), c->stream));
+    CK(cudaMemsetAsync(r.dgrad, 0, sizeof(double) * c->valstride, c->stream));
+    if (!d->forward_only) CK(cudaMemsetAsync(r.lam, 0, sizeof(double) * r.qsz, c->stream));
+    c->launches = 0;
+    if ((st = r.save(0))) return fail_free(st);
+    if (r.in_window(0)) launch_adj_objective(c->v, c->stream, r.ocells, r.owt, r.nobj, r.dJ, nullptr, 0);
+    if (d->forward_only)
+        st = r.advance(0, d->win_last);
+    else
+        st = r.revolve(0, d->nsteps, 0);
+    if (st) return fail_free(st);
+    // the uploaded state back: q, qp, qpp and the scalars
+    if ((st = r.restore(0))) return fail_free(st);
+    const size_t qb = sizeof(double) * r.qsz;
+    CK(cudaMemcpyAsync(c->v.qp, c->v.q, qb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->v.qpp, c->v.q, qb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_sc, &sc0, sizeof(DevScalars), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(J, r.dJ, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (grad) CK(cudaMemcpyAsync(grad, r.dgrad, sizeof(double) * c->valstride, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (counts) {
+        counts[0] = r.fwd;
+        counts[1] = r.rev;
+    }
+    fail_free(0);
+    return 0;
+}
+
 int scfd_tuning(scfd_ctx* c, char* json, int len) {
     if (!c || !json || len <= 0) return SCFD_E_ARG;
     std::snprintf(json, (size_t)len, "%s", c->tune_report.c_str());

@@ -196,6 +196,14 @@ int launch_res_import(const View& v, cudaStream_t s, const double* red, int inne
 int launch_status_export(const View& v, cudaStream_t s, double* red);    // red = [-status]
 int launch_status_import(const View& v, cudaStream_t s, const double* red);
 
+// discrete adjoint of the explicit ideal-gas step (k_adjoint.cu)
+int launch_adj_faces(const View& v, cudaStream_t s, const double* lam, double* wbar, double dt);
+int launch_adj_ghost(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride,
+                     double* wbar, double* grad, int param_bc);
+int launch_adj_prim(const View& v, cudaStream_t s, const double* wbar, double* lam);
+int launch_adj_objective(const View& v, cudaStream_t s, const long long* cells, const double* wt, int n, double* J,
+                         double* lam, int grad_only);
+
 // residual modes (RES_DUAL: NR's right-hand side multiplied by Gamma^-1 and the
 // coefficients of the preconditioned dual time)
 enum { RES_EULER = 0, RES_LUSGS = 1, RES_NR = 2, RES_DUAL = 3 };
