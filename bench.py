@@ -287,6 +287,81 @@ def cpu_reactors(cores, n=REACTOR_N):
     return n / dt, dt, out
 
 
+# ---------------------------------------------------------------------------
+# discrete adjoint of the explicit ideal-gas step (scfd_adjoint_run)
+# ---------------------------------------------------------------------------
+ADJ_N, ADJ_STEPS, ADJ_WINDOW, ADJ_SNAPSHOTS = 256, 300, (200, 299), 16
+
+
+def adjoint_workload():
+    return ("gradient of the pressure force on a slip wall (steps %d-%d) with respect to the inflow state: "
+            "2 ideal-gas blocks 256x256 + 512x256 (196 608 cells), MUSCL + SLAU, explicit Euler, %d steps, "
+            "binomial checkpointing with %d stored states" % (ADJ_WINDOW[0], ADJ_WINDOW[1], ADJ_STEPS, ADJ_SNAPSHOTS))
+
+
+def run_adjoint(args, rank, cores):
+    """One JSON line: primal and adjoint device time of the same run; value =
+    cell-steps per second of the gradient computation."""
+    unit = "Mcell-step/s"
+    case = cases.adjoint_channel(n=ADJ_N)
+    units = case.ncells * ADJ_STEPS / 1e6
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no adjoint (and no tangent-linear "
+                          "model); only the primal objective is restated on the CPU"}), flush=True)
+        return 0
+    if rank != 0:
+        return 0
+    import torch
+    from shared_cfd_b200 import build
+    from shared_cfd_b200.adjoint import adjoint_run
+    from shared_cfd_b200.solver import Solver
+    build.build()
+    s = Solver(case)
+    s.upload()
+    stream = torch.cuda.ExternalStream(s.stream(), device=0)
+    for _ in range(max(1, args.warmup)):
+        adjoint_run(s, 4, 2, (1, 3), 0, snapshots=2)
+        s.upload()
+        s.run(1, 3)
+        s.upload()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    prim, adj = [], []
+    with ClockSampler(0) as cs:
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            e0.record(stream)
+            st = s.run(1, ADJ_STEPS)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            prim.append(e0.elapsed_time(e1))
+            s.upload()
+            t0 = time.perf_counter()
+            J, grad, counts = adjoint_run(s, ADJ_STEPS, 2, ADJ_WINDOW, 0, snapshots=ADJ_SNAPSHOTS)
+            adj.append(1e3 * (time.perf_counter() - t0))
+    ms_p, ms_a = min(prim), min(adj)
+    q = s.download()[0]
+    s.close()
+    line = {
+        "metric": "Mcell-step/s of the adjoint gradient (FP64)", "value": units / (ms_a * 1e-3), "unit": unit,
+        "n_gpus": 1, "steps": max(1, args.steps), "warmup": args.warmup, "ms_per_step": ms_a,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": adjoint_workload(), "cells": case.ncells, "steps": ADJ_STEPS},
+        "adjoint_over_primal": ms_a / ms_p, "primal_ms": ms_p, "adjoint_ms": ms_a,
+        "forward_steps": counts[0], "reverse_steps": counts[1], "J": J,
+        "grad_inflow": {"rho": grad[0], "u": grad[1], "v": grad[2], "p": grad[3]},
+        "primal_status": st.status, "state_finite": bool(np.isfinite(q).all()),
+        "e2e": None, "cpu_baseline": None,
+        "clocks": cs.summary(),
+        "note": "primal = the same %d steps through scfd_run (CUDA graph); the adjoint time is host wall time of "
+                "scfd_adjoint_run (its forward recomputation, reverse steps and state copies)" % ADJ_STEPS,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reactors(args, rank, cores):
     """One JSON line for the 0-D reactor batch (rank 0 only; the batch does not
     shard across ranks in this benchmark)."""
@@ -391,7 +466,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="reacting_step", choices=["reacting_step", "flat_plate", "sod", "reactors"])
+    ap.add_argument("--config", default="reacting_step",
+                    choices=["reacting_step", "flat_plate", "sod", "reactors", "adjoint"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -404,6 +480,8 @@ def main():
 
     if args.config == "reactors":
         return run_reactors(args, rank, cores)
+    if args.config == "adjoint":
+        return run_adjoint(args, rank, cores)
 
     if args.impl == "reference":
         if rank != 0:

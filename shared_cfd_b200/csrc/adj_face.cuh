@@ -38,22 +38,21 @@ SCFD_HD void muscl_fwd(double wm1, double w0, double w1, double w2, double phi, 
 }
 
 // ds/da and ds/db of s = 2ab / (a^2 + b^2 + eps), written so that a = b = 0 gives 0
-SCFD_HD void limiter_grad(double a, double b, double& sa, double& sb) {
-    const double Q = a * a + b * b + kEps;
-    const double ra = 2.0 * b / Q, rb = 2.0 * a / Q;
-    sa = ra * (1.0 - 2.0 * a * a / Q);
-    sb = rb * (1.0 - 2.0 * b * b / Q);
+SCFD_HD void limiter_grad(double a, double b, double iQ, double& sa, double& sb) {
+    const double ra = 2.0 * b * iQ, rb = 2.0 * a * iQ;
+    sa = ra * (1.0 - 2.0 * a * a * iQ);
+    sb = rb * (1.0 - 2.0 * b * b * iQ);
 }
 
 // One-sided slope d(a, b) = s/2 ((1 + km s) a + (1 - km s) b), s = s(a, b): adds
 // its adjoint g times the partial derivatives to ab, bb.
 SCFD_HD void slope_rev(double a, double b, double km, double g, double& ab, double& bb) {
-    const double Q = a * a + b * b + kEps;
-    const double s = 2.0 * a * b / Q;
+    const double iQ = 1.0 / (a * a + b * b + kEps);
+    const double s = 2.0 * a * b * iQ;
     const double A = (1.0 + km * s) * a + (1.0 - km * s) * b;
     const double dds = 0.5 * A + 0.5 * s * km * (a - b);
     double sa, sb;
-    limiter_grad(a, b, sa, sb);
+    limiter_grad(a, b, iQ, sa, sb);
     ab += g * (0.5 * s * (1.0 + km * s) + dds * sa);
     bb += g * (0.5 * s * (1.0 - km * s) + dds * sb);
 }
@@ -162,6 +161,7 @@ SCFD_HD void slau_rev(int nY, const double* wl, const double* wr, double n1, dou
     const double betarb = ptb * (-0.5 * (pl - pr) + (1.0 - chi) * p_bar);
     double plb = ptb * 0.5 * (betal - betar), prb = -ptb * 0.5 * (betal - betar);
     double chib = -ptb * (betar + betal - 1.0) * p_bar;
+    const double ia = 1.0 / a_bar, ia2 = ia * ia;
     double mrb = 0.0, mlb = 0.0;
     if (rin) mrb += betarb * 0.25 * ((mr - 1.0) * (mr - 1.0) + (2.0 + mr) * 2.0 * (mr - 1.0));
     if (lin) mlb += betalb * 0.25 * (-(ml + 1.0) * (ml + 1.0) + (2.0 - ml) * 2.0 * (ml + 1.0));
@@ -169,16 +169,17 @@ SCFD_HD void slau_rev(int nY, const double* wl, const double* wr, double n1, dou
     double rholb = dmb * 0.5 * (unl + ubp), rhorb = dmb * 0.5 * (unr - ubm);
     double unlb = dmb * 0.5 * rhol, unrb = dmb * 0.5 * rhor;
     const double ubpb = dmb * 0.5 * rhol, ubmb = -dmb * 0.5 * rhor;
-    chib += -dmb * 0.5 * dp / a_bar;
-    double a_barb = dmb * 0.5 * chi * dp / (a_bar * a_bar);
-    const double dpb = -dmb * 0.5 * chi / a_bar;
+    chib += -dmb * 0.5 * dp * ia;
+    double a_barb = dmb * 0.5 * chi * dp * ia2;
+    const double dpb = -dmb * 0.5 * chi * ia;
     // ubp, ubm
     double ubb = ubpb * (1.0 - g) + ubmb * (1.0 - g);
     const double gb = ubpb * (fabs(unl) - ub) + ubmb * (fabs(unr) - ub);
     unlb += ubpb * g * sgn(unl);
     unrb += ubmb * g * sgn(unr);
     // ub = num / den
-    const double numb = ubb / den, denb = -ubb * num / (den * den);
+    const double iden = 1.0 / den;
+    const double numb = ubb * iden, denb = -ubb * num * iden * iden;
     unrb += numb * rhor * sgn(unr);
     rhorb += numb * fabs(unr) + denb;
     unlb += numb * rhol * sgn(unl);
@@ -190,8 +191,8 @@ SCFD_HD void slau_rev(int nY, const double* wl, const double* wr, double n1, dou
     // chi, m_tilde
     const double mtb = chib * (-2.0 * (1.0 - m_tilde));
     const double mrawb = mraw < 1.0 ? mtb : 0.0;
-    const double sqb = mrawb / a_bar;
-    a_barb += -mrawb * sq / (a_bar * a_bar);
+    const double sqb = mrawb * ia;
+    a_barb += -mrawb * sq * ia2;
     if (sq > 0.0) {
         const double Sb = sqb / (2.0 * sq);
         ulb += Sb * ul;
@@ -200,9 +201,9 @@ SCFD_HD void slau_rev(int nY, const double* wl, const double* wr, double n1, dou
         vrb += Sb * vr;
     }
     // Mach numbers
-    unlb += mlb / a_bar;
-    unrb += mrb / a_bar;
-    a_barb += -(mlb * unl + mrb * unr) / (a_bar * a_bar);
+    unlb += mlb * ia;
+    unrb += mrb * ia;
+    a_barb += -(mlb * unl + mrb * unr) * ia2;
     // p_bar, a_bar, dp
     prb += 0.5 * p_barb + dpb;
     plb += 0.5 * p_barb - dpb;
@@ -213,13 +214,14 @@ SCFD_HD void slau_rev(int nY, const double* wl, const double* wr, double n1, dou
     urb += n1 * unrb;
     vrb += n2 * unrb;
     // sound speeds a = sqrt(gamma p / rho)
-    const double Alb = alb / (2.0 * al), Arb = arb / (2.0 * ar);
-    wlb[4 + nY] += Alb * pl / rhol;
-    plb += Alb * gl / rhol;
-    rholb += -Alb * Al / rhol;
-    wrb[4 + nY] += Arb * pr / rhor;
-    prb += Arb * gr / rhor;
-    rhorb += -Arb * Ar / rhor;
+    const double irl = 1.0 / rhol, irr = 1.0 / rhor;
+    const double Alb = 0.5 * alb / al, Arb = 0.5 * arb / ar;
+    wlb[4 + nY] += Alb * pl * irl;
+    plb += Alb * gl * irl;
+    rholb += -Alb * Al * irl;
+    wrb[4 + nY] += Arb * pr * irr;
+    prb += Arb * gr * irr;
+    rhorb += -Arb * Ar * irr;
     wlb[0] += rholb;
     wlb[1] += ulb;
     wlb[2] += vlb;
@@ -238,25 +240,26 @@ SCFD_HD void ideal_prim_rev(int nY, const double* q, double kappa, double rhob, 
                             const double* Yb, double htb, double* qb) {
     double rho = 0.0;
     for (int k = 0; k < nY; ++k) rho = rho + q[k];
-    const double u = q[nY] / rho, v = q[nY + 1] / rho, E = q[nY + 2];
-    const double ei = E / rho - 0.5 * (u * u + v * v);
+    const double ir = 1.0 / rho, ir2 = ir * ir;
+    const double u = q[nY] * ir, v = q[nY + 1] * ir, E = q[nY + 2];
+    const double ei = E * ir - 0.5 * (u * u + v * v);
     const double p = rho * (kappa - 1.0) * ei;
-    double Eb = htb / rho;
-    pb += htb / rho;
-    rhob += -htb * (E + p) / (rho * rho);
+    double Eb = htb * ir;
+    pb += htb * ir;
+    rhob += -htb * (E + p) * ir2;
     rhob += pb * (kappa - 1.0) * ei;
     const double eib = pb * rho * (kappa - 1.0);
-    Eb += eib / rho;
-    rhob += -eib * E / (rho * rho);
+    Eb += eib * ir;
+    rhob += -eib * E * ir2;
     ub += -eib * u;
     vb += -eib * v;
     for (int k = 0; k < nY; ++k) {
-        qb[k] += Yb[k] / rho;
-        rhob += -Yb[k] * q[k] / (rho * rho);
+        qb[k] += Yb[k] * ir;
+        rhob += -Yb[k] * q[k] * ir2;
     }
-    qb[nY] += ub / rho;
-    qb[nY + 1] += vb / rho;
-    rhob += -(ub * q[nY] + vb * q[nY + 1]) / (rho * rho);
+    qb[nY] += ub * ir;
+    qb[nY + 1] += vb * ir;
+    rhob += -(ub * q[nY] + vb * q[nY + 1]) * ir2;
     qb[nY + 2] += Eb;
     for (int k = 0; k < nY; ++k) qb[k] += rhob;
 }

@@ -12,6 +12,9 @@
 //     they copy and to the boundary values (the parameter gradient)
 //   lam_c += (dw/dq)^T wb_c + [c on the objective boundary] ds dp/dq
 // so that lam becomes dJ/dq^n.  dt is the fixed time step (no derivative).
+// wb starts at zero once per run: every step's consumers clear what they read
+// (each ghost cell has one ghost write; the inviscid stencils never reach the
+// corner cells).
 #include "adj_face.cuh"
 #include "scfd_internal.h"
 
@@ -20,12 +23,14 @@ namespace scfd {
 namespace {
 constexpr int NY1 = 1;           // the ideal gas carries one species
 constexpr int NC = 6 + NY1;      // rho, u, v, p, Y, gamma, h_t
+constexpr int DD = NY1 + 3;      // conserved components
 }  // namespace
 
 // w component of the m-th SLAU state entry
 __device__ __forceinline__ int wcomp(int m, int D) { return m < 4 + NY1 ? m : (m == 4 + NY1 ? D + 1 : D + 2); }
 
-__global__ void k_adj_faces(View v, const double* __restrict__ lam, double* __restrict__ wbar, double dt) {
+__global__ void __launch_bounds__(128, 3) k_adj_faces(View v, const double* __restrict__ lam, double* __restrict__ wbar,
+                                                     double dt) {
     const int p = v.P.act[blockIdx.y];
     const int ni = v.P.ni[p], nj = v.P.nj[p];
     const int nfi = (ni + 1) * nj, nfj = ni * (nj + 1);
@@ -42,7 +47,7 @@ __global__ void k_adj_faces(View v, const double* __restrict__ lam, double* __re
         j = g / ni;
     }
     const long long N = v.ncell;
-    const int D = v.D;
+    const int D = DD;
     long long c[4];
     for (int s = 0; s < 4; ++s)
         c[s] = iface ? cidx(v.P, p, i - 1 + s, j) : cidx(v.P, p, i, j - 1 + s);
@@ -50,9 +55,10 @@ __global__ void k_adj_faces(View v, const double* __restrict__ lam, double* __re
     const bool inL = iface ? i >= 1 : j >= 1;
     const bool inR = iface ? i + 1 <= ni : j + 1 <= nj;
     const double ds = iface ? v.dsi[c[1]] : v.dsj[c[1]];
-    double tgb[NY1 + 3];
+    double tgb[DD];
     bool any = false;
-    for (int k = 0; k < D; ++k) {
+#pragma unroll
+    for (int k = 0; k < DD; ++k) {
         const double rl = inL ? dt / v.Vol[c[1]] * lam[k * N + c[1]] : 0.0;
         const double rr = inR ? dt / v.Vol[c[2]] * lam[k * N + c[2]] : 0.0;
         tgb[k] = ds * (rr - rl);
@@ -60,22 +66,27 @@ __global__ void k_adj_faces(View v, const double* __restrict__ lam, double* __re
     }
     if (!any) return;
     const double phi = v.recon == SCFD_RECON_MUSCL ? v.phi_mus : 0.0, km = v.k_mus;
-    double st[4][NC], wl[NC], wr[NC];
+    // face states first; the stencil is read again (from L1) for the reverse of MUSCL
+    double wl[NC], wr[NC];
+#pragma unroll
     for (int m = 0; m < NC; ++m) {
-        const int kw = wcomp(m, D);
-        for (int s = 0; s < 4; ++s) st[s][m] = v.w[kw * N + c[s]];
-        adj::muscl_fwd(st[0][m], st[1][m], st[2][m], st[3][m], phi, km, wl[m], wr[m]);
+        const double* wk = v.w + wcomp(m, D) * N;
+        adj::muscl_fwd(__ldg(wk + c[0]), __ldg(wk + c[1]), __ldg(wk + c[2]), __ldg(wk + c[3]), phi, km, wl[m], wr[m]);
     }
     const double* vn = iface ? v.vni : v.vnj;
     const double n1 = vn[c[1]], n2 = vn[N + c[1]];
     double wlb[NC] = {0}, wrb[NC] = {0};
     adj::slau_rev(NY1, wl, wr, n1, n2, tgb, wlb, wrb);
+#pragma unroll
     for (int m = 0; m < NC; ++m) {
+        const double* wk = v.w + wcomp(m, D) * N;
         double b[4] = {0, 0, 0, 0};
-        adj::muscl_rev(st[0][m], st[1][m], st[2][m], st[3][m], phi, km, wlb[m], wrb[m], b[0], b[1], b[2], b[3]);
-        const int kw = wcomp(m, D);
+        adj::muscl_rev(__ldg(wk + c[0]), __ldg(wk + c[1]), __ldg(wk + c[2]), __ldg(wk + c[3]), phi, km, wlb[m], wrb[m],
+                       b[0], b[1], b[2], b[3]);
+        double* wb = wbar + wcomp(m, D) * N;
+#pragma unroll
         for (int s = 0; s < 4; ++s)
-            if (b[s] != 0.0) atomicAdd(wbar + kw * N + c[s], b[s]);
+            if (b[s] != 0.0) atomicAdd(wb + c[s], b[s]);
     }
 }
 
@@ -97,9 +108,14 @@ __global__ void k_adj_ghost(View v, const GhostOp* __restrict__ ops, int nops, c
     auto to_grad = [&](int k, double x) {
         if (mine && x != 0.0) atomicAdd(grad + k, x);
     };
+    // the ghost's adjoint is consumed here: clear it for the next step
+    auto clear = [&]() {
+        for (int k = 0; k < W; ++k) wbar[k * N + d] = 0.0;
+    };
     switch (op.kind) {
         case SCFD_BC_FIXED:
             for (int k = 0; k < W; ++k) to_grad(k, wbar[k * N + d]);
+            clear();
             return;
         case SCFD_BC_FIXED_PIN: {
             // w_d = value except rho = pin value[W+nY] / value[W+nY+1], p = pin = w_s(p)
@@ -110,6 +126,7 @@ __global__ void k_adj_ghost(View v, const GhostOp* __restrict__ ops, int nops, c
             to_src(3, pb + rb * a / b);
             to_grad(W + nY, rb * pin / b);
             to_grad(W + nY + 1, -rb * pin * a / (b * b));
+            clear();
             return;
         }
         default:
@@ -135,25 +152,32 @@ __global__ void k_adj_ghost(View v, const GhostOp* __restrict__ ops, int nops, c
         to_grad(0, 2.0 * wbar[N + d]);
         to_grad(1, 2.0 * wbar[2 * N + d]);
     }
+    clear();
 }
 
 // lam_c += (dw/dq)^T wb_c over the interior cells (ideal gas: set_w and the
 // ideal thermal model; gamma, R and mu do not depend on q here)
-__global__ void k_adj_prim(View v, const double* __restrict__ wbar, double* __restrict__ lam) {
+__global__ void k_adj_prim(View v, double* __restrict__ wbar, double* __restrict__ lam) {
     const int p = v.P.act[blockIdx.y];
     const int ni = v.P.ni[p], nj = v.P.nj[p];
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= ni * nj) return;
     const long long N = v.ncell;
     const long long c = cidx(v.P, p, idx % ni + 1, idx / ni + 1);
-    const int D = v.D;
-    double q[NY1 + 3], qb[NY1 + 3] = {0};
+    constexpr int D = DD;
+    double q[DD], qb[DD] = {0};
+#pragma unroll
     for (int k = 0; k < D; ++k) q[k] = v.q[k * N + c];
     double Yb[NY1];
+#pragma unroll
     for (int k = 0; k < NY1; ++k) Yb[k] = wbar[(4 + k) * N + c];
     adj::ideal_prim_rev(NY1, q, v.kappa, wbar[c], wbar[N + c], wbar[2 * N + c], wbar[3 * N + c], Yb,
                         wbar[(D + 2) * N + c], qb);
+#pragma unroll
     for (int k = 0; k < D; ++k) lam[k * N + c] += qb[k];
+    // consumed: clear the components the faces add to (gamma's adjoint has no use here)
+#pragma unroll
+    for (int m = 0; m < NC; ++m) wbar[wcomp(m, D) * N + c] = 0.0;
 }
 
 // the objective's term of one state: J += sum_c wt_c p(q_c), in a fixed order
@@ -162,15 +186,17 @@ __global__ void k_adj_objective(View v, const long long* __restrict__ cells, con
                                 double* J, double* lam, int grad_only) {
     __shared__ double sh[256];
     const long long N = v.ncell;
-    const int D = v.D;
+    constexpr int D = DD;
     double acc = 0.0;
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
         const long long c = cells[t];
-        double q[NY1 + 3];
+        double q[DD];
+#pragma unroll
         for (int k = 0; k < D; ++k) q[k] = v.q[k * N + c];
         if (lam) {
-            double qb[NY1 + 3] = {0};
+            double qb[DD] = {0};
             adj::ideal_p_rev(NY1, q, v.kappa, wt[t], qb);
+#pragma unroll
             for (int k = 0; k < D; ++k) lam[k * N + c] += qb[k];
         }
         if (!grad_only) acc += wt[t] * adj::ideal_p(NY1, q, v.kappa);
@@ -204,7 +230,7 @@ int launch_adj_ghost(const View& v, cudaStream_t s, const GhostOp* ops, int nops
     return 1;
 }
 
-int launch_adj_prim(const View& v, cudaStream_t s, const double* wbar, double* lam) {
+int launch_adj_prim(const View& v, cudaStream_t s, double* wbar, double* lam) {
     int mx = 0;
     for (int a = 0; a < v.P.nact; ++a) {
         const int p = v.P.act[a];

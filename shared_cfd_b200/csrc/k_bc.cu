@@ -71,6 +71,13 @@ __global__ void k_corners(View v) {
         v.vhi[k * N + d] = 1.0 / 3.0 * (v.vhi[k * N + a] + v.vhi[k * N + b] + v.vhi[k * N + c]);
 }
 
+// the ghost-cell writes without set_corners (for stencils that never read corners)
+int launch_ghost_ops(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride) {
+    if (nops <= 0) return 0;
+    k_ghost<<<(nops + 127) / 128, 128, 0, s>>>(v, ops, nops, bcval, valstride);
+    return 1;
+}
+
 int launch_ghosts(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride) {
     int n = 0;
     if (nops > 0) {

@@ -94,6 +94,23 @@ struct scfd_ctx {
     int ds_stage = 0, ds_j = 0;
     long long ds_att0 = 0, ds_fb0 = 0;
     bool own(int p) const { return owner.empty() || owner[p] == rank; }  // p 0-based
+    // discrete adjoint (scfd_adjoint_run): face lengths on the host, and the
+    // device buffers and reverse-step graphs kept from one run to the next
+    std::vector<double> h_dsi, h_dsj;
+    struct AdjCache {
+        double* slots = nullptr;
+        int nslots = 0;
+        double* lam = nullptr;
+        double* wbar = nullptr;
+        double* dgrad = nullptr;
+        double* dJ = nullptr;
+        long long* ocells = nullptr;
+        double* owt = nullptr;
+        cudaGraphExec_t rev_graph[2] = {nullptr, nullptr};
+        int key_obj = -2, key_param = -2;
+        std::vector<std::vector<int>> best_split;  // checkpoint plan of the last (nsteps, snapshots)
+        int plan_n = -1, plan_s = -1;
+    } adj;
     // autotuner (launch shapes of the residual and thermo kernels)
     bool tuned = false;
     std::string tune_report = "{}";
@@ -598,6 +615,11 @@ int scfd_create(const scfd_desc* d, scfd_ctx** out) {
 
 int scfd_destroy(scfd_ctx* c) {
     if (!c) return SCFD_E_ARG;
+    for (auto& g : c->adj.rev_graph)
+        if (g) cudaGraphExecDestroy(g);
+    for (void* b : {(void*)c->adj.slots, (void*)c->adj.lam, (void*)c->adj.wbar, (void*)c->adj.dgrad, (void*)c->adj.dJ,
+                    (void*)c->adj.ocells, (void*)c->adj.owt})
+        if (b) cudaFree(b);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     for (int b = 0; b < 2; ++b) {
         if (c->h_ring[b]) cudaFreeHost(c->h_ring[b]);
@@ -669,6 +691,8 @@ int scfd_commit(scfd_ctx* c) {
     CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     HostGeo g;
     build_geometry(c, g);
+    c->h_dsi = g.dsi;
+    c->h_dsj = g.dsj;
     std::vector<GhostOp> ops;
     int st = build_ghost_ops(c, g, ops);
     if (st) return st;
@@ -1432,6 +1456,7 @@ struct AdjRun {
     int nobj = 0;
     long long fwd = 0, rev = 0;
     int visited = 0;           // highest step index whose state has been formed
+    cudaGraphExec_t* rev_graph = nullptr;  // [2]: reverse step without / with the objective term (context-owned)
 
     bool in_window(int n) const { return n >= d->win_first && n <= d->win_last; }
     int save(int slot) {
@@ -1457,23 +1482,64 @@ struct AdjRun {
         }
         return 0;
     }
-    // q^n in the context; lam = dJ/dq^{n+1} -> dJ/dq^n
-    int step_back(int n) {
+    // the kernels of one reverse step (captured once per variant into a CUDA graph)
+    void enqueue_back(bool obj) {
         const View& v = c->v;
         cudaStream_t s = c->stream;
         launch_thermo(v, s, c->cells_max);
-        launch_ghosts(v, s, c->d_ops, c->nops, c->d_bcval, c->valstride);
-        CK(cudaMemsetAsync(wbar, 0, sizeof(double) * (size_t)c->W * c->ncell, s));
+        launch_ghost_ops(v, s, c->d_ops, c->nops, c->d_bcval, c->valstride);
         launch_adj_faces(v, s, lam, wbar, dt);
         launch_adj_ghost(v, s, c->d_ops, c->nops, c->d_bcval, c->valstride, wbar, dgrad, d->param_bc);
         launch_adj_prim(v, s, wbar, lam);
-        if (in_window(n)) launch_adj_objective(v, s, ocells, owt, nobj, nullptr, lam, 1);
-        CK(cudaGetLastError());
+        if (obj) launch_adj_objective(v, s, ocells, owt, nobj, nullptr, lam, 1);
+    }
+    // q^n in the context; lam = dJ/dq^{n+1} -> dJ/dq^n
+    int step_back(int n) {
+        const int var = in_window(n) ? 1 : 0;
+        if (!rev_graph[var]) {
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            enqueue_back(var == 1);
+            const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            if (e != cudaSuccess) return c->fail(SCFD_E_CUDA, std::string("adjoint graph capture: ") + cudaGetErrorString(e));
+            const cudaError_t ei = cudaGraphInstantiate(&rev_graph[var], g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) {
+                rev_graph[var] = nullptr;
+                return c->fail(SCFD_E_CUDA, std::string("adjoint graph instantiate: ") + cudaGetErrorString(ei));
+            }
+        }
+        CK(cudaGraphLaunch(rev_graph[var], c->stream));
+        c->launches += 6 + var;
         ++rev;
         return 0;
     }
+    // optimal first stored state of a segment (dynamic programming over the cost
+    // F(l, s) = min over l1 of l1 + F(l - l1, s - 1) + F(l1, s) of this
+    // recursion, in forward steps), when the table is affordable
+    std::vector<std::vector<int>> best_split;
+    void plan(int n, int S) {
+        // with a stored state per step (or none) the split rule below is already optimal
+        if (S < 1 || S >= n - 1 || (double)n * n * S > 2e9) return;
+        std::vector<std::vector<long long>> F(S + 1, std::vector<long long>(n + 1, 0));
+        best_split.assign(S + 1, std::vector<int>(n + 1, 1));
+        for (int l = 1; l <= n; ++l) F[0][l] = (long long)l * (l - 1) / 2;
+        for (int sf = 1; sf <= S; ++sf)
+            for (int l = 2; l <= n; ++l) {
+                long long bestc = -1;
+                for (int l1 = 1; l1 < l; ++l1) {
+                    const long long cst = l1 + F[sf - 1][l - l1] + F[sf][l1];
+                    if (bestc < 0 || cst < bestc) {
+                        bestc = cst;
+                        best_split[sf][l] = l1;
+                    }
+                }
+                F[sf][l] = bestc;
+            }
+    }
     int split(int a, int b, int sfree) const {
         const int n = b - a;
+        if (sfree < (int)best_split.size() && n < (int)best_split[sfree].size()) return a + best_split[sfree][n];
         int t = 1;
         while (binom_steps(sfree, t) < n) ++t;
         const long long tail = binom_steps(sfree - 1, t);
@@ -1520,62 +1586,98 @@ int scfd_adjoint_run(scfd_ctx* c, const scfd_adj_desc* d, double* J, double* gra
     r.d = d;
     r.dt = cd.dt_fixed;
     r.qsz = (size_t)c->D * c->ncell;
+    auto& A = c->adj;
+    const int S = d->forward_only ? 0 : std::min(d->snapshots, d->nsteps);
+    // buffers: allocated once per context (the state slots grow when a run needs more)
+    if (!A.lam) {
+        int mx = 1;
+        for (int p = 0; p < c->np; ++p) mx = std::max(mx, std::max(c->P.ni[p], c->P.nj[p]));
+        if (cudaMalloc(&A.lam, sizeof(double) * r.qsz) != cudaSuccess ||
+            cudaMalloc(&A.wbar, sizeof(double) * (size_t)c->W * c->ncell) != cudaSuccess ||
+            cudaMalloc(&A.dgrad, sizeof(double) * c->valstride) != cudaSuccess ||
+            cudaMalloc(&A.dJ, sizeof(double)) != cudaSuccess ||
+            cudaMalloc(&A.ocells, sizeof(long long) * mx) != cudaSuccess ||
+            cudaMalloc(&A.owt, sizeof(double) * mx) != cudaSuccess) {
+            cudaGetLastError();
+            return c->fail(SCFD_E_CUDA, "no device memory for the adjoint");
+        }
+    }
+    if (A.nslots < S + 1) {
+        if (A.slots) cudaFree(A.slots);
+        A.slots = nullptr;
+        A.nslots = 0;
+        if (cudaMalloc(&A.slots, sizeof(double) * r.qsz * (S + 1)) != cudaSuccess) {
+            cudaGetLastError();
+            return c->fail(SCFD_E_CUDA, "no device memory for the adjoint's stored states");
+        }
+        A.nslots = S + 1;
+    }
+    r.slots = A.slots;
+    r.nslots = S + 1;
+    r.lam = A.lam;
+    r.wbar = A.wbar;
+    r.dgrad = A.dgrad;
+    r.dJ = A.dJ;
+    r.ocells = A.ocells;
+    r.owt = A.owt;
     // objective cells: the first interior cells along the descriptor's range, weighted by the face length
     {
         const scfd_bc& b = c->bcs[d->obj_bc];
         const int p = b.plane - 1, ni = c->P.ni[p], nj = c->P.nj[p];
-        std::vector<long long> cells, faces;
+        std::vector<long long> cells;
+        std::vector<double> wt;
         for (int sx = b.first; sx <= b.last; ++sx) {
             switch (b.side) {
-                case SCFD_SIDE_ILO: cells.push_back(cidx(c->P, p, 1, sx)); faces.push_back(cidx(c->P, p, 0, sx)); break;
-                case SCFD_SIDE_IHI: cells.push_back(cidx(c->P, p, ni, sx)); faces.push_back(cidx(c->P, p, ni, sx)); break;
-                case SCFD_SIDE_JLO: cells.push_back(cidx(c->P, p, sx, 1)); faces.push_back(cidx(c->P, p, sx, 0)); break;
-                default: cells.push_back(cidx(c->P, p, sx, nj)); faces.push_back(cidx(c->P, p, sx, nj)); break;
+                case SCFD_SIDE_ILO: cells.push_back(cidx(c->P, p, 1, sx)); wt.push_back(c->h_dsi[cidx(c->P, p, 0, sx)]); break;
+                case SCFD_SIDE_IHI: cells.push_back(cidx(c->P, p, ni, sx)); wt.push_back(c->h_dsi[cidx(c->P, p, ni, sx)]); break;
+                case SCFD_SIDE_JLO: cells.push_back(cidx(c->P, p, sx, 1)); wt.push_back(c->h_dsj[cidx(c->P, p, sx, 0)]); break;
+                default: cells.push_back(cidx(c->P, p, sx, nj)); wt.push_back(c->h_dsj[cidx(c->P, p, sx, nj)]); break;
             }
         }
-        const double* ds = (b.side == SCFD_SIDE_ILO || b.side == SCFD_SIDE_IHI) ? c->v.dsi : c->v.dsj;
-        std::vector<double> wt(cells.size());
-        for (size_t k = 0; k < cells.size(); ++k)
-            CK(cudaMemcpy(&wt[k], ds + faces[k], sizeof(double), cudaMemcpyDeviceToHost));
         r.nobj = (int)cells.size();
-        CK(cudaMalloc(&r.ocells, sizeof(long long) * std::max(1, r.nobj)));
-        CK(cudaMalloc(&r.owt, sizeof(double) * std::max(1, r.nobj)));
-        CK(cudaMemcpy(r.ocells, cells.data(), sizeof(long long) * cells.size(), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(r.owt, wt.data(), sizeof(double) * wt.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(r.ocells, cells.data(), sizeof(long long) * cells.size(), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(r.owt, wt.data(), sizeof(double) * wt.size(), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
     }
-    const int S = d->forward_only ? 0 : std::min(d->snapshots, d->nsteps);
-    r.nslots = S + 1;
+    // the reverse-step graphs bake the descriptor indices in: rebuild them when those change
+    if (A.key_obj != d->obj_bc || A.key_param != d->param_bc) {
+        for (auto& g : A.rev_graph)
+            if (g) cudaGraphExecDestroy(g);
+        A.rev_graph[0] = A.rev_graph[1] = nullptr;
+        A.key_obj = d->obj_bc;
+        A.key_param = d->param_bc;
+    }
+    r.rev_graph = A.rev_graph;
     int st = 0;
-    auto fail_free = [&](int code) {
-        cudaFree(r.slots); cudaFree(r.lam); cudaFree(r.wbar); cudaFree(r.dgrad); cudaFree(r.dJ);
-        cudaFree(r.ocells); cudaFree(r.owt);
-        return code;
-    };
-    if (cudaMalloc(&r.slots, sizeof(double) * r.qsz * r.nslots) != cudaSuccess ||
-        cudaMalloc(&r.dgrad, sizeof(double) * c->valstride) != cudaSuccess ||
-        cudaMalloc(&r.dJ, sizeof(double)) != cudaSuccess ||
-        (!d->forward_only && (cudaMalloc(&r.lam, sizeof(double) * r.qsz) != cudaSuccess ||
-                              cudaMalloc(&r.wbar, sizeof(double) * (size_t)c->W * c->ncell) != cudaSuccess))) {
-        cudaGetLastError();
-        return fail_free(c->fail(SCFD_E_CUDA, "no device memory for the adjoint's states"));
-    }
     for (int k = S; k >= 1; --k) r.free_slot.push_back(k);
+    if (!d->forward_only) {
+        if (A.plan_n != d->nsteps || A.plan_s != S) {
+            r.plan(d->nsteps, S);
+            A.best_split = std::move(r.best_split);
+            A.plan_n = d->nsteps;
+            A.plan_s = S;
+        }
+        r.best_split = A.best_split;
+    }
     DevScalars sc0;
-    if ((st = sync_scalars(c))) return fail_free(st);
+    if ((st = sync_scalars(c))) return st;
     sc0 = *c->h_sc;
     CK(cudaMemsetAsync(r.dJ, 0, sizeof(double), c->stream));
     CK(cudaMemsetAsync(r.dgrad, 0, sizeof(double) * c->valstride, c->stream));
-    if (!d->forward_only) CK(cudaMemsetAsync(r.lam, 0, sizeof(double) * r.qsz, c->stream));
+    if (!d->forward_only) {
+        CK(cudaMemsetAsync(r.lam, 0, sizeof(double) * r.qsz, c->stream));
+        CK(cudaMemsetAsync(r.wbar, 0, sizeof(double) * (size_t)c->W * c->ncell, c->stream));
+    }
     c->launches = 0;
-    if ((st = r.save(0))) return fail_free(st);
+    if ((st = r.save(0))) return st;
     if (r.in_window(0)) launch_adj_objective(c->v, c->stream, r.ocells, r.owt, r.nobj, r.dJ, nullptr, 0);
     if (d->forward_only)
         st = r.advance(0, d->win_last);
     else
         st = r.revolve(0, d->nsteps, 0);
-    if (st) return fail_free(st);
+    if (st) return st;
     // the uploaded state back: q, qp, qpp and the scalars
-    if ((st = r.restore(0))) return fail_free(st);
+    if ((st = r.restore(0))) return st;
     const size_t qb = sizeof(double) * r.qsz;
     CK(cudaMemcpyAsync(c->v.qp, c->v.q, qb, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemcpyAsync(c->v.qpp, c->v.q, qb, cudaMemcpyDeviceToDevice, c->stream));
@@ -1587,7 +1689,6 @@ int scfd_adjoint_run(scfd_ctx* c, const scfd_adj_desc* d, double* J, double* gra
         counts[0] = r.fwd;
         counts[1] = r.rev;
     }
-    fail_free(0);
     return 0;
 }
 

@@ -118,6 +118,7 @@ struct GhostOp {
 // kernels / launchers (stream-ordered); each returns the number of launches
 int launch_thermo(const View& v, cudaStream_t s, int cells_per_plane_max);
 int launch_ghosts(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride);
+int launch_ghost_ops(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride);
 int launch_set_dt(const View& v, cudaStream_t s);
 int launch_set_dt_cells(const View& v, cudaStream_t s);  // dt_mat and the local minimum only
 int launch_residual(const View& v, cudaStream_t s, int mode, bool need_coeffs);
@@ -200,7 +201,7 @@ int launch_status_import(const View& v, cudaStream_t s, const double* red);
 int launch_adj_faces(const View& v, cudaStream_t s, const double* lam, double* wbar, double dt);
 int launch_adj_ghost(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride,
                      double* wbar, double* grad, int param_bc);
-int launch_adj_prim(const View& v, cudaStream_t s, const double* wbar, double* lam);
+int launch_adj_prim(const View& v, cudaStream_t s, double* wbar, double* lam);
 int launch_adj_objective(const View& v, cudaStream_t s, const long long* cells, const double* wt, int n, double* J,
                          double* lam, int grad_only);
 
