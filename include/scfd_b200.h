@@ -54,7 +54,9 @@ enum {
     SCFD_E_CONNECT      = 9,  /* bad connectivity record                          */
     SCFD_E_IO           = 10, /* file input / output                              */
     SCFD_E_STATE        = 11, /* call out of order (e.g. step before commit)      */
-    SCFD_E_UNSUPPORTED  = 12  /* option combination not provided                 */
+    SCFD_E_UNSUPPORTED  = 12, /* option combination not provided                 */
+    SCFD_E_SINGULAR     = 13  /* CEA Newton matrix singular twice in one cell: the
+                                 reference stops the program (NASA/core/sub_chem.f90:1472-1488) */
 };
 
 /* ---- option enums (values follow checkout.inp where one exists) ------- */
@@ -388,6 +390,79 @@ int   scfd_reactors_run(scfd_reactors* r, const scfd_reactor_desc* d, const doub
 void* scfd_reactors_stream(scfd_reactors* r);
 /* kernel launches made by the last scfd_reactors_launch */
 int   scfd_reactors_launch_count(const scfd_reactors* r, int64_t* launches);
+
+/* ---- CEA equilibrium thermochemistry (NASA/core) ------------------------ */
+/* Per-cell chemical equilibrium at given density, internal energy and
+ * fuel/oxidizer mass fractions: `cea` of store/therm_lib/NASA/core/sub_chem.f90
+ * (1320-1651), a Newton iteration on the element potentials pi_i and ln T with
+ * a dense (ne+1) x (ne+1) pivoted LU (NASA/core/LU.f90), NASA-9 polynomials
+ * (NASA/core/thermo.inp, 7 coefficients + 2 integration constants per
+ * temperature section) and Wilke-mixed viscosity fits (NASA/core/trans.inp).
+ * Units follow the reference: n in mol/kg, E in J/kg, MW in g/mol. */
+#define SCFD_CEA_MAX_SPECIES   32
+#define SCFD_CEA_MAX_ELEMENTS  6
+#define SCFD_CEA_MAX_SECTIONS  6   /* thermo temperature sections (chem module: co(9,6,:)) */
+#define SCFD_CEA_MAX_TSECTIONS 3   /* viscosity temperature sections (trans(4,3,:))      */
+
+/* Tables of one species set, as set_therm_data / set_trans_data /
+ * read_fo_composition read them (sub_chem.f90:70-305). */
+typedef struct scfd_cea_data {
+    int32_t abi_version;
+    int32_t ns, ne, nt;    /* species, elements, species with a viscosity fit */
+    int32_t nsec[SCFD_CEA_MAX_SPECIES];                            /* num_sctn */
+    double  trange[SCFD_CEA_MAX_SPECIES][SCFD_CEA_MAX_SECTIONS][2];/* Trange(1:2,l,j) K */
+    double  co[SCFD_CEA_MAX_SPECIES][SCFD_CEA_MAX_SECTIONS][9];    /* co(1:9,l,j) */
+    double  mw[SCFD_CEA_MAX_SPECIES];                              /* g/mol */
+    double  ac[SCFD_CEA_MAX_SPECIES][SCFD_CEA_MAX_ELEMENTS];       /* Ac(i,j): atoms of element i in species j */
+    double  mwe[SCFD_CEA_MAX_ELEMENTS];                            /* element weights, MW.inp */
+    int32_t ntsec[SCFD_CEA_MAX_SPECIES];                           /* num_sctn_trans */
+    int32_t tr2th[SCFD_CEA_MAX_SPECIES];                           /* 0-based species of each fit */
+    double  trange_t[SCFD_CEA_MAX_SPECIES][SCFD_CEA_MAX_TSECTIONS][2];
+    double  trans[SCFD_CEA_MAX_SPECIES][SCFD_CEA_MAX_TSECTIONS][4];/* ln mu = A ln T + B/T + C/T^2 + D */
+    double  pf, Tf, po, To;                                        /* fuel / oxidizer stream, Pa and K */
+    double  nf[SCFD_CEA_MAX_SPECIES], no[SCFD_CEA_MAX_SPECIES];    /* stream mole ratios */
+    int32_t reserved[8];
+} scfd_cea_data;
+
+/* The fuel and oxidizer states initialize_cea('uv') derives
+ * (sub_chem.f90:1136-1230): element amounts b0 (mol/kg), element mass
+ * fractions, the equilibrium state of each stream at its own density and
+ * energy, and the initial value of every cell's saved composition n_save. */
+typedef struct scfd_cea_stream {
+    double rho, p, T, e, h, mw, kappa, mu;
+    double b0[SCFD_CEA_MAX_ELEMENTS];
+    double ye[SCFD_CEA_MAX_ELEMENTS];
+    double n[SCFD_CEA_MAX_SPECIES];
+} scfd_cea_stream;
+typedef struct scfd_cea_info {
+    scfd_cea_stream fuel, oxidizer;
+    double of;        /* oxidizer/fuel mass ratio of the stream compositions */
+    double n_init;    /* n_save initial value: sum(no + nf) / ns */
+    int32_t iters_fuel, iters_oxidizer;
+    int32_t reserved[6];
+} scfd_cea_info;
+
+typedef struct scfd_cea scfd_cea;
+
+/* Parses nothing: builds the element lists and masks of initialize_cea and
+ * solves the two stream states.  SCFD_E_ARG for counts out of range. */
+int  scfd_cea_create(const scfd_cea_data* data, scfd_cea** out);
+int  scfd_cea_destroy(scfd_cea* cea);
+int  scfd_cea_info_get(const scfd_cea* cea, scfd_cea_info* info);
+/* One `cea` call per cell on DEVICE arrays, component-major: Y[2][ncell]
+ * (fuel, oxidizer mass fractions), n[ns][ncell], Yv[ns][ncell],
+ * vhi[ns][ncell], DHi[2][ncell]; T and n are the reference's intent(inout)
+ * guess / result.  Outputs other than T and n may be NULL; iters[ncell]
+ * receives the Newton iterations (0 when the entry state already satisfies
+ * the convergence test).  Enqueued on `stream` (cudaStream_t or NULL). */
+int  scfd_cea_solve(scfd_cea* cea, int64_t ncell, const double* rho, const double* Y, const double* e,
+                    double* T, double* n, double* mwave, double* kappa, double* mu, double* Yv,
+                    double* vhi, double* DHi, int32_t* iters, void* stream);
+/* Synchronises the last solve's stream and returns, in counts[0..1], the
+ * cells of the solves since the previous call that stopped at the
+ * 500-iteration limit (the reference prints "not converted. at cea" and goes
+ * on) and that met a singular matrix twice (SCFD_E_SINGULAR is returned). */
+int  scfd_cea_status(scfd_cea* cea, int64_t* counts);
 
 /* ---- no-allocation entry point ------------------------------------------ */
 /* Capacity of the library's static scratch for scfd_rms_noalloc: partial sums

@@ -14,10 +14,11 @@ BC_MAXVAL = 2 * MAX_SPECIES + 8
 
 # status codes
 OK, E_ARG, E_CUDA, E_TNEWTON, E_CHEM, E_OMEGA, E_RESRATE, E_NAN, E_SPIN, E_CONNECT, E_IO, E_STATE, \
-    E_UNSUPPORTED = range(13)
+    E_UNSUPPORTED, E_SINGULAR = range(14)
 STATUS_NAMES = {
     0: "OK", 1: "E_ARG", 2: "E_CUDA", 3: "E_TNEWTON", 4: "E_CHEM", 5: "E_OMEGA", 6: "E_RESRATE",
     7: "E_NAN", 8: "E_SPIN", 9: "E_CONNECT", 10: "E_IO", 11: "E_STATE", 12: "E_UNSUPPORTED",
+    13: "E_SINGULAR",
 }
 
 DIM_2D, DIM_Q2D = 0, 1
@@ -165,6 +166,56 @@ class ReactorDesc(C.Structure):
     ]
 
 
+# CEA equilibrium tables (scfd_cea_data / scfd_cea_info)
+CEA_MAX_SPECIES, CEA_MAX_ELEMENTS, CEA_MAX_SECTIONS, CEA_MAX_TSECTIONS = 32, 6, 6, 3
+
+
+class CeaData(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32),
+        ("ns", C.c_int32),
+        ("ne", C.c_int32),
+        ("nt", C.c_int32),
+        ("nsec", C.c_int32 * CEA_MAX_SPECIES),
+        ("trange", C.c_double * (CEA_MAX_SPECIES * CEA_MAX_SECTIONS * 2)),
+        ("co", C.c_double * (CEA_MAX_SPECIES * CEA_MAX_SECTIONS * 9)),
+        ("mw", C.c_double * CEA_MAX_SPECIES),
+        ("ac", C.c_double * (CEA_MAX_SPECIES * CEA_MAX_ELEMENTS)),
+        ("mwe", C.c_double * CEA_MAX_ELEMENTS),
+        ("ntsec", C.c_int32 * CEA_MAX_SPECIES),
+        ("tr2th", C.c_int32 * CEA_MAX_SPECIES),
+        ("trange_t", C.c_double * (CEA_MAX_SPECIES * CEA_MAX_TSECTIONS * 2)),
+        ("trans", C.c_double * (CEA_MAX_SPECIES * CEA_MAX_TSECTIONS * 4)),
+        ("pf", C.c_double),
+        ("Tf", C.c_double),
+        ("po", C.c_double),
+        ("To", C.c_double),
+        ("nf", C.c_double * CEA_MAX_SPECIES),
+        ("no", C.c_double * CEA_MAX_SPECIES),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
+class CeaStream(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("rho", "p", "T", "e", "h", "mw", "kappa", "mu")] + [
+        ("b0", C.c_double * CEA_MAX_ELEMENTS),
+        ("ye", C.c_double * CEA_MAX_ELEMENTS),
+        ("n", C.c_double * CEA_MAX_SPECIES),
+    ]
+
+
+class CeaInfo(C.Structure):
+    _fields_ = [
+        ("fuel", CeaStream),
+        ("oxidizer", CeaStream),
+        ("of", C.c_double),
+        ("n_init", C.c_double),
+        ("iters_fuel", C.c_int32),
+        ("iters_oxidizer", C.c_int32),
+        ("reserved", C.c_int32 * 6),
+    ]
+
+
 # Exported entry points: name -> (restype, argtypes); the prefix (scfd_ for the
 # CUDA library) is added by bind().
 _P = C.c_void_p
@@ -207,6 +258,11 @@ SIGNATURES = {
                                C.POINTER(C.c_int32)]),
     "reactors_stream": (_P, [_P]),
     "reactors_launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "cea_create": (C.c_int, [C.POINTER(CeaData), C.POINTER(_P)]),
+    "cea_destroy": (C.c_int, [_P]),
+    "cea_info_get": (C.c_int, [_P, C.POINTER(CeaInfo)]),
+    "cea_solve": (C.c_int, [_P, C.c_int64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "cea_status": (C.c_int, [_P, C.POINTER(C.c_int64)]),
 }
 K_THERMO, K_BC, K_DT, K_CHEM, K_RESIDUAL, K_SWEEP_FWD, K_SWEEP_BWD, K_UPDATE, K_COPY, K_OTHER, K_PACK, K_COUNT = \
     range(12)

@@ -49,12 +49,13 @@ def test_struct_sizes_match_c(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text('#include <stdio.h>\n#include "%s"\nint main(void){printf("%%zu %%zu %%zu %%zu %%zu\\n",'
                    'sizeof(scfd_desc),sizeof(scfd_bc),sizeof(scfd_chem),sizeof(scfd_stats),'
-                   'sizeof(scfd_reactor_desc));return 0;}\n' % HEADER)
+                   'sizeof(scfd_reactor_desc));printf("%%zu %%zu\\n",sizeof(scfd_cea_data),'
+                   'sizeof(scfd_cea_info));return 0;}\n' % HEADER)
     exe = tmp_path / "sz"
     subprocess.check_call(["gcc", "-o", str(exe), str(src)])
     out = [int(v) for v in subprocess.check_output([str(exe)]).split()]
     assert out == [C.sizeof(abi.Desc), C.sizeof(abi.BC), C.sizeof(abi.Chem), C.sizeof(abi.Stats),
-                   C.sizeof(abi.ReactorDesc)]
+                   C.sizeof(abi.ReactorDesc), C.sizeof(abi.CeaData), C.sizeof(abi.CeaInfo)]
 
 
 def test_create_rejects_bad_descriptors_without_gpu():
