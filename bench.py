@@ -2,7 +2,7 @@
 """Benchmark of the per-step residual-and-implicit-update path on B200.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
-                    [--config reacting_step|flat_plate|sod|reactors] [--scale S]
+                    [--config reacting_step|flat_plate|sod|reactors|adjoint|cea] [--scale S]
 
 Metric: Mcell-iter/s (cells x inner iterations per second; for the explicit
 Euler configuration one step is one iteration), mixed (FP32 reconstruction,
@@ -12,6 +12,8 @@ C ABI with host buffers copied in and the result copied out every step.
 
 --config reactors measures the batched 0-D reactors instead: reactors/s for
 one batch of 8192 H2/air reactors integrated to 2 ms (a step is one batch).
+--config cea measures the CEA equilibrium solve: Mcell/s over 2^22 cells, each
+step a warm-started re-solve of every cell.
 
 One JSON line is printed by rank 0.  Under torchrun (N > 1) the flow
 configurations are block-sharded over the ranks (strong scaling: the same
@@ -120,6 +122,7 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.f = None
+        self.skip = 0
 
     def __enter__(self):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
@@ -132,6 +135,13 @@ class ClockSampler:
                  "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        # the first sample takes a moment: start timing only once it is in
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and os.path.getsize(self.f.name) == 0 and self.proc.poll() is None:
+            time.sleep(0.02)
+        with open(self.f.name) as f:
+            self.skip = len([r for r in f.read().splitlines() if r.strip()])
         return self
 
     def __exit__(self, *a):
@@ -148,6 +158,10 @@ class ClockSampler:
             with open(self.f.name) as f:
                 rows = [r.split(",") for r in f.read().strip().splitlines() if r.strip()]
             os.unlink(self.f.name)
+            # samples taken before the timed region began are dropped (kept
+            # when nothing else arrived, so that a short region still reports)
+            if len(rows) > self.skip:
+                rows = rows[self.skip:]
         except OSError:
             return None
         sm, mx, reasons = [], None, set()
@@ -460,6 +474,193 @@ def run_reactors(args, rank, cores):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# CEA chemical equilibrium (scfd_cea_solve)
+# ---------------------------------------------------------------------------
+CEA_N = 1 << 22
+CEA_DE = 0.01
+
+
+def cea_workload():
+    return ("%d cells of CEA chemical equilibrium at fixed density, energy and fuel / oxidizer mass fractions: "
+            "H2 against air over 9 H/O/N species (3 elements, NASA-9 data); seeded states (Y_fuel = u^3, "
+            "rho 0.2-2 kg/m^3, e = mixed-stream e + 0-3 MJ/kg); each step re-solves every cell from the previous "
+            "step's T and n with e alternately raised and lowered by %g of |e| (the warm start of the flow "
+            "model's saved n)" % (CEA_N, CEA_DE))
+
+
+def cea_states(info):
+    from shared_cfd_b200 import cea
+    rho, Y, e, T = cea.random_states(info, CEA_N, seed=21)
+    return rho, Y, e, e + CEA_DE * np.abs(e), T
+
+
+def cpu_cea(cores, seconds=10.0):
+    """The CPU restatement on the benchmark workload: one cold solve
+    (untimed), then warm steps until `seconds` have passed (at least 2)."""
+    from shared_cfd_b200 import cea
+    so = os.path.join(ROOT, "oracle", "_build", "liborc.so")
+    if not os.path.exists(so):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    orc = abi.Bound(C.CDLL(so), "orc_")
+    with cea.Cea(cea.h2_air_data(), lib=orc) as m:
+        rho, Y, e0, e1, T = cea_states(m.info())
+        n = m.initial_n(CEA_N)
+        Tp = np.empty(CEA_N)
+        np.copyto(Tp, T)
+        z = np.zeros(CEA_N)
+        zs = np.zeros((m.ns, CEA_N))
+        zz = np.zeros((m.ns, CEA_N))
+        d2 = np.zeros((2, CEA_N))
+        it = np.zeros(CEA_N, dtype=np.int32)
+        z1, z2 = np.zeros(CEA_N), np.zeros(CEA_N)
+
+        def step(e):
+            m.solve_ptr(CEA_N, rho.ctypes.data, Y.ctypes.data, e.ctypes.data, Tp.ctypes.data, n.ctypes.data,
+                        z.ctypes.data, z1.ctypes.data, z2.ctypes.data, zs.ctypes.data, zz.ctypes.data,
+                        d2.ctypes.data, it.ctypes.data, None)
+        step(e0)
+        k, t0 = 0, time.perf_counter()
+        while k < 2 or time.perf_counter() - t0 < seconds:
+            step(e1 if k % 2 == 0 else e0)
+            k += 1
+        dt = time.perf_counter() - t0
+        return CEA_N * k / dt / 1e6, dt, k
+
+
+def run_cea(args, rank, cores):
+    """One JSON line for the CEA equilibrium batch (rank 0 only; the cells are
+    independent and the benchmark does not shard them)."""
+    unit = "Mcell/s"
+    metric = "Mcell/s of CEA equilibrium solves (FP64)"
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        val, dt, k = cpu_cea(cores)
+        print(json.dumps({
+            "impl": "reference", "metric": metric, "value": val, "unit": unit, "n_gpus": args.gpus, "steps": k,
+            "warmup": 1, "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": {"workload": cea_workload()},
+            "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port",
+                             "sample": "%d warm steps of the full workload (%.1f s) on %d OpenMP threads, C++ FP64 "
+                                       "restatement of cea" % (k, dt, cores)},
+            "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
+    if rank != 0:
+        return 0
+    import torch
+    from shared_cfd_b200 import build, cea
+    build.build()
+    g = cea.Cea(cea.h2_air_data())
+    info = g.info()
+    ns = g.ns
+    rho, Y, e0, e1, T = cea_states(info)
+    dev = torch.device("cuda", 0)
+
+    def t(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    d = {"rho": t(rho), "Y": t(Y), "e0": t(e0), "e1": t(e1), "T": t(T), "n": t(np.full((ns, CEA_N), info.n_init))}
+    outs = [torch.empty(CEA_N, dtype=torch.float64, device=dev) for _ in range(3)] + \
+        [torch.empty((ns, CEA_N), dtype=torch.float64, device=dev) for _ in range(2)] + \
+        [torch.empty((2, CEA_N), dtype=torch.float64, device=dev)]
+    it = torch.empty(CEA_N, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def solve(e):
+        g.solve_device(d["rho"], d["Y"], e, d["T"], d["n"], *outs, iters=it, stream=stream)
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    # cold start from the initial n_save: one launch, its own sub-measure
+    torch.cuda.synchronize(dev)
+    ev[0].record(stream)
+    solve(d["e0"])
+    ev[1].record(stream)
+    torch.cuda.synchronize(dev)
+    cold_ms = ev[0].elapsed_time(ev[1])
+    cold_it = float(it.float().mean())
+    code, nc, ng = g.status()
+    if code or ng:
+        raise RuntimeError("cea status %d (%d singular)" % (code, ng))
+    k = 0
+    for _ in range(max(3, args.warmup)):
+        solve(d["e1"] if k % 2 == 0 else d["e0"])
+        k += 1
+    torch.cuda.synchronize(dev)
+    with ClockSampler(0) as cs:
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            solve(d["e1"] if k % 2 == 0 else d["e0"])
+            k += 1
+        ev[1].record(stream)
+        torch.cuda.synchronize(dev)
+    ms = ev[0].elapsed_time(ev[1]) / args.steps
+    warm_it = float(it.float().mean())
+    code, nc, ng = g.status()
+    if code or ng:
+        raise RuntimeError("cea status %d (%d singular)" % (code, ng))
+    value = CEA_N / (ms * 1e-3) / 1e6
+    # end to end through the same call with host buffers: the step's inputs
+    # (rho, Y, e, T, n) copied in from pinned memory, every output copied back
+    hp = {k_: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k_, v in
+          (("rho", rho), ("Y", Y), ("e0", e0), ("e1", e1))}
+    hT = d["T"].cpu().pin_memory()
+    hn = d["n"].cpu().pin_memory()
+    hout = [torch.empty(o.shape, dtype=o.dtype).pin_memory() for o in outs]
+    dd = {k_: torch.empty_like(d[k_]) for k_ in ("rho", "Y", "T", "n")}
+    de = torch.empty_like(d["e0"])
+
+    def e2e_step(e_host):
+        dd["rho"].copy_(hp["rho"], non_blocking=True)
+        dd["Y"].copy_(hp["Y"], non_blocking=True)
+        de.copy_(e_host, non_blocking=True)
+        dd["T"].copy_(hT, non_blocking=True)
+        dd["n"].copy_(hn, non_blocking=True)
+        g.solve_device(dd["rho"], dd["Y"], de, dd["T"], dd["n"], *outs, stream=stream)
+        hT.copy_(dd["T"], non_blocking=True)
+        hn.copy_(dd["n"], non_blocking=True)
+        for h, o in zip(hout, outs):
+            h.copy_(o, non_blocking=True)
+        torch.cuda.synchronize(dev)
+    for _ in range(2):
+        e2e_step(hp["e1"] if k % 2 == 0 else hp["e0"])
+        k += 1
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step(hp["e1"] if k % 2 == 0 else hp["e0"])
+        k += 1
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    g.close()
+    h2d = 8 * CEA_N * (1 + 2 + 1 + 1 + ns)
+    d2h = 8 * CEA_N * (1 + ns + 3 + 2 * ns + 2)
+    peak, src = measured_peaks()
+    bpl = 8 * CEA_N * ((1 + 2 + 1 + 1 + ns) + (1 + ns + 3 + 2 * ns + 2))
+    ach = bpl / (ms * 1e-3) / 1e9
+    line = {
+        "metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": cea_workload(), "cells": CEA_N,
+                   "l2": "inputs and outputs (%d MB per step) are larger than L2" % (bpl // 10**6)},
+        "newton_iterations_mean": warm_it,
+        "cold_start": {"value": CEA_N / (cold_ms * 1e-3) / 1e6, "unit": unit, "newton_iterations_mean": cold_it,
+                       "note": "one launch from the initial n_save (sum(no + nf) / ns in every cell)"},
+        "e2e": {"value": CEA_N / e2e_s / 1e6, "unit": unit, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": args.steps, "clocks": cs.summary(),
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                     "peak_source": src, "traffic": None, "bytes_per_cell": bpl // CEA_N,
+                     "note": "the kernel is FP64 latency-bound (a Newton iteration of exp / log per species per "
+                             "cell); HBM carries only its inputs and outputs"},
+    }
+    if not args.no_cpu_baseline:
+        v_cpu, dt, kc = cpu_cea(cores)
+        line["cpu_baseline"] = {"value": v_cpu, "unit": unit, "cores": cores, "kind": "port",
+                                "sample": "%d warm steps of the full workload (%.1f s) on %d OpenMP threads, C++ FP64 "
+                                          "restatement of cea" % (kc, dt, cores)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -467,11 +668,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="reacting_step",
-                    choices=["reacting_step", "flat_plate", "sod", "reactors", "adjoint"])
+                    choices=["reacting_step", "flat_plate", "sod", "reactors", "adjoint", "cea"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sharded", action="store_true", help="block-sharded path also at N = 1 (needs torchrun)")
+    ap.add_argument("--cea-cells", type=int, default=0, help="cells of --config cea (default 2^22)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -482,6 +684,11 @@ def main():
         return run_reactors(args, rank, cores)
     if args.config == "adjoint":
         return run_adjoint(args, rank, cores)
+    if args.config == "cea":
+        if args.cea_cells > 0:
+            global CEA_N
+            CEA_N = args.cea_cells
+        return run_cea(args, rank, cores)
 
     if args.impl == "reference":
         if rank != 0:

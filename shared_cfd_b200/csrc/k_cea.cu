@@ -15,9 +15,9 @@
 // the Wilke-mixed viscosity.
 //
 // Layout: one thread per cell; the species vectors are register arrays of a
-// compile-time length (12 species / 4 elements / 3 temperature sections for
-// the hydrogen-air sets, 32 / 6 / 6 otherwise) and the tables are staged in
-// shared memory once per block.  Cells where one stream is absent
+// compile-time length (exactly 9 species / 3 elements for the hydrogen-air
+// set, up to 12 / 4 with 3 temperature sections, 32 / 6 / 6 otherwise) and the
+// tables are staged in shared memory once per block.  Cells where one stream is absent
 // (Y < 1e-6) drop the elements only that stream carries; the reference
 // compresses the system to the kept rows (sub_chem.f90:1456-1469), this kernel
 // keeps the full system and makes the dropped rows and columns identity rows,
@@ -65,6 +65,7 @@ struct CeaTab {
     double keepf[NE], keepo[NE]; // maskbf / maskbo of the elements
 };
 
+using TabH2Air = CeaTab<9, 3, 3>;   // the 9-species H/O/N set, exactly
 using TabSmall = CeaTab<12, 4, 3>;
 using TabBig = CeaTab<SCFD_CEA_MAX_SPECIES, SCFD_CEA_MAX_ELEMENTS, SCFD_CEA_MAX_SECTIONS>;
 
@@ -150,8 +151,10 @@ struct CellOut {
     int32_t* iters;
 };
 
-template <int NS, int NE, int NSEC>
-__global__ void __launch_bounds__(128) k_cea(const CeaTab<NS, NE, NSEC>* __restrict__ gtab, int64_t ncell,
+// EXACT: the species set has exactly NS species and NE elements, so that the
+// counts are compile-time constants and no register holds an unused slot.
+template <int NS, int NE, int NSEC, bool EXACT, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_cea(const CeaTab<NS, NE, NSEC>* __restrict__ gtab, int64_t ncell,
                                              const double* __restrict__ rho_in, const double* __restrict__ Y_in,
                                              const double* __restrict__ E_in, double* __restrict__ T_io,
                                              double* __restrict__ n_io, CellOut out,
@@ -166,7 +169,7 @@ __global__ void __launch_bounds__(128) k_cea(const CeaTab<NS, NE, NSEC>* __restr
     const Tab& t = *reinterpret_cast<const Tab*>(smem_tab);
     const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
-    const int ns = t.ns, ne = t.ne, nt = t.nt;
+    const int ns = EXACT ? NS : t.ns, ne = EXACT ? NE : t.ne, nt = t.nt;
     constexpr int M = NE + 1;
 
     const double rho = rho_in[c], Y0 = Y_in[c], Y1 = Y_in[ncell + c], E = E_in[c];
@@ -296,8 +299,7 @@ __global__ void __launch_bounds__(128) k_cea(const CeaTab<NS, NE, NSEC>* __restr
                 bd[r] = 0.0;
             }
             // LU.f90: partial pivoting (first largest |A(i,k)|), singular when
-            // the pivot is below 1e-30; rows are swapped by value so that the
-            // arrays stay in registers
+            // the pivot is below 1e-30
             bool sing = false;
 #pragma unroll
             for (int k = 0; k < M; ++k) {
@@ -312,18 +314,20 @@ __global__ void __launch_bounds__(128) k_cea(const CeaTab<NS, NE, NSEC>* __restr
                     }
                 }
                 if (p < 1e-30) sing = true;
+                // unconditional selects: a predicated swap makes the
+                // compiler index the rows by ip and move A to local memory
 #pragma unroll
                 for (int i = k + 1; i < M; ++i) {
-                    if (i != ip) continue;
+                    const bool sw = i == ip;
 #pragma unroll
                     for (int j = 0; j < M; ++j) {
-                        const double x = A[k][j];
-                        A[k][j] = A[i][j];
-                        A[i][j] = x;
+                        const double x = A[k][j], y = A[i][j];
+                        A[k][j] = sw ? y : x;
+                        A[i][j] = sw ? x : y;
                     }
-                    const double x = bd[k];
-                    bd[k] = bd[i];
-                    bd[i] = x;
+                    const double x = bd[k], y = bd[i];
+                    bd[k] = sw ? y : x;
+                    bd[i] = sw ? x : y;
                 }
                 const double inv = 1.0 / A[k][k];
 #pragma unroll
@@ -498,13 +502,18 @@ __global__ void __launch_bounds__(128) k_cea(const CeaTab<NS, NE, NSEC>* __restr
         // calc_vTmu (func_chem.f90:143-155) and the Wilke mixing rule
         const double tt = 1.0 / (T * T);
         const double vmu1 = tt * T, vmu2 = tt;
-        double muN[NS];
+        // sqrt(muN_i / muN_j) as sqrt(muN_i) * rsqrt(muN_j): nt square roots
+        // instead of nt^2 (a few ulp apart from the quotient's root)
+        double sq[NS], rs[NS];
 #pragma unroll
         for (int i = 0; i < NS; ++i) {
+            sq[i] = rs[i] = 0.0;
             if (i >= nt) continue;
             const int s = tsection(t.tthi[i], t.ttlo[i], t.ntsec[i], T);
             const double* a = t.trans[i][s];
-            muN[i] = exp(a[0] * logT + a[1] * vmu1 + a[2] * vmu2 + a[3] * 1.0);
+            const double muN = exp(a[0] * logT + a[1] * vmu1 + a[2] * vmu2 + a[3] * 1.0);
+            sq[i] = sqrt(muN);
+            rs[i] = rsqrt(muN);
         }
         double nfit[NS];  // n(tr2th(i))
 #pragma unroll
@@ -522,11 +531,11 @@ __global__ void __launch_bounds__(128) k_cea(const CeaTab<NS, NE, NSEC>* __restr
 #pragma unroll
             for (int j = 0; j < NS; ++j) {
                 if (j >= nt) continue;
-                const double f = 1.0 + sqrt(muN[i] / muN[j]) * t.wmw[i][j];
+                const double f = 1.0 + sq[i] * rs[j] * t.wmw[i][j];
                 const double phi = 0.25 * (f * f) * t.wsq[i][j];
                 denom += nfit[j] * phi;
             }
-            mu += nfit[i] * muN[i] / denom;
+            mu += nfit[i] * (sq[i] * sq[i]) / denom;
         }
         out.mu[c] = mu * 1e-7;
     }
@@ -583,10 +592,12 @@ void fill_tab(Tab& t, const scfd_cea_data& d, const double* b0f, const double* b
 
 }  // namespace
 
+enum { KIND_9_3 = 0, KIND_SMALL = 1, KIND_BIG = 2 };
+
 struct scfd_cea {
     scfd_cea_data data;
     scfd_cea_info info;
-    bool small = true;
+    int kind = KIND_SMALL;
     void* d_tab = nullptr;
     size_t tab_bytes = 0;
     unsigned long long* d_fail = nullptr;
@@ -601,11 +612,16 @@ int cea_launch(scfd_cea* h, int64_t ncell, const double* rho, const double* Y, c
     const int threads = 128;
     const int64_t blocks = (ncell + threads - 1) / threads;
     if (blocks > 0x7fffffff) return SCFD_E_ARG;
-    if (h->small)
-        k_cea<12, 4, 3><<<(unsigned)blocks, threads, sizeof(TabSmall), st>>>(
+    // three resident blocks of 128 threads (168 registers) measured faster
+    // than two (no spills) and than four (more spills) on B200
+    if (h->kind == KIND_9_3)
+        k_cea<9, 3, 3, true, 3><<<(unsigned)blocks, threads, sizeof(TabH2Air), st>>>(
+            (const TabH2Air*)h->d_tab, ncell, rho, Y, e, T, n, out, h->d_fail);
+    else if (h->kind == KIND_SMALL)
+        k_cea<12, 4, 3, false, 3><<<(unsigned)blocks, threads, sizeof(TabSmall), st>>>(
             (const TabSmall*)h->d_tab, ncell, rho, Y, e, T, n, out, h->d_fail);
     else
-        k_cea<SCFD_CEA_MAX_SPECIES, SCFD_CEA_MAX_ELEMENTS, SCFD_CEA_MAX_SECTIONS>
+        k_cea<SCFD_CEA_MAX_SPECIES, SCFD_CEA_MAX_ELEMENTS, SCFD_CEA_MAX_SECTIONS, false, 1>
             <<<(unsigned)blocks, threads, sizeof(TabBig), st>>>((const TabBig*)h->d_tab, ncell, rho, Y, e, T, n,
                                                                  out, h->d_fail);
     return cudaGetLastError() == cudaSuccess ? 0 : SCFD_E_CUDA;
@@ -744,9 +760,14 @@ int scfd_cea_create(const scfd_cea_data* data, scfd_cea** out) {
     int nsecmax = 1, ntsecmax = 1;
     for (int j = 0; j < ns; ++j) nsecmax = std::max(nsecmax, d.nsec[j]);
     for (int i = 0; i < d.nt; ++i) ntsecmax = std::max(ntsecmax, d.ntsec[i]);
-    h->small = ns <= 12 && ne <= 4 && nsecmax <= 3 && ntsecmax <= 3;
+    const bool small = nsecmax <= 3 && ntsecmax <= 3;
+    h->kind = small && ns == 9 && ne == 3 ? KIND_9_3 : (small && ns <= 12 && ne <= 4 ? KIND_SMALL : KIND_BIG);
     std::vector<char> tab;
-    if (h->small) {
+    if (h->kind == KIND_9_3) {
+        tab.resize(sizeof(TabH2Air));
+        fill_tab(*(TabH2Air*)tab.data(), d, b0f, b0o, inf.fuel.ye, inf.oxidizer.ye, maskf.data(), masko.data(),
+                 keepf, keepo, yac);
+    } else if (h->kind == KIND_SMALL) {
         tab.resize(sizeof(TabSmall));
         fill_tab(*(TabSmall*)tab.data(), d, b0f, b0o, inf.fuel.ye, inf.oxidizer.ye, maskf.data(), masko.data(),
                  keepf, keepo, yac);

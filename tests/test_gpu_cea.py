@@ -105,6 +105,20 @@ def test_generic_kernel_matches_restatement(gpu, orc):
         compare(a, b, 17)
 
 
+def test_twelve_species_kernel_matches_restatement(gpu, orc):
+    # 8 of the 9 species: the library's kernel for up to 12 species / 4
+    # elements with runtime counts
+    d = cea.h2_air_data(species=["H2", "O2", "H2O", "H", "O", "OH", "HO2", "N2"])
+    with cea.Cea(d, lib=gpu) as g, cea.Cea(d, lib=orc) as o:
+        inf = o.info()
+        rho, Y, e, T = cea.random_states(inf, 2048, seed=6)
+        n0 = o.initial_n(2048)
+        a = g.solve(rho, Y, e, T, n0)
+        b = o.solve(rho, Y, e, T, n0)
+        assert b["not_converged"] == 0
+        compare(a, b, 8)
+
+
 def test_device_api_optional_outputs_and_empty_batch(pair):
     import torch
     _, g, o = pair
