@@ -349,7 +349,8 @@ int  scfd_dstep(scfd_ctx* ctx, int step, scfd_dreq* req, scfd_stats* stats);
  * T >= T0 + dT_ign, interpolated linearly between the accepted substeps around
  * it (the state at t = 0 is the first of them).  Where the reference hands the
  * rest of a call to DVODE after 10 CHEMEQ2 attempts, the library takes
- * two-stage Rosenbrock (ROS2) substeps and flags the reactor
+ * two-stage Rosenbrock (ROS2) substeps on Fex and its exact Jacobian Jex
+ * (FJ.f90:152-300, 454-709, the pair the reference hands DVODE) and flags the reactor
  * SCFD_REACTOR_FELL_BACK. */
 enum {
     SCFD_REACTOR_QUEUE = 0,      /* one persistent launch, reactors drawn from a device work queue
@@ -380,7 +381,7 @@ int   scfd_reactors_upload(scfd_reactors* r, int n, const double* T0, const doub
 int   scfd_reactors_launch(scfd_reactors* r, const scfd_reactor_desc* d);
 /* after a launch: T_end[n], vrho_end[n][ns], t_ign[n] (s, -1 when T never
  * reached T0 + dT_ign), evals[n] = source-term (Fex_var) evaluations (2 per
- * CHEMEQ2 attempt, ns+3 per Rosenbrock substep), flags[n]; any pointer may be
+ * CHEMEQ2 attempt, 2 per Rosenbrock substep: one Jex, one Fex), flags[n]; any pointer may be
  * NULL.  Returns the worst status of the run. */
 int   scfd_reactors_download(scfd_reactors* r, double* T_end, double* vrho_end, double* t_ign, int64_t* evals,
                              int32_t* flags);
@@ -390,6 +391,15 @@ int   scfd_reactors_run(scfd_reactors* r, const scfd_reactor_desc* d, const doub
 void* scfd_reactors_stream(scfd_reactors* r);
 /* kernel launches made by the last scfd_reactors_launch */
 int   scfd_reactors_launch_count(const scfd_reactors* r, int64_t* launches);
+
+/* ---- chemical source terms and their Jacobian -------------------------- */
+/* Fex and Jex (store/therm_lib/chemkin/uvhp/uv/FJ.f90:152-300 and 454-709), the
+ * right-hand side and exact Jacobian the reference hands DVODE, for n states
+ * at once on the device.  states[n][ns+1] = (n_1..n_ns in mol/cm^3, T in K);
+ * dndt[n][ns+1] receives the net rates and dT/dt at constant volume;
+ * jac[n][ns+1][ns+1] (row-major, d dndt_i / d state_j) the Jacobian, or
+ * nothing when jac is NULL.  Host arrays; returns when the results are in. */
+int  scfd_chem_rates(const scfd_chem* chem, int n, const double* states, double* dndt, double* jac);
 
 /* ---- CEA equilibrium thermochemistry (NASA/core) ------------------------ */
 /* Per-cell chemical equilibrium at given density, internal energy and

@@ -503,6 +503,171 @@ void fex_var(const scfd_chem& ch, const double* n, double* dndtp, double* dndtm)
     dndtm[ns] = std::min(-de * T / cv, 0.0);
 }
 
+// Fex (J == nullptr; FJ.f90:152-300) or Jex (FJ.f90:454-709): net rates dndt of
+// the species and dT/dt at constant volume, and with J the exact Jacobian,
+// row-major (ns+1) x (ns+1), J[i*(ns+1)+j] = d dndt_i / d n_j (T last).  The
+// T-derivative coefficients are those of set_coeff_more (sub_chem.f90:91-150).
+void fex_jex(const scfd_chem& ch, const double* n, double* dndt, double* J) {
+    const int ns = ch.ns, N = ns + 1;
+    const bool jac = J != nullptr;
+    const double T = n[ns];
+    const double logT = std::log(T), Tinv = 1.0 / T;
+    const double logPRT = std::log(pst / Ru_cgs) - logT;
+    double sn = 0.0;
+    for (int j = 0; j < ns; ++j) sn += n[j];
+    if (jac) sn = std::max(sn, 1e-300);
+    const double logsn = std::log(sn);
+    const double Ti2 = Tinv * Tinv, T2 = T * T, T3 = T2 * T, T4 = T3 * T;
+    const double cmurt[7] = {1.0 - logT, -T / 2.0, -T2 / 6.0, -T3 / 12.0, -T4 / 20.0, Tinv, -1.0};
+    const double chrt[7] = {1.0, T / 2.0, T2 / 3.0, T3 / 4.0, T4 / 5.0, Tinv, 0.0};
+    const double ccpr[7] = {1.0, T, T2, T3, T4, 0.0, 0.0};
+    const double cdmurt[7] = {-Tinv, -1.0 / 2.0, -T / 3.0, -T2 / 4.0, -T3 / 5.0, -Ti2, 0.0};
+    const double cdcpr[7] = {0.0, 1.0, 2.0 * T, 3.0 * T2, 4.0 * T3, 0.0, 0.0};
+    double vmu0rt[SCFD_MAX_SPECIES], vdmu0rt[SCFD_MAX_SPECIES], vert[SCFD_MAX_SPECIES], vcvr[SCFD_MAX_SPECIES],
+        vdcvrdT[SCFD_MAX_SPECIES];
+    for (int j = 0; j < ns; ++j) {
+        const int s = sec_of(ch, j, T);
+        double t1 = 0.0, t2 = 0.0, t3 = -1.0, t4 = -1.0, t5 = 0.0;
+        for (int i = 0; i < 7; ++i) {
+            const double tmp = ch.coeff[j][s][i];
+            t1 = t1 + tmp * cmurt[i];
+            t2 = t2 + tmp * cdmurt[i];
+            t3 = t3 + tmp * chrt[i];
+            t4 = t4 + tmp * ccpr[i];
+            t5 = t5 + tmp * cdcpr[i];
+        }
+        vmu0rt[j] = t1;
+        vdmu0rt[j] = t2;
+        vert[j] = t3;
+        vcvr[j] = t4;
+        vdcvrdT[j] = t5;
+        dndt[j] = 0.0;
+        if (jac)
+            for (int i = 0; i < N; ++i) J[j * N + i] = 0.0;
+    }
+    const double dd = 0.14;
+    double vM = 0.0, vlogM = 0.0, dlnkdlnM = 0.0;
+    double drdn[SCFD_MAX_SPECIES + 1];
+    for (int i = 0; i < ch.nr; ++i) {
+        if (ch.exist_m[i]) {
+            double tmp = sn;
+            for (int j = 0; j < ch.numm[i]; ++j) tmp = tmp + ch.men[i][j] * n[ch.indm[i][j]];
+            vM = tmp;
+            vlogM = (tmp == sn) ? logsn : std::log(tmp);
+        }
+        double vlogk1 = ch.abe[i][0] + ch.abe[i][1] * logT - ch.abe[i][2] * Tinv;
+        double dlnkdT1 = (ch.abe[i][1] + ch.abe[i][2] * Tinv) * Tinv;
+        double vlogk2 = 0.0, dlnkdT2 = 0.0;
+        if (ch.rstate[i][1] >= 4) {
+            vlogk1 = vlogk1 + vlogM;
+            dlnkdlnM = 1.0;
+        }
+        if (ch.rstate[i][0] == 0) {
+            if (ch.rstate[i][1] == 1 || ch.rstate[i][1] == 5) {
+                vlogk2 = ch.cabe[i][0] + ch.cabe[i][1] * logT - ch.cabe[i][2] * Tinv;
+                dlnkdT2 = (ch.cabe[i][1] + ch.cabe[i][2] * Tinv) * Tinv;
+                if (ch.rstate[i][1] == 5) vlogk2 = vlogk2 + vlogM;
+            } else {
+                if (ch.rstate[i][1] == 2 || ch.rstate[i][1] == 3) {
+                    const double logk0 = ch.cabe[i][0] + ch.cabe[i][1] * logT - ch.cabe[i][2] * Tinv;
+                    const double dlnk0dT = (ch.cabe[i][1] + ch.cabe[i][2] * Tinv) * Tinv;
+                    const double logkinf = vlogk1, dlnkinfdT = dlnkdT1;
+                    const double log_Pr = logk0 - logkinf + vlogM;
+                    const double Pr = std::exp(log_Pr);
+                    vlogk1 = logkinf + std::log(Pr / (1.0 + Pr));
+                    dlnkdT1 = (dlnk0dT + Pr * dlnkinfdT) / (1.0 + Pr);
+                    dlnkdlnM = 1.0 / (1.0 + Pr);
+                    if (ch.rstate[i][1] == 3) {
+                        const double dlnPrdT = dlnk0dT - dlnkinfdT;
+                        const double aa = ch.troe[i][0];
+                        const double Fcent = (1.0 - aa) * std::exp(-T * ch.troe[i][1]) +
+                                             aa * std::exp(-T * ch.troe[i][2]) + std::exp(-ch.troe[i][3] * Tinv);
+                        const double dFcentdT = -(1.0 - aa) * ch.troe[i][1] * std::exp(-T * ch.troe[i][1]) -
+                                                aa * ch.troe[i][2] * std::exp(-T * ch.troe[i][2]) +
+                                                ch.troe[i][3] * sq(Tinv) * std::exp(-ch.troe[i][3] * Tinv);
+                        const double dlnFcentdT = dFcentdT / Fcent;
+                        const double logFcent = std::log10(Fcent);
+                        const double cc = -0.4 - 0.67 * logFcent;
+                        const double nn = 0.75 - 1.27 * logFcent;
+                        const double logPrc = log_Pr * loge210 + cc;
+                        const double temp1 = logPrc / (nn - dd * logPrc);
+                        const double temp2 = 1.0 / (1.0 + sq(temp1));
+                        const double logF = temp2 * logFcent;
+                        vlogk1 = vlogk1 + logF / loge210;
+                        dlnkdT1 = dlnkdT1 + temp2 * (-2.0 * logF * temp1 / sq(nn - dd * logPrc) *
+                                                         (nn * dlnPrdT + (1.27 * logPrc - 0.67 * nn) * dlnFcentdT) +
+                                                     dlnFcentdT);
+                        dlnkdlnM = dlnkdlnM - 2.0 * temp2 * logF * temp1 / sq(nn - dd * logPrc) * nn;
+                    }
+                }
+                double numu0rt = 0.0, nudmu0rt = 0.0;
+                for (int k = 0; k < ch.numnu[i][0]; ++k) {
+                    numu0rt = numu0rt - vmu0rt[ch.indnu[i][0][k]];
+                    nudmu0rt = nudmu0rt - vdmu0rt[ch.indnu[i][0][k]];
+                }
+                for (int k = 0; k < ch.numnu[i][1]; ++k) {
+                    numu0rt = numu0rt + vmu0rt[ch.indnu[i][1][k]];
+                    nudmu0rt = nudmu0rt + vdmu0rt[ch.indnu[i][1][k]];
+                }
+                vlogk2 = vlogk1 - ch.snu[i] * logPRT + numu0rt;
+                dlnkdT2 = dlnkdT1 + ch.snu[i] * Tinv + nudmu0rt;
+            }
+        }
+        for (int k = 0; k < ns; ++k) drdn[k] = 0.0;
+        double r = std::exp(vlogk1);
+        for (int k = 0; k < ch.numnu[i][0]; ++k) r = r * n[ch.indnu[i][0][k]];
+        double Dr = r;
+        drdn[ns] = dlnkdT1 * r;
+        for (int k = 0; k < ch.numnu[i][0]; ++k) {
+            const int it = ch.indnu[i][0][k];
+            drdn[it] = drdn[it] + r / n[it];
+        }
+        if (ch.rstate[i][0] == 0) {
+            r = std::exp(vlogk2);
+            for (int k = 0; k < ch.numnu[i][1]; ++k) r = r * n[ch.indnu[i][1][k]];
+            Dr = Dr - r;
+            drdn[ns] = drdn[ns] - r * dlnkdT2;
+            for (int k = 0; k < ch.numnu[i][1]; ++k) {
+                const int it = ch.indnu[i][1][k];
+                drdn[it] = drdn[it] - r / n[it];
+            }
+        }
+        if (ch.exist_m[i]) {
+            const double temp1 = Dr * dlnkdlnM / vM;
+            for (int k = 0; k < ns; ++k) drdn[k] = drdn[k] + temp1;
+            for (int k = 0; k < ch.numm[i]; ++k) drdn[ch.indm[i][k]] = drdn[ch.indm[i][k]] + temp1 * ch.men[i][k];
+        }
+        for (int k = 0; k < ch.numnu[i][0]; ++k) {
+            const int it = ch.indnu[i][0][k];
+            dndt[it] = dndt[it] - Dr;
+            if (jac)
+                for (int j = 0; j < N; ++j) J[it * N + j] = J[it * N + j] - drdn[j];
+        }
+        for (int k = 0; k < ch.numnu[i][1]; ++k) {
+            const int it = ch.indnu[i][1][k];
+            dndt[it] = dndt[it] + Dr;
+            if (jac)
+                for (int j = 0; j < N; ++j) J[it * N + j] = J[it * N + j] + drdn[j];
+        }
+    }
+    double de = 0.0, cv = 0.0, dcv = 0.0, temp1 = 0.0, temp2 = 0.0;
+    for (int j = 0; j < ns; ++j) {
+        if (jac) temp1 = temp1 + vert[j] * J[j * N + ns];
+        de = de + vert[j] * dndt[j];
+        dcv = dcv + vcvr[j] * dndt[j];
+        cv = cv + vcvr[j] * n[j];
+        temp2 = temp2 + vdcvrdT[j] * n[j];
+    }
+    dndt[ns] = -de * T / cv;
+    if (!jac) return;
+    J[ns * N + ns] = -(T * temp1 + dcv + dndt[ns] * temp2) / cv;
+    for (int j = 0; j < ns; ++j) {
+        double t = 0.0;
+        for (int k = 0; k < ns; ++k) t = t + vert[k] * J[k * N + j];
+        J[ns * N + j] = -(T * t + dndt[ns] * vcvr[j]) / cv;
+    }
+}
+
 }  // namespace
 
 namespace {
@@ -525,11 +690,6 @@ void track_ignition(Ignition& g, double tt, double T) {
     }
     g.T_old = T;
     g.t_old = t;
-}
-
-void rates(const scfd_chem& ch, const double* y, double* f, double* tmp) {
-    fex_var(ch, y, f, tmp);
-    for (int i = 0; i <= ch.ns; ++i) f[i] = f[i] + tmp[i];
 }
 
 // CHEMEQ2 tolerance y*rtol + rtol*1e-5 for the species (sub_chem.f90:1801), rtol*T for T
@@ -576,15 +736,15 @@ void lu_solve(const double* M, const int* piv, int N, double* b) {
 // Spee, Blom, Hundsdorfer, SIAM J. Sci. Comput. 20, 1999), gamma = 1 + 1/sqrt(2),
 //     (I - gamma h J) k1 = f(y0),  (I - gamma h J) k2 = f(y0 + h k1) - 2 k1,
 //     y = y0 + 3/2 h k1 + 1/2 h k2,  error |h/2 (k1 + k2)|,
-// with a forward-difference Jacobian at y0 and step factor 0.8/sqrt(err) in
-// [0.2, 2].  y holds the accepted state at tt on entry and the state at tout
+// with f = Fex and J = Jex at y0 (the pair the reference hands DVODE, mf = 21)
+// and step factor 0.8/sqrt(err) in [0.2, 2].  y holds the accepted state at tt on entry and the state at tout
 // on return.  The same substeps as be_attempt of the CUDA path, in the same order.
 int implicit_rest(const scfd_chem& ch, double* y, double tt, double tout, double dt, double rtol,
                   long long& attempts, int& substeps, int max_substeps, Ignition* ign, long long& evals,
                   double& h_carry) {
     const int ns = ch.ns, N = ns + 1;
     const double gam = 1.7071067811865475;
-    double y0[SCFD_MAX_SPECIES + 1], f0[SCFD_MAX_SPECIES + 1], f[SCFD_MAX_SPECIES + 1], tmp[SCFD_MAX_SPECIES + 1],
+    double y0[SCFD_MAX_SPECIES + 1], f0[SCFD_MAX_SPECIES + 1], f[SCFD_MAX_SPECIES + 1],
         k1[SCFD_MAX_SPECIES + 1], k2[SCFD_MAX_SPECIES + 1], M[(SCFD_MAX_SPECIES + 1) * (SCFD_MAX_SPECIES + 1)];
     int piv[SCFD_MAX_SPECIES + 1];
     for (int i = 0; i < N; ++i) y0[i] = y[i];
@@ -594,20 +754,16 @@ int implicit_rest(const scfd_chem& ch, double* y, double tt, double tout, double
         ++attempts;
         double h = dt;
         if (tout - tt < h) h = tout - tt;
-        rates(ch, y0, f0, tmp);
-        for (int j = 0; j < N; ++j) {
-            for (int i = 0; i < N; ++i) y[i] = y0[i];
-            const double dj = 1.4901161193847656e-8 * std::max(std::fabs(y0[j]), j < ns ? 1e-10 : 1.0);
-            y[j] = y0[j] + dj;
-            rates(ch, y, f, tmp);
-            for (int i = 0; i < N; ++i) M[i * N + j] = (i == j ? 1.0 : 0.0) - gam * h * (f[i] - f0[i]) / dj;
-        }
+        // M = I - gamma h J with Jex's exact Jacobian at y0; f0 = Fex(y0) (Jex's dndt)
+        fex_jex(ch, y0, f0, M);
+        for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N; ++j) M[i * N + j] = (i == j ? 1.0 : 0.0) - gam * h * M[i * N + j];
         double err = 1e300;
         if (lu_factor(M, piv, N)) {
             for (int i = 0; i < N; ++i) k1[i] = f0[i];
             lu_solve(M, piv, N, k1);
             for (int i = 0; i < N; ++i) y[i] = y0[i] + h * k1[i];
-            rates(ch, y, f, tmp);
+            fex_jex(ch, y, f, nullptr);
             for (int i = 0; i < N; ++i) k2[i] = f[i] - 2.0 * k1[i];
             lu_solve(M, piv, N, k2);
             err = 0.0;
@@ -617,7 +773,7 @@ int implicit_rest(const scfd_chem& ch, double* y, double tt, double tout, double
                 err = (e > err || e != e) ? e : err;
             }
         }
-        evals += N + 2;
+        evals += 2;
         if (!(err <= 1.0)) {
             dt = h * (err == err && err < 1e300 ? std::max(0.2, 0.8 / std::sqrt(err)) : 0.25);
             if (++rejects > 30) return SCFD_E_CHEM;
@@ -2417,6 +2573,16 @@ int orc_kernel_stats(orc_ctx* c, int kind, double* ms, int64_t* n, char* name, i
 int orc_calc_T(const scfd_chem* ch, const double* vrho, double rho, double E, double* T, double* kappa,
                double* MW, double* DHi, double* vhi, double* mu) {
     return calc_T(*ch, vrho, rho, E, *T, *kappa, *MW, DHi, vhi, *mu);
+}
+
+int orc_chem_rates(const scfd_chem* ch, int n, const double* states, double* dndt, double* jac) {
+    if (!ch || n < 0 || (n > 0 && (!states || !dndt)) || ch->ns < 1 || ch->ns > SCFD_MAX_SPECIES ||
+        ch->nr < 0 || ch->nr > SCFD_MAX_REACTIONS)
+        return SCFD_E_ARG;
+    const int N = ch->ns + 1;
+    for (int c = 0; c < n; ++c)
+        fex_jex(*ch, states + (size_t)c * N, dndt + (size_t)c * N, jac ? jac + (size_t)c * N * N : nullptr);
+    return 0;
 }
 
 int orc_fex_var(const scfd_chem* ch, const double* n, double* p, double* m) {

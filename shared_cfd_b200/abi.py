@@ -258,6 +258,7 @@ SIGNATURES = {
                                C.POINTER(C.c_int32)]),
     "reactors_stream": (_P, [_P]),
     "reactors_launch_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "chem_rates": (C.c_int, [C.POINTER(Chem), C.c_int, _D, _D, _D]),
     "cea_create": (C.c_int, [C.POINTER(CeaData), C.POINTER(_P)]),
     "cea_destroy": (C.c_int, [_P]),
     "cea_info_get": (C.c_int, [_P, C.POINTER(CeaInfo)]),

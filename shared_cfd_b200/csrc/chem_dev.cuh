@@ -1,8 +1,8 @@
-// chem_dev.cuh -- device restatement of the UV source terms Fex_var
-// (store/therm_lib/chemkin/uvhp/uv/FJ.f90:301-453) and of one CHEMEQ2 attempt
-// (store/therm_lib/chemkin/core/sub_chem.f90:1714-1819), with the implicit
-// substeps that take over where the reference calls DVODE; shared by the flow
-// chemistry kernel and the batched 0-D reactors.
+// chem_dev.cuh -- device restatement of the UV source terms Fex_var, Fex and
+// their exact Jacobian Jex (store/therm_lib/chemkin/uvhp/uv/FJ.f90:152-709) and
+// of one CHEMEQ2 attempt (store/therm_lib/chemkin/core/sub_chem.f90:1714-1819),
+// with the implicit substeps that take over where the reference calls DVODE;
+// shared by the flow chemistry kernel and the batched 0-D reactors.
 #pragma once
 
 #include "scfd_internal.h"
@@ -154,6 +154,240 @@ __device__ inline void dev_fex_var(const DevChem& ch, const double* n, double* d
     dndtm[ns] = fmin(-de * f.T / cv, 0.0);
 }
 
+// T-derivatives of mu0/RT and cv/R per NASA-7 coefficient (the cdmurt and
+// cdcpr of set_coeff_more, store/therm_lib/chemkin/core/sub_chem.f90:91-150).
+__device__ inline void jex_pre(double T, double* cdmurt, double* cdcpr) {
+    const double Ti1 = 1.0 / T, Ti2 = Ti1 * Ti1, T2 = T * T, T3 = T2 * T;
+    cdmurt[0] = -Ti1;
+    cdmurt[1] = -1.0 / 2.0;
+    cdmurt[2] = -T / 3.0;
+    cdmurt[3] = -T2 / 4.0;
+    cdmurt[4] = -T3 / 5.0;
+    cdmurt[5] = -Ti2;
+    cdmurt[6] = 0.0;
+    cdcpr[0] = 0.0;
+    cdcpr[1] = 1.0;
+    cdcpr[2] = 2.0 * T;
+    cdcpr[3] = 3.0 * T2;
+    cdcpr[4] = 4.0 * T3;
+    cdcpr[5] = 0.0;
+    cdcpr[6] = 0.0;
+}
+
+// mu0/RT, its T-derivative, e/RT, cv/R and its T-derivative of species j (Jex).
+__device__ inline void species_thermo_d(const DevChem& ch, int j, const FexPre& f, const double* cdmurt,
+                                        const double* cdcpr, double& mu, double& dmu, double& e, double& cv,
+                                        double& dcv) {
+    const double* cf = ch.coeff + (j * 2 + (f.T <= ch.tcommon[j] ? 0 : 1)) * 7;
+    double t1 = 0.0, t2 = 0.0, t3 = -1.0, t4 = -1.0, t5 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        const double c = cf[i];
+        t1 = t1 + c * f.cmurt[i];
+        t2 = t2 + c * cdmurt[i];
+        t3 = t3 + c * f.chrt[i];
+        t4 = t4 + c * f.ccpr[i];
+        t5 = t5 + c * cdcpr[i];
+    }
+    mu = t1;
+    dmu = t2;
+    e = t3;
+    cv = t4;
+    dcv = t5;
+}
+
+// One reaction of Jex (store/therm_lib/chemkin/uvhp/uv/FJ.f90:519-660): its
+// net rate Dr and the derivatives drdn[0..ns] of Dr with respect to n_1..n_ns
+// and T, before the third-body term (reaction_jac_m).  vlogM is the
+// third-body term in effect; dlnkdlnM is set when this reaction has a
+// third-body or fall-off rate, and otherwise keeps the value of an earlier
+// reaction (the reference's variable lives across the reaction loop).
+__device__ inline void reaction_jac(const DevChem& ch, int i, const double* n, const FexPre& f, double vlogM,
+                                    const double* vmu0rt, const double* vdmu0rt, double& dlnkdlnM, double& Dr,
+                                    double* drdn) {
+    const double loge210 = (double)0.43429448190325f;
+    const double dd = 0.14;
+    const int ns = ch.ns;
+    const int rs0 = ch.rstate[2 * i], rs1 = ch.rstate[2 * i + 1];
+    const double* abe = ch.abe + 3 * i;
+    double vlogk1 = abe[0] + abe[1] * f.logT - abe[2] * f.Tinv;
+    double dlnkdT1 = (abe[1] + abe[2] * f.Tinv) * f.Tinv;
+    double vlogk2 = 0.0, dlnkdT2 = 0.0;
+    if (rs1 >= 4) {
+        vlogk1 = vlogk1 + vlogM;
+        dlnkdlnM = 1.0;
+    }
+    const int* ind = ch.indnu + 6 * i;
+    const int nreac = ch.numnu[2 * i], nprod = ch.numnu[2 * i + 1];
+    if (rs0 == 0) {
+        const double* cabe = ch.cabe + 3 * i;
+        if (rs1 == 1 || rs1 == 5) {
+            vlogk2 = cabe[0] + cabe[1] * f.logT - cabe[2] * f.Tinv;
+            dlnkdT2 = (cabe[1] + cabe[2] * f.Tinv) * f.Tinv;
+            if (rs1 == 5) vlogk2 = vlogk2 + vlogM;
+        } else {
+            if (rs1 == 2 || rs1 == 3) {
+                const double logk0 = cabe[0] + cabe[1] * f.logT - cabe[2] * f.Tinv;
+                const double dlnk0dT = (cabe[1] + cabe[2] * f.Tinv) * f.Tinv;
+                const double logkinf = vlogk1, dlnkinfdT = dlnkdT1;
+                const double log_Pr = logk0 - logkinf + vlogM;
+                const double Pr = exp(log_Pr);
+                vlogk1 = logkinf + log(Pr / (1.0 + Pr));
+                dlnkdT1 = (dlnk0dT + Pr * dlnkinfdT) / (1.0 + Pr);
+                dlnkdlnM = 1.0 / (1.0 + Pr);
+                if (rs1 == 3) {
+                    const double* tr = ch.troe + 4 * i;
+                    const double dlnPrdT = dlnk0dT - dlnkinfdT;
+                    const double aa = tr[0];
+                    const double e2 = exp(-f.T * tr[1]), e3 = exp(-f.T * tr[2]), e4 = exp(-tr[3] * f.Tinv);
+                    const double Fcent = (1.0 - aa) * e2 + aa * e3 + e4;
+                    const double dFcentdT = -(1.0 - aa) * tr[1] * e2 - aa * tr[2] * e3 + tr[3] * (f.Tinv * f.Tinv) * e4;
+                    const double dlnFcentdT = dFcentdT / Fcent;
+                    const double logFcent = log10(Fcent);
+                    const double cc = -0.4 - 0.67 * logFcent;
+                    const double nn = 0.75 - 1.27 * logFcent;
+                    const double logPrc = log_Pr * loge210 + cc;
+                    const double q = nn - dd * logPrc;
+                    const double t1 = logPrc / q;
+                    const double t2 = 1.0 / (1.0 + t1 * t1);
+                    const double logF = t2 * logFcent;
+                    vlogk1 = vlogk1 + logF / loge210;
+                    dlnkdT1 = dlnkdT1 + t2 * (-2.0 * logF * t1 / (q * q) *
+                                                  (nn * dlnPrdT + (1.27 * logPrc - 0.67 * nn) * dlnFcentdT) +
+                                              dlnFcentdT);
+                    dlnkdlnM = dlnkdlnM - 2.0 * t2 * logF * t1 / (q * q) * nn;
+                }
+            }
+            double numu0rt = 0.0, nudmu0rt = 0.0;
+            for (int k = 0; k < nreac; ++k) {
+                numu0rt = numu0rt - vmu0rt[ind[k]];
+                nudmu0rt = nudmu0rt - vdmu0rt[ind[k]];
+            }
+            for (int k = 0; k < nprod; ++k) {
+                numu0rt = numu0rt + vmu0rt[ind[3 + k]];
+                nudmu0rt = nudmu0rt + vdmu0rt[ind[3 + k]];
+            }
+            vlogk2 = vlogk1 - ch.snu[i] * f.logPRT + numu0rt;
+            dlnkdT2 = dlnkdT1 + ch.snu[i] * f.Tinv + nudmu0rt;
+        }
+    }
+    for (int k = 0; k < ns; ++k) drdn[k] = 0.0;
+    double r = exp(vlogk1);
+    for (int k = 0; k < nreac; ++k) r = r * n[ind[k]];
+    Dr = r;
+    drdn[ns] = dlnkdT1 * r;
+    for (int k = 0; k < nreac; ++k) drdn[ind[k]] = drdn[ind[k]] + r / n[ind[k]];
+    if (rs0 == 0) {
+        r = exp(vlogk2);
+        for (int k = 0; k < nprod; ++k) r = r * n[ind[3 + k]];
+        Dr = Dr - r;
+        drdn[ns] = drdn[ns] - r * dlnkdT2;
+        for (int k = 0; k < nprod; ++k) drdn[ind[3 + k]] = drdn[ind[3 + k]] - r / n[ind[3 + k]];
+    }
+}
+
+// Third-body part of Jex's derivatives of reaction i (FJ.f90:646-655), for
+// reactions with exist_m: vM is the third-body concentration.
+__device__ inline void reaction_jac_m(const DevChem& ch, int i, double Dr, double dlnkdlnM, double vM, double* drdn) {
+    const int ns = ch.ns;
+    const double t = Dr * dlnkdlnM / vM;
+    for (int k = 0; k < ns; ++k) drdn[k] = drdn[k] + t;
+    const int nm = ch.numm[i];
+    for (int k = 0; k < nm; ++k) drdn[ch.indm[i * ns + k]] = drdn[ch.indm[i * ns + k]] + t * ch.men[i * ns + k];
+}
+
+// Fex (FJ.f90:152-300): net rates dn/dt of the species and dT/dt at constant
+// volume (the right-hand side the reference hands DVODE).
+__device__ inline void dev_fex(const DevChem& ch, const double* n, double* dndt) {
+    const int ns = ch.ns;
+    double sn = 0.0;
+    for (int j = 0; j < ns; ++j) sn += n[j];
+    FexPre f;
+    fex_pre(f, n[ns], sn);
+    double vmu0rt[kMaxSpecies], vert[kMaxSpecies], vcvr[kMaxSpecies];
+    for (int j = 0; j < ns; ++j) {
+        species_thermo(ch, j, f, vmu0rt[j], vert[j], vcvr[j]);
+        dndt[j] = 0.0;
+    }
+    double vlogM = 0.0;
+    for (int i = 0; i < ch.nr; ++i) {
+        if (ch.exist_m[i]) vlogM = third_body_logM(ch, i, n, f);
+        double rf, rr;
+        reaction_rates(ch, i, n, f, vlogM, vmu0rt, rf, rr);
+        const double Dr = ch.rstate[2 * i] == 0 ? rf - rr : rf;
+        const int* ind = ch.indnu + 6 * i;
+        const int nreac = ch.numnu[2 * i], nprod = ch.numnu[2 * i + 1];
+        for (int k = 0; k < nreac; ++k) dndt[ind[k]] = dndt[ind[k]] - Dr;
+        for (int k = 0; k < nprod; ++k) dndt[ind[3 + k]] = dndt[ind[3 + k]] + Dr;
+    }
+    double de = 0.0, cv = 0.0;
+    for (int j = 0; j < ns; ++j) {
+        de = de + vert[j] * dndt[j];
+        cv = cv + vcvr[j] * n[j];
+    }
+    dndt[ns] = -de * f.T / cv;
+}
+
+// Jex (FJ.f90:454-709): the net rates dndt (as Fex) and their exact Jacobian
+// J (row-major (ns+1) x (ns+1), J[i*(ns+1)+j] = d dndt_i / d n_j, T last).
+__device__ inline void dev_jex(const DevChem& ch, const double* n, double* dndt, double* J) {
+    const int ns = ch.ns, N = ns + 1;
+    double sn = 0.0;
+    for (int j = 0; j < ns; ++j) sn += n[j];
+    sn = fmax(sn, 1e-300);
+    FexPre f;
+    fex_pre(f, n[ns], sn);
+    double cdmurt[7], cdcpr[7];
+    jex_pre(f.T, cdmurt, cdcpr);
+    double vmu0rt[kMaxSpecies], vdmu0rt[kMaxSpecies], vert[kMaxSpecies], vcvr[kMaxSpecies], vdcvr[kMaxSpecies];
+    for (int j = 0; j < ns; ++j) {
+        species_thermo_d(ch, j, f, cdmurt, cdcpr, vmu0rt[j], vdmu0rt[j], vert[j], vcvr[j], vdcvr[j]);
+        dndt[j] = 0.0;
+        for (int i = 0; i < N; ++i) J[j * N + i] = 0.0;
+    }
+    double vM = 0.0, vlogM = 0.0, dlnkdlnM = 0.0;
+    double drdn[kMaxSpecies + 1];
+    for (int i = 0; i < ch.nr; ++i) {
+        if (ch.exist_m[i]) {
+            double tmp = sn;
+            const int nm = ch.numm[i];
+            for (int j = 0; j < nm; ++j) tmp = tmp + ch.men[i * ns + j] * n[ch.indm[i * ns + j]];
+            vM = tmp;
+            vlogM = (tmp == sn) ? f.logsn : log(tmp);
+        }
+        double Dr;
+        reaction_jac(ch, i, n, f, vlogM, vmu0rt, vdmu0rt, dlnkdlnM, Dr, drdn);
+        if (ch.exist_m[i]) reaction_jac_m(ch, i, Dr, dlnkdlnM, vM, drdn);
+        const int* ind = ch.indnu + 6 * i;
+        const int nreac = ch.numnu[2 * i], nprod = ch.numnu[2 * i + 1];
+        for (int k = 0; k < nreac; ++k) {
+            const int s = ind[k];
+            dndt[s] = dndt[s] - Dr;
+            for (int j = 0; j < N; ++j) J[s * N + j] = J[s * N + j] - drdn[j];
+        }
+        for (int k = 0; k < nprod; ++k) {
+            const int s = ind[3 + k];
+            dndt[s] = dndt[s] + Dr;
+            for (int j = 0; j < N; ++j) J[s * N + j] = J[s * N + j] + drdn[j];
+        }
+    }
+    double de = 0.0, cv = 0.0, dcv = 0.0, t1 = 0.0, t2 = 0.0;
+    for (int j = 0; j < ns; ++j) {
+        t1 = t1 + vert[j] * J[j * N + ns];
+        de = de + vert[j] * dndt[j];
+        dcv = dcv + vcvr[j] * dndt[j];
+        cv = cv + vcvr[j] * n[j];
+        t2 = t2 + vdcvr[j] * n[j];
+    }
+    dndt[ns] = -de * f.T / cv;
+    J[ns * N + ns] = -(f.T * t1 + dcv + dndt[ns] * t2) / cv;
+    for (int j = 0; j < ns; ++j) {
+        double t = 0.0;
+        for (int k = 0; k < ns; ++k) t = t + vert[k] * J[k * N + j];
+        J[ns * N + j] = -(f.T * t + dndt[ns] * vcvr[j]) / cv;
+    }
+}
+
 // Per-thread CHEMEQ2 state machine (sub_chem.f90:1714-1819).
 struct Ceq {
     double y[kMaxSpecies + 1], y0[kMaxSpecies + 1];
@@ -165,12 +399,6 @@ struct Ceq {
     double h_carry;   // step proposed by the last accepted implicit substep (0: none), kept
                       // across the reaction_chemeq2 calls of one 0-D reactor
 };
-
-// Sum of production and destruction rates: dy/dt of the UV source terms.
-__device__ inline void dev_rates(const DevChem& ch, const double* y, double* f, double* tmp) {
-    dev_fex_var(ch, y, f, tmp);
-    for (int i = 0; i <= ch.ns; ++i) f[i] = f[i] + tmp[i];
-}
 
 // Weight of component i in the error norm: the CHEMEQ2 tolerance
 // y*rtol + rtol*1e-5 for the species (sub_chem.f90:1801), rtol*T for T.
@@ -229,34 +457,29 @@ __device__ inline void lu_solve(const double* M, const int* piv, int N, double* 
 // 2, with gamma = 1 + 1/sqrt(2):
 //     (I - gamma h J) k1 = f(y0),   (I - gamma h J) k2 = f(y0 + h k1) - 2 k1,
 //     y = y0 + 3/2 h k1 + 1/2 h k2,  error estimate |h/2 (k1 + k2)| (vs. y0 + h k1),
-// J a forward-difference Jacobian of the rates at y0, step factor
-// 0.8/sqrt(err) in [0.2, 2].  Used for the rest of an interval once CHEMEQ2
+// f = Fex and J = Jex at y0 (the pair the reference hands DVODE, mf = 21),
+// step factor 0.8/sqrt(err) in [0.2, 2].  Used for the rest of an interval once CHEMEQ2
 // has made 10 attempts (where sub_chem.f90:1755-1775 calls DVODE).
 // Returns 1 when the interval is done, 0 to continue, <0 error.
 __device__ inline int be_attempt(const DevChem& ch, Ceq& s, double rtol, int max_substeps, long long& attempts) {
     const int ns = ch.ns, N = ns + 1;
     const double gam = 1.7071067811865475;  // 1 + 1/sqrt(2)
-    double f0[kMaxSpecies + 1], f[kMaxSpecies + 1], tmp[kMaxSpecies + 1], k1[kMaxSpecies + 1], k2[kMaxSpecies + 1];
+    double f0[kMaxSpecies + 1], f[kMaxSpecies + 1], k1[kMaxSpecies + 1], k2[kMaxSpecies + 1];
     double M[(kMaxSpecies + 1) * (kMaxSpecies + 1)];
     int piv[kMaxSpecies + 1];
     ++attempts;
     double h = s.dt;
     if (s.tout - s.tt < h) h = s.tout - s.tt;
-    dev_rates(ch, s.y0, f0, tmp);
-    // M = I - gamma h J,  J(:, j) = (f(y0 + e_j dj) - f0) / dj
-    for (int j = 0; j < N; ++j) {
-        for (int i = 0; i < N; ++i) s.y[i] = s.y0[i];
-        const double dj = 1.4901161193847656e-8 * fmax(fabs(s.y0[j]), j < ns ? 1e-10 : 1.0);
-        s.y[j] = s.y0[j] + dj;
-        dev_rates(ch, s.y, f, tmp);
-        for (int i = 0; i < N; ++i) M[i * N + j] = (i == j ? 1.0 : 0.0) - gam * h * (f[i] - f0[i]) / dj;
-    }
+    // M = I - gamma h J with Jex's exact Jacobian at y0; f0 = Fex(y0) (Jex's dndt)
+    dev_jex(ch, s.y0, f0, M);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) M[i * N + j] = (i == j ? 1.0 : 0.0) - gam * h * M[i * N + j];
     double err = 1e300;
     if (lu_factor(M, piv, N)) {
         for (int i = 0; i < N; ++i) k1[i] = f0[i];
         lu_solve(M, piv, N, k1);
         for (int i = 0; i < N; ++i) s.y[i] = s.y0[i] + h * k1[i];
-        dev_rates(ch, s.y, f, tmp);
+        dev_fex(ch, s.y, f);
         for (int i = 0; i < N; ++i) k2[i] = f[i] - 2.0 * k1[i];
         lu_solve(M, piv, N, k2);
         err = 0.0;
@@ -266,7 +489,7 @@ __device__ inline int be_attempt(const DevChem& ch, Ceq& s, double rtol, int max
             err = (e > err || e != e) ? e : err;
         }
     }
-    s.evals += N + 2;
+    s.evals += 2;
     if (!(err <= 1.0)) {
         s.dt = h * (err == err && err < 1e300 ? fmax(0.2, 0.8 / sqrt(err)) : 0.25);
         if (++s.rejects > 30) return -SCFD_E_CHEM;

@@ -10,10 +10,11 @@
 //
 // One warp integrates one reactor: every source-term evaluation spreads the
 // species thermo and the reaction rates over the lanes (the rates are summed
-// per species in Fex_var's order), the Rosenbrock Jacobian and LU work on rows
-// across lanes, and the serial-order sums and the triangular solves run on
-// lane 0, so each step does the arithmetic of the one-thread code
-// (chem_dev.cuh) in the same order.
+// per species in Fex_var's order), the Rosenbrock substep's Jex spreads the
+// reactions' derivative rows over the lanes and sums them per species in
+// Jex's order, its LU works on rows across lanes, and the serial-order sums
+// and the triangular solves run on lane 0, so each step does the arithmetic of
+// the one-thread code (chem_dev.cuh) in the same order.
 //
 // Work distribution (SCFD_REACTOR_QUEUE): reactors need very different numbers
 // of substeps, so one persistent launch has every warp pull reactors from a
@@ -38,12 +39,21 @@ namespace scfd {
 // (kind 0) or reverse (kind 1) rate of reaction i; p lists the production
 // terms, m the destruction terms; mref[i] is the reaction whose third-body
 // term reaction i uses (-1: none yet).
+//
+// For Fex / Jex (FJ.f90:152-709), the net list of species j, n_ptr[j] ..
+// n_ptr[j+1], holds 2*i + 1 for every reactant slot of j in reaction i and
+// 2*i for every product slot, reactions in order and reactants first, as the
+// reference subtracts and adds Dr; dref[i] is the last reaction up to i that
+// sets dlnkdlnM (third-body or fall-off rate; -1: none yet).
 struct RateLists {
     const int* p_ptr;  // [ns+1]
     const int* p_ent;
     const int* m_ptr;  // [ns+1]
     const int* m_ent;
     const int* mref;   // [nr]
+    const int* n_ptr;  // [ns+1]
+    const int* n_ent;
+    const int* dref;   // [nr]
 };
 
 struct ReactorArgs {
@@ -66,18 +76,20 @@ struct ReactorArgs {
 struct WarpMem {
     double *y0, *y, *yp, *q0, *p0, *q, *p, *f0, *k1, *k2, *M;
     double *mu, *e, *cv, *lm, *rf, *rr;
+    double *dmu, *dcv, *vm, *dl, *dr, *drdn;  // Jex: per-species T-derivatives, per-reaction terms
     int* piv;
     __device__ WarpMem(double* b, int N, int ns, int nr) {
         y0 = b; y = y0 + N; yp = y + N; q0 = yp + N; p0 = q0 + N; q = p0 + N; p = q + N;
         f0 = p + N; k1 = f0 + N; k2 = k1 + N; M = k2 + N;
         mu = M + N * N; e = mu + ns; cv = e + ns; lm = cv + ns; rf = lm + nr; rr = rf + nr;
-        piv = reinterpret_cast<int*>(rr + nr);
+        dmu = rr + nr; dcv = dmu + ns; vm = dcv + ns; dl = vm + nr; dr = dl + nr; drdn = dr + nr;
+        piv = reinterpret_cast<int*>(drdn + nr * N);
     }
 };
 
 __host__ __device__ inline int warp_mem_doubles(int ns, int nr) {
     const int N = ns + 1;
-    return 10 * N + N * N + 3 * ns + 3 * nr + (N + 1) / 2 + 1;
+    return 10 * N + N * N + 5 * ns + 6 * nr + nr * N + (N + 1) / 2 + 1;
 }
 
 // Fex_var of the state n (shared memory) by one warp: species thermo and
@@ -127,6 +139,92 @@ __device__ void warp_fex(const DevChem& ch, const RateLists& rl, const double* n
     __syncwarp();
 }
 
+// Fex (J == nullptr) or Jex (FJ.f90:152-709) of the state n (shared memory)
+// by one warp: species thermo and reactions across lanes, the per-species
+// sums in the reference's serial order (net lists), the T row on lane j.
+// dndt[0..ns] and, for Jex, J (row-major N x N) are written to shared memory.
+__device__ void warp_jex(const DevChem& ch, const RateLists& rl, const double* n, double* dndt, double* J,
+                         WarpMem& w, int lane) {
+    const int ns = ch.ns, nr = ch.nr, N = ns + 1;
+    const bool jac = J != nullptr;
+    double sn = 0.0;
+    if (lane == 0)
+        for (int j = 0; j < ns; ++j) sn += n[j];
+    sn = __shfl_sync(0xffffffffu, sn, 0);
+    if (jac) sn = fmax(sn, 1e-300);
+    FexPre f;
+    fex_pre(f, n[ns], sn);
+    double cdmurt[7], cdcpr[7];
+    jex_pre(f.T, cdmurt, cdcpr);
+    for (int j = lane; j < ns; j += 32) species_thermo_d(ch, j, f, cdmurt, cdcpr, w.mu[j], w.dmu[j], w.e[j], w.cv[j], w.dcv[j]);
+    for (int i = lane; i < nr; i += 32)
+        if (ch.exist_m[i]) {
+            double tmp = f.sn;
+            const int nm = ch.numm[i];
+            for (int j = 0; j < nm; ++j) tmp = tmp + ch.men[i * ns + j] * n[ch.indm[i * ns + j]];
+            w.vm[i] = tmp;
+            w.lm[i] = (tmp == f.sn) ? f.logsn : log(tmp);
+        }
+    __syncwarp();
+    for (int i = lane; i < nr; i += 32) {
+        const int r = rl.mref[i];
+        double dl = 0.0;  // read only where this reaction sets it (dref)
+        reaction_jac(ch, i, n, f, r >= 0 ? w.lm[r] : 0.0, w.mu, w.dmu, dl, w.dr[i], w.drdn + i * N);
+        w.dl[i] = dl;
+    }
+    __syncwarp();
+    if (jac)
+        for (int i = lane; i < nr; i += 32)
+            if (ch.exist_m[i]) {
+                const int d = rl.dref[i];
+                reaction_jac_m(ch, i, w.dr[i], d >= 0 ? w.dl[d] : 0.0, w.vm[i], w.drdn + i * N);
+            }
+    __syncwarp();
+    for (int j = lane; j < ns; j += 32) {
+        double a = 0.0;
+        for (int k = rl.n_ptr[j]; k < rl.n_ptr[j + 1]; ++k) {
+            const int en = rl.n_ent[k];
+            a = (en & 1) ? a - w.dr[en >> 1] : a + w.dr[en >> 1];
+        }
+        dndt[j] = a;
+    }
+    if (jac)
+        for (int t = lane; t < ns * N; t += 32) {
+            const int j = t / N, c = t - j * N;
+            double a = 0.0;
+            for (int k = rl.n_ptr[j]; k < rl.n_ptr[j + 1]; ++k) {
+                const int en = rl.n_ent[k];
+                const double v = w.drdn[(en >> 1) * N + c];
+                a = (en & 1) ? a - v : a + v;
+            }
+            J[j * N + c] = a;
+        }
+    __syncwarp();
+    if (lane == 0) {
+        double de = 0.0, cv = 0.0, dcv = 0.0, t1 = 0.0, t2 = 0.0;
+        for (int j = 0; j < ns; ++j) {
+            if (jac) t1 = t1 + w.e[j] * J[j * N + ns];
+            de = de + w.e[j] * dndt[j];
+            dcv = dcv + w.cv[j] * dndt[j];
+            cv = cv + w.cv[j] * n[j];
+            t2 = t2 + w.dcv[j] * n[j];
+        }
+        dndt[ns] = -de * f.T / cv;
+        if (jac) J[ns * N + ns] = -(f.T * t1 + dcv + dndt[ns] * t2) / cv;
+    }
+    __syncwarp();
+    if (jac) {
+        double cv = 0.0;  // the same sum on every lane
+        for (int j = 0; j < ns; ++j) cv = cv + w.cv[j] * n[j];
+        for (int j = lane; j < ns; j += 32) {
+            double t = 0.0;
+            for (int k = 0; k < ns; ++k) t = t + w.e[k] * J[k * N + j];
+            J[ns * N + j] = -(f.T * t + dndt[ns] * w.cv[j]) / cv;
+        }
+    }
+    __syncwarp();
+}
+
 // NaN-propagating min / max over the warp (order-free: exact comparisons)
 __device__ inline double warp_min_nan(double v) {
     for (int o = 16; o > 0; o >>= 1) {
@@ -151,23 +249,19 @@ struct CallState {
     long long evals;
 };
 
-// Rosenbrock substep (be_attempt of chem_dev.cuh) by one warp.
+// Rosenbrock substep (be_attempt of chem_dev.cuh) by one warp: Jex for the
+// matrix, Fex for the second stage.
 __device__ int warp_ros_attempt(const DevChem& ch, const RateLists& rl, WarpMem& w, CallState& s, double rtol,
                                 int max_substeps, int lane) {
     const int ns = ch.ns, N = ns + 1;
     const double gam = 1.7071067811865475;
     double h = s.dt;
     if (s.tout - s.tt < h) h = s.tout - s.tt;
-    warp_fex(ch, rl, w.y0, w.q0, w.p0, w, lane);
-    for (int i = lane; i < N; i += 32) w.f0[i] = w.q0[i] + w.p0[i];
-    for (int j = 0; j < N; ++j) {
-        const double dj = 1.4901161193847656e-8 * fmax(fabs(w.y0[j]), j < ns ? 1e-10 : 1.0);
-        __syncwarp();
-        for (int i = lane; i < N; i += 32) w.y[i] = (i == j) ? w.y0[i] + dj : w.y0[i];
-        __syncwarp();
-        warp_fex(ch, rl, w.y, w.q, w.p, w, lane);
-        for (int i = lane; i < N; i += 32)
-            w.M[i * N + j] = (i == j ? 1.0 : 0.0) - gam * h * ((w.q[i] + w.p[i]) - w.f0[i]) / dj;
+    // M = I - gamma h J with Jex's exact Jacobian at y0; f0 = Fex(y0) (Jex's dndt)
+    warp_jex(ch, rl, w.y0, w.f0, w.M, w, lane);
+    for (int t = lane; t < N * N; t += 32) {
+        const int i = t / N, j = t - i * N;
+        w.M[t] = (i == j ? 1.0 : 0.0) - gam * h * w.M[t];
     }
     __syncwarp();
     // LU with partial pivoting: first largest pivot, rows eliminated across lanes
@@ -213,9 +307,9 @@ __device__ int warp_ros_attempt(const DevChem& ch, const RateLists& rl, WarpMem&
         __syncwarp();
         for (int i = lane; i < N; i += 32) w.y[i] = w.y0[i] + h * w.k1[i];
         __syncwarp();
-        warp_fex(ch, rl, w.y, w.q, w.p, w, lane);
+        warp_jex(ch, rl, w.y, w.q, nullptr, w, lane);
         if (lane == 0) {
-            for (int i = 0; i < N; ++i) w.k2[i] = (w.q[i] + w.p[i]) - 2.0 * w.k1[i];
+            for (int i = 0; i < N; ++i) w.k2[i] = w.q[i] - 2.0 * w.k1[i];
             lu_solve(w.M, w.piv, N, w.k2);
         }
         __syncwarp();
@@ -227,7 +321,7 @@ __device__ int warp_ros_attempt(const DevChem& ch, const RateLists& rl, WarpMem&
         }
         err = warp_max_nan(e);
     }
-    s.evals += N + 2;
+    s.evals += 2;
     __syncwarp();
     if (!(err <= 1.0)) {
         s.dt = h * (err == err && err < 1e300 ? fmax(0.2, 0.8 / sqrt(err)) : 0.25);
@@ -384,6 +478,20 @@ __device__ void warp_reactor(const DevChem& ch, const ReactorArgs& a, WarpMem& w
     __syncwarp();
 }
 
+// Fex / Jex of independent states, one thread each (scfd_chem_rates).
+__global__ void k_chem_rates(DevChem ch, int n, const double* states, double* dndt, double* jac) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int N = ch.ns + 1;
+    double y[kMaxSpecies + 1], f[kMaxSpecies + 1];
+    for (int i = 0; i < N; ++i) y[i] = states[(size_t)c * N + i];
+    if (jac)
+        dev_jex(ch, y, f, jac + (size_t)c * N * N);
+    else
+        dev_fex(ch, y, f);
+    for (int i = 0; i < N; ++i) dndt[(size_t)c * N + i] = f[i];
+}
+
 // One warp per reactor; in queue mode each warp takes reactors from the
 // device counter until none is left.
 __global__ void __launch_bounds__(128) k_reactors(DevChem ch, ReactorArgs a) {
@@ -537,13 +645,19 @@ int scfd_reactors_create(const scfd_chem* chem, int n_max, scfd_reactors** out) 
     const size_t nn = (size_t)n_max, nv = nn * r->ns;
     // per-species rate lists in the accumulation order of Fex_var (FJ.f90:301-453)
     const int ns = chem->ns, nr = chem->nr;
-    std::vector<int> pp(ns + 1, 0), mp(ns + 1, 0), pe, me, mref(nr > 0 ? nr : 1, -1);
+    std::vector<int> pp(ns + 1, 0), mp(ns + 1, 0), np_(ns + 1, 0), pe, me, ne_, mref(nr > 0 ? nr : 1, -1),
+        dref(nr > 0 ? nr : 1, -1);
     {
-        std::vector<std::vector<int>> pl(ns), ml(ns);
-        int last = -1;
+        std::vector<std::vector<int>> pl(ns), ml(ns), nl(ns);
+        int last = -1, lastd = -1;
         for (int i = 0; i < nr; ++i) {
             if (chem->exist_m[i]) last = i;
             mref[i] = last;
+            const int rs0 = chem->rstate[i][0], rs1 = chem->rstate[i][1];
+            if (rs1 >= 4 || (rs0 == 0 && (rs1 == 2 || rs1 == 3))) lastd = i;
+            dref[i] = lastd;
+            for (int k = 0; k < chem->numnu[i][0]; ++k) nl[chem->indnu[i][0][k]].push_back(2 * i + 1);
+            for (int k = 0; k < chem->numnu[i][1]; ++k) nl[chem->indnu[i][1][k]].push_back(2 * i);
             const int nreac = chem->numnu[i][0], nprod = chem->numnu[i][1];
             for (int k = 0; k < nreac; ++k) ml[chem->indnu[i][0][k]].push_back(2 * i);
             for (int k = 0; k < nprod; ++k) pl[chem->indnu[i][1][k]].push_back(2 * i);
@@ -555,11 +669,14 @@ int scfd_reactors_create(const scfd_chem* chem, int n_max, scfd_reactors** out) 
         for (int j = 0; j < ns; ++j) {
             pe.insert(pe.end(), pl[j].begin(), pl[j].end());
             me.insert(me.end(), ml[j].begin(), ml[j].end());
+            ne_.insert(ne_.end(), nl[j].begin(), nl[j].end());
             pp[j + 1] = (int)pe.size();
             mp[j + 1] = (int)me.size();
+            np_[j + 1] = (int)ne_.size();
         }
         if (pe.empty()) pe.push_back(0);
         if (me.empty()) me.push_back(0);
+        if (ne_.empty()) ne_.push_back(0);
     }
     r->wstride = (warp_mem_doubles(ns, nr) + 1) & ~1;
     const int blk_smem = 4 * r->wstride * (int)sizeof(double);
@@ -569,7 +686,8 @@ int scfd_reactors_create(const scfd_chem* chem, int n_max, scfd_reactors** out) 
     }
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
     const size_t bytes = tabs.bytes() + 3 * al(nn * 8) + 2 * al(nv * 8) + al(nn * 8) + al(nn * 4) + 2 * 256 +
-                         2 * al(pp.size() * 4) + al(pe.size() * 4) + al(me.size() * 4) + al(mref.size() * 4);
+                         2 * al(pp.size() * 4) + al(pe.size() * 4) + al(me.size() * 4) + al(mref.size() * 4) +
+                         al(np_.size() * 4) + al(ne_.size() * 4) + al(dref.size() * 4);
     e = cudaMalloc(&r->arena, bytes);
     if (e != cudaSuccess) return fail(e);
     char* p = r->arena;
@@ -589,13 +707,17 @@ int scfd_reactors_create(const scfd_chem* chem, int n_max, scfd_reactors** out) 
     int* dmp = carve_r<int>(p, mp.size());
     int* dme = carve_r<int>(p, me.size());
     int* dmr = carve_r<int>(p, mref.size());
+    int* dnp = carve_r<int>(p, np_.size());
+    int* dne = carve_r<int>(p, ne_.size());
+    int* ddr = carve_r<int>(p, dref.size());
     for (auto cp : {std::make_pair(dpp, &pp), std::make_pair(dpe, &pe), std::make_pair(dmp, &mp),
-                    std::make_pair(dme, &me), std::make_pair(dmr, &mref)}) {
+                    std::make_pair(dme, &me), std::make_pair(dmr, &mref), std::make_pair(dnp, &np_),
+                    std::make_pair(dne, &ne_), std::make_pair(ddr, &dref)}) {
         e = cudaMemcpyAsync(cp.first, cp.second->data(), cp.second->size() * sizeof(int), cudaMemcpyHostToDevice,
                             r->stream);
         if (e != cudaSuccess) return fail(e);
     }
-    r->rl = RateLists{dpp, dpe, dmp, dme, dmr};
+    r->rl = RateLists{dpp, dpe, dmp, dme, dmr, dnp, dne, ddr};
     if (p > r->arena + bytes) {
         r->err = "arena overflow";
         scfd_reactors_destroy(r);
@@ -665,4 +787,37 @@ int scfd_reactors_launch_count(const scfd_reactors* r, int64_t* launches) {
     return 0;
 }
 
+int scfd_chem_rates(const scfd_chem* chem, int n, const double* states, double* dndt, double* jac) {
+    if (!chem || n < 0 || (n > 0 && (!states || !dndt)) || chem->ns < 1 || chem->ns > SCFD_MAX_SPECIES ||
+        chem->nr < 0 || chem->nr > SCFD_MAX_REACTIONS)
+        return SCFD_E_ARG;
+    if (n == 0) return 0;
+    const ChemTables tabs(*chem);
+    const size_t N = (size_t)chem->ns + 1;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t bs = al(n * N * 8), bj = jac ? al(n * N * N * 8) : 0;
+    char* arena = nullptr;
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&arena, tabs.bytes() + 2 * bs + bj);
+    DevChem ch{};
+    char* p = arena;
+    if (e == cudaSuccess) e = tabs.upload(ch, p, st);
+    double* ds = reinterpret_cast<double*>(p);
+    double* dd = reinterpret_cast<double*>(p + bs);
+    double* dj = jac ? reinterpret_cast<double*>(p + 2 * bs) : nullptr;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ds, states, n * N * 8, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        k_chem_rates<<<(n + 127) / 128, 128, 0, st>>>(ch, n, ds, dd, dj);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dndt, dd, n * N * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && jac) e = cudaMemcpyAsync(jac, dj, n * N * N * 8, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (arena) cudaFree(arena);
+    if (st) cudaStreamDestroy(st);
+    return e == cudaSuccess ? 0 : SCFD_E_CUDA;
+}
+
 }  // extern "C"
+
