@@ -431,7 +431,9 @@ typedef struct scfd_cea_data {
     double  trans[SCFD_CEA_MAX_SPECIES][SCFD_CEA_MAX_TSECTIONS][4];/* ln mu = A ln T + B/T + C/T^2 + D */
     double  pf, Tf, po, To;                                        /* fuel / oxidizer stream, Pa and K */
     double  nf[SCFD_CEA_MAX_SPECIES], no[SCFD_CEA_MAX_SPECIES];    /* stream mole ratios */
-    int32_t reserved[8];
+    int32_t init_hp;       /* stream states by cea_hp at the stream's p, h (initialize_cea('hp'));
+                              0: by cea at its rho, e (initialize_cea('uv')) */
+    int32_t reserved[7];
 } scfd_cea_data;
 
 /* The fuel and oxidizer states initialize_cea('uv') derives
@@ -468,6 +470,19 @@ int  scfd_cea_info_get(const scfd_cea* cea, scfd_cea_info* info);
 int  scfd_cea_solve(scfd_cea* cea, int64_t ncell, const double* rho, const double* Y, const double* e,
                     double* T, double* n, double* mwave, double* kappa, double* mu, double* Yv,
                     double* vhi, double* DHi, int32_t* iters, void* stream);
+/* cea_hp (sub_chem.f90:1652-1962): equilibrium at fixed pressure p[ncell] (Pa)
+ * and enthalpy h[ncell] (J/kg); T is the guess / result.  Outputs as
+ * scfd_cea_solve (no DHi; vhi = Ru 1e3 T / MW h/RT as the routine forms it).
+ * The reference's retry after a singular matrix has no bound; here it counts
+ * towards the 500-iteration limit. */
+int  scfd_cea_solve_hp(scfd_cea* cea, int64_t ncell, const double* p, const double* Y, const double* h, double* T,
+                       double* n, double* mwave, double* kappa, double* mu, double* Yv, double* vhi,
+                       int32_t* iters, void* stream);
+/* cea_tp (sub_chem.f90:1963-2248): equilibrium at fixed p and T; h[ncell]
+ * (J/kg, may be NULL) receives the mixture enthalpy.  Retry bounded as hp. */
+int  scfd_cea_solve_tp(scfd_cea* cea, int64_t ncell, const double* p, const double* Y, const double* T, double* n,
+                       double* h, double* mwave, double* kappa, double* mu, double* Yv, double* vhi,
+                       int32_t* iters, void* stream);
 /* Synchronises the last solve's stream and returns, in counts[0..1], the
  * cells of the solves since the previous call that stopped at the
  * 500-iteration limit (the reference prints "not converted. at cea" and goes

@@ -3,6 +3,7 @@
 //
 // Follows store/therm_lib/NASA/core:
 //   cea              sub_chem.f90:1320-1651 (Newton on element potentials)
+//   cea_hp, cea_tp   sub_chem.f90:1652-2248 (fixed p and h; fixed p and T)
 //   initialize_cea   sub_chem.f90:1136-1287 (stream states, element lists, masks)
 //   set_therm_data   sub_chem.f90:159-170   (YAc, element mass fractions)
 //   LU               LU.f90:1-83            (pivoted LU, singular below 1e-30)
@@ -178,7 +179,7 @@ bool LU(double A[NEX][NEX], double* b, double* x, int n) {
 }
 
 struct CeaOut {
-    double MWave, kappa, mu, DHi[3];
+    double MWave, kappa, mu, DHi[3], H;
     double Yv[NSX], vhi[NSX];
     int counter;
     int status;  // 0, 1 = stopped at the iteration limit, 2 = singular twice
@@ -426,6 +427,422 @@ void cea(const Model& M, double rho, const double* Y /*[1..2]*/, double E, doubl
     o.mu = mu * 1e-7;
 }
 
+// The mixture properties that close cea_hp and cea_tp (sub_chem.f90:1902-1961,
+// 2192-2247): MWave from sn, kappa, vhi = Ru 1e3 T / MW h/RT (and H for tp),
+// Yv, Wilke mu.
+void hp_tp_tail(const Model& M, double T, double logT, double sn, double tinyn, const int* sec_num, const double* n,
+                bool with_H, CeaOut& o) {
+    const int ns = M.ns, nt = M.nt;
+    double vTcpr[10], vThrt[10], vTmu[5];
+    o.MWave = 1e3 / sn;
+    calc_vTcpr(T, vTcpr);
+    double kappa = 0.0;
+    for (int i = 1; i <= ns; ++i)
+        if (n[i] > tinyn) kappa = kappa + n[i] * dot9(M.co[i][sec_num[i]], vTcpr);
+    o.kappa = kappa / (kappa - sn);
+    calc_vThrt(T, logT, vThrt);
+    double H = 0.0;
+    const double tmp = Ru * 1e3 * T;
+    for (int i = 1; i <= ns; ++i) {
+        double dh = 0.0;
+        for (int j = 1; j <= 9; ++j) dh = dh + M.co[i][sec_num[i]][j] * vThrt[j];
+        o.vhi[i] = tmp / M.MW[i] * dh;
+        H = H + n[i] * dh;
+    }
+    o.H = with_H ? H * Ru * T : 0.0;
+    for (int i = 1; i <= ns; ++i) o.Yv[i] = n[i] * M.MW[i] * 1e-3;
+    calc_vTmu(T, logT, vTmu);
+    double muN[NSX];
+    for (int i = 1; i <= nt; ++i) {
+        const int sect = check_section_number_trans(M, i, T);
+        const double* a = M.d.trans[i - 1][sect - 1];
+        double s = 0.0;
+        for (int k = 1; k <= 4; ++k) s = s + a[k - 1] * vTmu[k];
+        muN[i] = std::exp(s);
+    }
+    double mu = 0.0;
+    for (int i = 1; i <= nt; ++i) {
+        double denom = 0.0;
+        const double MWi = M.MW[M.d.tr2th[i - 1] + 1];
+        for (int j = 1; j <= nt; ++j) {
+            const double MWj = M.MW[M.d.tr2th[j - 1] + 1];
+            const double f = 1.0 + std::sqrt(muN[i] / muN[j]) * std::pow(MWj / MWi, 0.25);
+            const double phi = 0.25 * (f * f) * std::sqrt(2.0 * MWj / (MWi + MWj));
+            denom = denom + n[M.d.tr2th[j - 1] + 1] * phi;
+        }
+        mu = mu + n[M.d.tr2th[i - 1] + 1] * muN[i] / denom;
+    }
+    o.mu = mu * 1e-7;
+    o.DHi[1] = o.DHi[2] = 0.0;
+}
+
+// cea_hp (sub_chem.f90:1652-1962): equilibrium at fixed p and h; the unknowns
+// are pi_1..pi_ne, ln sn and ln T.  The reference's singular-matrix retry has
+// no bound (it cycles past the iteration test); here it counts towards the
+// same 500-iteration limit.
+void cea_hp(const Model& M, double p, const double* Y, double H, double& T, double* n, CeaOut& o) {
+    const int ns = M.ns, ne = M.ne;
+    double b0[NEX] = {0}, b[NEX] = {0}, bd[NEX] = {0}, vpi[NEX] = {0};
+    double vmurt[NSX], vhrt[NSX], Dlogn[NSX], logn[NSX];
+    int sec_num[NSX];
+    double Ad[NEX][NEX];
+    int elist[NEX], nelist[NEX], nen = 0;
+    bool REDUCEflag;
+    double vTmurt[10], vTcpr[10], vThrt[10];
+    o.status = 0;
+
+    const double logP = std::log(p / pst);
+    for (int i = 1; i <= ne + 2; ++i) b0[i] = Y[1] * M.b0f[i] + Y[2] * M.b0o[i];
+    double b0max = b0[1];
+    for (int i = 2; i <= ne; ++i)
+        if (b0[i] > b0max) b0max = b0[i];
+    double sn = 0.0;
+    for (int j = 1; j <= ns; ++j) sn = sn + n[j];
+    b0[ne + 1] = sn;
+
+    if (Y[1] < Y_eps) {
+        REDUCEflag = true;
+        nen = M.neo + 1;
+        std::memcpy(elist, M.elisto, sizeof(elist));
+        std::memcpy(nelist, M.nelisto, sizeof(nelist));
+        for (int j = 1; j <= ns; ++j) n[j] = n[j] * M.masko[j];
+    } else if (Y[2] < Y_eps) {
+        REDUCEflag = true;
+        nen = M.nef + 1;
+        std::memcpy(elist, M.elistf, sizeof(elist));
+        std::memcpy(nelist, M.nelistf, sizeof(nelist));
+        for (int j = 1; j <= ns; ++j) n[j] = n[j] * M.maskf[j];
+    } else {
+        REDUCEflag = false;
+    }
+
+    const double tinyn = TSIZE * sn;
+    const double logtinyn = std::log(tinyn);
+    const double tinytinyn = TTSIZE * sn;
+    const double logtinytinyn = std::log(tinytinyn);
+
+    double logT = std::log(T);
+    calc_vThrt(T, logT, vThrt);
+    for (int i = 1; i <= ne + 2; ++i) b[i] = 0.0;
+    b[ne + 1] = sn;
+    for (int j = 1; j <= ns; ++j) {
+        vhrt[j] = 0.0;
+        logn[j] = logtinyn;
+    }
+    for (int j = 1; j <= ns; ++j) {
+        sec_num[j] = check_section_number(M, j, T);
+        if (n[j] > tinyn) {
+            vhrt[j] = dot9(M.co[j][sec_num[j]], vThrt);
+            logn[j] = std::log(n[j]);
+            for (int i = 1; i <= ne; ++i) b[i] = b[i] + M.Ac[i][j] * n[j];
+            b[ne + 2] = b[ne + 2] + vhrt[j] * n[j];
+        }
+    }
+    bool flag = true;
+    for (int i = 1; i <= ne; ++i)
+        if (b0[i] > eps && std::fabs(b0[i] - b[i]) > b0max * eps) flag = false;
+    if (std::fabs(H - b[ne + 2] * Ru * T) > eps * std::fabs(H)) flag = false;
+
+    int counter = 0;
+    if (!flag) {
+        counter = 1;
+        for (;;) {
+            b0[ne + 2] = H / (Ru * T);
+            for (int i = 1; i <= ne; ++i) b[i] = 0.0;
+            for (int i = 1; i <= ne + 2; ++i) bd[i] = b0[i];
+            bd[ne + 1] = b0[ne + 1] - b[ne + 1];
+            bd[ne + 2] = b0[ne + 2] - b[ne + 2];
+            for (int i = 1; i <= ne + 2; ++i)
+                for (int j = 1; j <= ne + 2; ++j) Ad[i][j] = 0.0;
+            calc_vTmurt(T, logT, vTmurt);
+            calc_vTcpr(T, vTcpr);
+            for (int k = 1; k <= ns; ++k) {
+                vmurt[k] = dot9(M.co[k][sec_num[k]], vTmurt) + logn[k] - std::log(b0[ne + 1]) + logP;
+                if (n[k] > tinyn) {
+                    const double vmurtn = vmurt[k] * n[k];
+                    for (int i = 1; i <= ne; ++i) {
+                        for (int j = i; j <= ne; ++j) Ad[i][j] = Ad[i][j] + M.Ac[i][k] * M.Ac[j][k] * n[k];
+                        Ad[i][ne + 1] = Ad[i][ne + 1] + M.Ac[i][k] * n[k];
+                        Ad[i][ne + 2] = Ad[i][ne + 2] + M.Ac[i][k] * vhrt[k] * n[k];
+                        b[i] = b[i] + M.Ac[i][k] * n[k];
+                        bd[i] = bd[i] + M.Ac[i][k] * (vmurtn - n[k]);
+                    }
+                    Ad[ne + 1][ne + 2] = Ad[ne + 1][ne + 2] + n[k] * vhrt[k];
+                    Ad[ne + 2][ne + 2] =
+                        Ad[ne + 2][ne + 2] + n[k] * (vhrt[k] * vhrt[k] + dot9(M.co[k][sec_num[k]], vTcpr));
+                    bd[ne + 1] = bd[ne + 1] + vmurtn;
+                    bd[ne + 2] = bd[ne + 2] + vmurtn * vhrt[k];
+                }
+            }
+            Ad[ne + 1][ne + 1] = b[ne + 1] - b0[ne + 1];
+            for (int i = 1; i <= ne + 2; ++i)
+                for (int j = i + 1; j <= ne + 2; ++j) Ad[j][i] = Ad[i][j];
+
+            bool LUflag;
+            if (REDUCEflag) {
+                for (int i = 1; i <= nen; ++i) {
+                    for (int j = 1; j <= nen; ++j) Ad[i][j] = Ad[elist[i]][elist[j]];
+                    bd[i] = bd[elist[i]];
+                }
+                LUflag = LU(Ad, bd, vpi, nen);
+                if (!LUflag) {
+                    for (int i = nen; i >= 1; --i) vpi[elist[i]] = vpi[i];
+                    for (int i = 1; i <= ne + 2 - nen; ++i) vpi[nelist[i]] = -1e300;
+                }
+            } else {
+                LUflag = LU(Ad, bd, vpi, ne + 2);
+            }
+            if (LUflag) {
+                for (int j = 1; j <= ns; ++j) n[j] = n[j] + initial_eps;
+                sn = 0.0;
+                b[ne + 2] = 0.0;
+                for (int j = 1; j <= ns; ++j) logn[j] = logtinytinyn;
+                for (int j = 1; j <= ns; ++j) {
+                    if (n[j] < tinytinyn)
+                        n[j] = tinytinyn;
+                    else
+                        logn[j] = std::log(n[j]);
+                    if (n[j] > tinyn) {
+                        vhrt[j] = dot9(M.co[j][sec_num[j]], vThrt);
+                        b[ne + 2] = b[ne + 2] + vhrt[j] * n[j];
+                        sn = sn + n[j];
+                    }
+                }
+                b[ne + 1] = sn;
+                counter = counter + 1;
+                if (counter > 500) break;
+                continue;
+            }
+
+            const double Dlogsn = vpi[ne + 1];
+            const double DlogT = vpi[ne + 2];
+            for (int j = 1; j <= ns; ++j) {
+                double tmp = 0.0;
+                for (int i = 1; i <= ne; ++i) tmp = tmp + M.Ac[i][j] * vpi[i];
+                Dlogn[j] = -vmurt[j] + tmp + Dlogsn + vhrt[j] * DlogT;
+            }
+            double lambda1 = 0.0, lambda2 = 1e300;
+            const double logsn = std::log(b0[ne + 1]);
+            for (int j = 1; j <= ns; ++j) {
+                if (logn[j] - logsn > -18.420681)
+                    lambda1 = std::fmax(lambda1, std::fabs(Dlogn[j]));
+                else if (Dlogn[j] > 0.0)
+                    lambda2 = std::fmin(lambda2, std::fabs((-logn[j] + logsn - 9.2103404) / (Dlogn[j] - Dlogsn)));
+            }
+            lambda1 = 2.0 / std::fmax(std::fmax(std::fmax(5.0 * std::fabs(DlogT), 5.0 * std::fabs(Dlogsn)),
+                                                std::fabs(lambda1)),
+                                      2.0);
+            const double omega_var = std::fmin(1.0, std::fmin(lambda1, lambda2));
+
+            b0[ne + 1] = b0[ne + 1] * std::exp(omega_var * Dlogsn);
+            T = T * std::exp(omega_var * DlogT);
+            logT = std::log(T);
+            for (int j = 1; j <= ns; ++j) sec_num[j] = check_section_number(M, j, T);
+
+            sn = 0.0;
+            b[ne + 2] = 0.0;
+            double Dnmax = 0.0;
+            for (int j = 1; j <= ns; ++j) logn[j] = logtinytinyn;
+            calc_vThrt(T, logT, vThrt);
+            for (int j = 1; j <= ns; ++j) {
+                n[j] = n[j] * std::exp(omega_var * Dlogn[j]);
+                if (n[j] < tinytinyn)
+                    n[j] = tinytinyn;
+                else
+                    logn[j] = std::log(n[j]);
+                if (n[j] > tinyn) {
+                    vhrt[j] = dot9(M.co[j][sec_num[j]], vThrt);
+                    b[ne + 2] = b[ne + 2] + vhrt[j] * n[j];
+                    sn = sn + n[j];
+                    const double tmp = std::fabs(Dlogn[j]) * n[j];
+                    if (Dnmax < tmp) Dnmax = tmp;
+                }
+            }
+            b[ne + 1] = sn;
+
+            flag = true;
+            if (std::fabs(Dnmax) > eps * sn) flag = false;
+            for (int i = 1; i <= ne; ++i)
+                if (b0[i] > eps && std::fabs(b0[i] - b[i]) > b0max * eps) flag = false;
+            if (std::fabs(Dlogsn) > eps || std::fabs(b0[ne + 1] - b[ne + 1]) > eps * std::fabs(sn)) flag = false;
+            if (std::fabs(DlogT) > eps || std::fabs(H - b[ne + 2] * Ru * T) > eps * std::fabs(H)) flag = false;
+            if (counter > 500) flag = true;
+            if (flag) break;
+            counter = counter + 1;
+        }
+        if (counter > 500) o.status = 1;
+    }
+    o.counter = counter;
+    hp_tp_tail(M, T, logT, sn, tinyn, sec_num, n, false, o);
+}
+
+// cea_tp (sub_chem.f90:1963-2248): equilibrium at fixed T and p; the
+// unknowns are pi_1..pi_ne and ln sn.  H is returned.  The singular-matrix
+// retry is bounded as in cea_hp.
+void cea_tp(const Model& M, double p, const double* Y, double T, double* n, CeaOut& o) {
+    const int ns = M.ns, ne = M.ne;
+    double b0[NEX] = {0}, b[NEX] = {0}, bd[NEX] = {0}, vpi[NEX] = {0};
+    double vmurt[NSX], Dlogn[NSX], logn[NSX];
+    int sec_num[NSX];
+    double Ad[NEX][NEX];
+    int elist[NEX], nelist[NEX], nen = 0;
+    bool REDUCEflag;
+    double vTmurt[10];
+    o.status = 0;
+
+    const double logP = std::log(p / pst);
+    for (int i = 1; i <= ne + 2; ++i) b0[i] = Y[1] * M.b0f[i] + Y[2] * M.b0o[i];
+    double b0max = b0[1];
+    for (int i = 2; i <= ne; ++i)
+        if (b0[i] > b0max) b0max = b0[i];
+    double sn = 0.0;
+    for (int j = 1; j <= ns; ++j) sn = sn + n[j];
+    b0[ne + 1] = sn;
+
+    if (Y[1] < Y_eps) {
+        REDUCEflag = true;
+        nen = M.neo;
+        std::memcpy(elist, M.elisto, sizeof(elist));
+        std::memcpy(nelist, M.nelisto, sizeof(nelist));
+        for (int j = 1; j <= ns; ++j) n[j] = n[j] * M.masko[j];
+    } else if (Y[2] < Y_eps) {
+        REDUCEflag = true;
+        nen = M.nef;
+        std::memcpy(elist, M.elistf, sizeof(elist));
+        std::memcpy(nelist, M.nelistf, sizeof(nelist));
+        for (int j = 1; j <= ns; ++j) n[j] = n[j] * M.maskf[j];
+    } else {
+        REDUCEflag = false;
+    }
+
+    const double tinyn = TSIZE * sn;
+    const double logtinyn = std::log(tinyn);
+    const double tinytinyn = TTSIZE * sn;
+    const double logtinytinyn = std::log(tinytinyn);
+
+    const double logT = std::log(T);
+    for (int i = 1; i <= ne + 2; ++i) b[i] = 0.0;
+    b[ne + 1] = sn;
+    for (int j = 1; j <= ns; ++j) logn[j] = logtinyn;
+    for (int j = 1; j <= ns; ++j) {
+        sec_num[j] = check_section_number(M, j, T);
+        if (n[j] > tinyn) {
+            logn[j] = std::log(n[j]);
+            for (int i = 1; i <= ne; ++i) b[i] = b[i] + M.Ac[i][j] * n[j];
+        }
+    }
+    bool flag = true;
+    for (int i = 1; i <= ne; ++i)
+        if (b0[i] > eps && std::fabs(b0[i] - b[i]) > b0max * eps) flag = false;
+
+    int counter = 0;
+    if (!flag) {
+        counter = 1;
+        for (;;) {
+            for (int i = 1; i <= ne; ++i) b[i] = 0.0;
+            for (int i = 1; i <= ne + 2; ++i) bd[i] = b0[i];
+            bd[ne + 1] = b0[ne + 1] - b[ne + 1];
+            for (int i = 1; i <= ne + 2; ++i)
+                for (int j = 1; j <= ne + 2; ++j) Ad[i][j] = 0.0;
+            calc_vTmurt(T, logT, vTmurt);
+            for (int k = 1; k <= ns; ++k) {
+                vmurt[k] = dot9(M.co[k][sec_num[k]], vTmurt) + logn[k] - std::log(b0[ne + 1]) + logP;
+                if (n[k] > tinyn) {
+                    const double vmurtn = vmurt[k] * n[k];
+                    for (int i = 1; i <= ne; ++i) {
+                        for (int j = i; j <= ne; ++j) Ad[i][j] = Ad[i][j] + M.Ac[i][k] * M.Ac[j][k] * n[k];
+                        Ad[i][ne + 1] = Ad[i][ne + 1] + M.Ac[i][k] * n[k];
+                        b[i] = b[i] + M.Ac[i][k] * n[k];
+                        bd[i] = bd[i] + M.Ac[i][k] * (vmurtn - n[k]);
+                    }
+                    bd[ne + 1] = bd[ne + 1] + vmurtn;
+                }
+            }
+            Ad[ne + 1][ne + 1] = b[ne + 1] - b0[ne + 1];
+            for (int i = 1; i <= ne + 1; ++i)
+                for (int j = i + 1; j <= ne + 1; ++j) Ad[j][i] = Ad[i][j];
+
+            bool LUflag;
+            if (REDUCEflag) {
+                for (int i = 1; i <= nen; ++i) {
+                    for (int j = 1; j <= nen; ++j) Ad[i][j] = Ad[elist[i]][elist[j]];
+                    bd[i] = bd[elist[i]];
+                }
+                LUflag = LU(Ad, bd, vpi, nen);
+                if (!LUflag) {
+                    for (int i = nen; i >= 1; --i) vpi[elist[i]] = vpi[i];
+                    for (int i = 1; i <= ne + 1 - nen; ++i) vpi[nelist[i]] = -1e300;
+                }
+            } else {
+                LUflag = LU(Ad, bd, vpi, ne + 1);
+            }
+            if (LUflag) {
+                for (int j = 1; j <= ns; ++j) n[j] = n[j] + initial_eps;
+                sn = 0.0;
+                for (int j = 1; j <= ns; ++j) logn[j] = logtinytinyn;
+                for (int j = 1; j <= ns; ++j) {
+                    if (n[j] < tinytinyn)
+                        n[j] = tinytinyn;
+                    else
+                        logn[j] = std::log(n[j]);
+                    if (n[j] > tinyn) sn = sn + n[j];
+                }
+                b[ne + 1] = sn;
+                counter = counter + 1;
+                if (counter > 500) break;
+                continue;
+            }
+
+            const double Dlogsn = vpi[ne + 1];
+            for (int j = 1; j <= ns; ++j) {
+                double tmp = 0.0;
+                for (int i = 1; i <= ne; ++i) tmp = tmp + M.Ac[i][j] * vpi[i];
+                Dlogn[j] = -vmurt[j] + tmp + Dlogsn;
+            }
+            double lambda1 = 0.0, lambda2 = 1e300;
+            const double logsn = std::log(b0[ne + 1]);
+            for (int j = 1; j <= ns; ++j) {
+                if (logn[j] - logsn > -18.420681)
+                    lambda1 = std::fmax(lambda1, std::fabs(Dlogn[j]));
+                else if (Dlogn[j] > 0.0)
+                    lambda2 = std::fmin(lambda2, std::fabs((-logn[j] + logsn - 9.2103404) / (Dlogn[j] - Dlogsn)));
+            }
+            lambda1 = 2.0 / std::fmax(std::fmax(5.0 * std::fabs(Dlogsn), std::fabs(lambda1)), 2.0);
+            const double omega_var = std::fmin(1.0, std::fmin(lambda1, lambda2));
+
+            b0[ne + 1] = b0[ne + 1] * std::exp(omega_var * Dlogsn);
+            sn = 0.0;
+            double Dnmax = 0.0;
+            for (int j = 1; j <= ns; ++j) logn[j] = logtinytinyn;
+            for (int j = 1; j <= ns; ++j) {
+                n[j] = n[j] * std::exp(omega_var * Dlogn[j]);
+                if (n[j] < tinytinyn)
+                    n[j] = tinytinyn;
+                else
+                    logn[j] = std::log(n[j]);
+                if (n[j] > tinyn) {
+                    sn = sn + n[j];
+                    const double tmp = std::fabs(Dlogn[j]) * n[j];
+                    if (Dnmax < tmp) Dnmax = tmp;
+                }
+            }
+            b[ne + 1] = sn;
+
+            flag = true;
+            if (std::fabs(Dnmax) > eps * sn) flag = false;
+            for (int i = 1; i <= ne; ++i)
+                if (b0[i] > eps && std::fabs(b0[i] - b[i]) > b0max * eps) flag = false;
+            if (std::fabs(Dlogsn) > eps || std::fabs(b0[ne + 1] - b[ne + 1]) > eps * std::fabs(sn)) flag = false;
+            if (counter > 500) flag = true;
+            if (flag) break;
+            counter = counter + 1;
+        }
+        if (counter > 500) o.status = 1;
+    }
+    o.counter = counter;
+    hp_tp_tail(M, T, logT, sn, tinyn, sec_num, n, true, o);
+}
+
 // calc_ini of initialize_cea (sub_chem.f90:1237-1287)
 void calc_ini(const Model& M, double T, double* n, double& E, double& MWave, double* Yfoe) {
     const int ns = M.ns, ne = M.ne;
@@ -575,24 +992,34 @@ int orc_cea_create(const scfd_cea_data* data, scfd_cea** out) {
     for (int s = 0; s < 2; ++s) {
         Y[1] = s == 0 ? 1.0 : 0.0;
         Y[2] = s == 0 ? 0.0 : 1.0;
-        const double rho = ps[s] / (Ru * 1e3 / MWs[s] * Ts[s]);
+        double rho = ps[s] / (Ru * 1e3 / MWs[s] * Ts[s]);
         double* n = ns_[s];
         for (int j = 1; j <= ns; ++j) n[j] = n[j] + initial_eps;
         double T = Ts[s];
-        cea(M, rho, Y, Es[s], T, n, o);
-        if (o.status == 2) {
-            delete h;
-            return SCFD_E_SINGULAR;
-        }
         scfd_cea_stream& S = *st[s];
+        if (d.init_hp) {
+            // sub_chem.f90:1206-1211: H = E + p/rho, cea_hp, then rho and E again
+            const double H = Es[s] + ps[s] / rho;
+            cea_hp(M, ps[s], Y, H, T, n, o);
+            rho = ps[s] / (Ru * 1e3 / o.MWave * T);
+            S.e = H - ps[s] / rho;
+            S.p = ps[s];
+            S.h = H;
+        } else {
+            cea(M, rho, Y, Es[s], T, n, o);
+            if (o.status == 2) {
+                delete h;
+                return SCFD_E_SINGULAR;
+            }
+            S.e = Es[s];
+            S.p = rho * Ru * 1e3 / o.MWave * T;
+            S.h = S.e + S.p / rho;
+        }
         S.rho = rho;
         S.T = T;
-        S.e = Es[s];
         S.mw = o.MWave;
         S.kappa = o.kappa;
         S.mu = o.mu;
-        S.p = rho * Ru * 1e3 / o.MWave * T;
-        S.h = S.e + S.p / rho;
         for (int j = 1; j <= ns; ++j) S.n[j - 1] = n[j];
         (s == 0 ? inf.iters_fuel : inf.iters_oxidizer) = o.counter;
     }
@@ -652,6 +1079,57 @@ int orc_cea_solve(scfd_cea* h, int64_t ncell, const double* rho, const double* Y
     h->fails[0] += f0;
     h->fails[1] += f1;
     return 0;
+}
+
+// fixed p and h (hp) or fixed p and T (tp) over ncell cells
+static int solve_hp_tp(scfd_cea* h, bool hp, int64_t ncell, const double* p, const double* Y, const double* hh,
+                       double* T, double* n, double* hout, double* mwave, double* kappa, double* mu, double* Yv,
+                       double* vhi, int32_t* iters) {
+    if (!h || ncell < 0) return SCFD_E_ARG;
+    if (ncell > 0 && (!p || !Y || !T || !n || (hp && !hh))) return SCFD_E_ARG;
+    const Model& M = *h;
+    const int ns = M.ns;
+    int64_t f0 = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : f0)
+    for (int64_t c = 0; c < ncell; ++c) {
+        double nn[NSX], y[3];
+        CeaOut o;
+        for (int j = 1; j <= ns; ++j) nn[j] = n[(j - 1) * ncell + c];
+        y[1] = Y[c];
+        y[2] = Y[ncell + c];
+        double t = T[c];
+        if (hp)
+            cea_hp(M, p[c], y, hh[c], t, nn, o);
+        else
+            cea_tp(M, p[c], y, t, nn, o);
+        if (o.status == 1) f0 += 1;
+        if (hp) T[c] = t;
+        for (int j = 1; j <= ns; ++j) n[(j - 1) * ncell + c] = nn[j];
+        if (hout) hout[c] = o.H;
+        if (mwave) mwave[c] = o.MWave;
+        if (kappa) kappa[c] = o.kappa;
+        if (mu) mu[c] = o.mu;
+        if (iters) iters[c] = o.counter;
+        for (int j = 1; j <= ns; ++j) {
+            if (Yv) Yv[(j - 1) * ncell + c] = o.Yv[j];
+            if (vhi) vhi[(j - 1) * ncell + c] = o.vhi[j];
+        }
+    }
+    h->fails[0] += f0;
+    return 0;
+}
+
+int orc_cea_solve_hp(scfd_cea* h, int64_t ncell, const double* p, const double* Y, const double* hh, double* T,
+                     double* n, double* mwave, double* kappa, double* mu, double* Yv, double* vhi, int32_t* iters,
+                     void* /*stream*/) {
+    return solve_hp_tp(h, true, ncell, p, Y, hh, T, n, nullptr, mwave, kappa, mu, Yv, vhi, iters);
+}
+
+int orc_cea_solve_tp(scfd_cea* h, int64_t ncell, const double* p, const double* Y, const double* T, double* n,
+                     double* hh, double* mwave, double* kappa, double* mu, double* Yv, double* vhi, int32_t* iters,
+                     void* /*stream*/) {
+    return solve_hp_tp(h, false, ncell, p, Y, nullptr, const_cast<double*>(T), n, hh, mwave, kappa, mu, Yv, vhi,
+                       iters);
 }
 
 int orc_cea_status(scfd_cea* h, int64_t* counts) {

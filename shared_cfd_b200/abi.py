@@ -192,7 +192,8 @@ class CeaData(C.Structure):
         ("To", C.c_double),
         ("nf", C.c_double * CEA_MAX_SPECIES),
         ("no", C.c_double * CEA_MAX_SPECIES),
-        ("reserved", C.c_int32 * 8),
+        ("init_hp", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 
@@ -263,6 +264,8 @@ SIGNATURES = {
     "cea_destroy": (C.c_int, [_P]),
     "cea_info_get": (C.c_int, [_P, C.POINTER(CeaInfo)]),
     "cea_solve": (C.c_int, [_P, C.c_int64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "cea_solve_hp": (C.c_int, [_P, C.c_int64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "cea_solve_tp": (C.c_int, [_P, C.c_int64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "cea_status": (C.c_int, [_P, C.POINTER(C.c_int64)]),
 }
 K_THERMO, K_BC, K_DT, K_CHEM, K_RESIDUAL, K_SWEEP_FWD, K_SWEEP_BWD, K_UPDATE, K_COPY, K_OTHER, K_PACK, K_COUNT = \

@@ -132,11 +132,13 @@ def parse_trans(text, species):
 
 
 def make_data(species, elements, thermo_text, trans_text, mw_text, fuel, oxidizer, pf=1e5, Tf=300.0,
-              po=1e5, To=300.0):
+              po=1e5, To=300.0, init_hp=False):
     """scfd_cea_data of a species set; fuel / oxidizer map species names to
-    mole ratios (control_chem.inp)."""
+    mole ratios (control_chem.inp); init_hp selects initialize_cea('hp') for
+    the stream states (default 'uv')."""
     d = abi.CeaData()
     d.abi_version = abi.ABI_VERSION
+    d.init_hp = 1 if init_hp else 0
     ns, ne = len(species), len(elements)
     if ns > abi.CEA_MAX_SPECIES or ne > abi.CEA_MAX_ELEMENTS:
         raise ValueError("species set too large")
@@ -179,13 +181,13 @@ def _rd(name):
         return f.read()
 
 
-def h2_air_data(pf=1e5, Tf=300.0, po=1e5, To=300.0, fuel=None, oxidizer=None, species=None):
+def h2_air_data(pf=1e5, Tf=300.0, po=1e5, To=300.0, fuel=None, oxidizer=None, species=None, init_hp=False):
     """Hydrogen fuel against air (O2 : N2 = 1 : 3.76) over H2 O2 H2O H O OH
     HO2 H2O2 N2 (or `species`, a subset of them) with the NASA-9 tables of the
     reference's NASA/core."""
     return make_data(species or H2AIR_SPECIES, H2AIR_ELEMENTS, _rd("h2air9_nasa9.dat"),
                      _rd("h2air9_nasa_trans.dat"), _rd("elements_mw_nasa.dat"), fuel or {"H2": 1.0},
-                     oxidizer or {"O2": 1.0, "N2": 3.76}, pf, Tf, po, To)
+                     oxidizer or {"O2": 1.0, "N2": 3.76}, pf, Tf, po, To, init_hp)
 
 
 def hon17_data(pf=1e5, Tf=300.0, po=1e5, To=300.0, fuel=None, oxidizer=None):
@@ -323,3 +325,53 @@ class Cea:
             raise RuntimeError("cea: %d cells met a singular matrix twice" % ng)
         arrs["not_converged"] = nc
         return arrs
+
+    def _host_call(self, fn, order, arrs):
+        if self.on_device:
+            import torch
+            dev = {k: (torch.from_numpy(arrs[k]).cuda() if arrs[k] is not None else None) for k in order}
+            fn(*[dev[k].data_ptr() if dev[k] is not None else None for k in order])
+            code, nc, ng = self.status()
+            for k in order:
+                if dev[k] is not None:
+                    arrs[k] = dev[k].cpu().numpy()
+        else:
+            fn(*[arrs[k].ctypes.data if arrs[k] is not None else None for k in order])
+            code, nc, ng = self.status()
+        arrs["not_converged"] = nc
+        return arrs
+
+    def solve_hp(self, p, Y, h, T, n):
+        """cea_hp per cell at fixed p (Pa) and h (J/kg) on host arrays: returns
+        T, n, MWave, kappa, mu, Yv, vhi, iters (sub_chem.f90:1652-1962)."""
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        m, ns = p.size, self.ns
+        arrs = {"p": p, "Y": np.ascontiguousarray(Y, dtype=np.float64).reshape(2, m),
+                "h": np.ascontiguousarray(h, dtype=np.float64).reshape(m),
+                "T": np.array(T, dtype=np.float64).reshape(m), "n": np.array(n, dtype=np.float64).reshape(ns, m),
+                "MWave": np.zeros(m), "kappa": np.zeros(m), "mu": np.zeros(m), "Yv": np.zeros((ns, m)),
+                "vhi": np.zeros((ns, m)), "iters": np.zeros(m, dtype=np.int32)}
+        order = ["p", "Y", "h", "T", "n", "MWave", "kappa", "mu", "Yv", "vhi", "iters"]
+
+        def fn(*ptr):
+            code = self.lib.cea_solve_hp(self.h, m, *ptr, None)
+            if code:
+                raise RuntimeError("cea_solve_hp failed: %d" % code)
+        return self._host_call(fn, order, arrs)
+
+    def solve_tp(self, p, Y, T, n):
+        """cea_tp per cell at fixed p (Pa) and T (K) on host arrays: returns n,
+        h (J/kg), MWave, kappa, mu, Yv, vhi, iters (sub_chem.f90:1963-2248)."""
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        m, ns = p.size, self.ns
+        arrs = {"p": p, "Y": np.ascontiguousarray(Y, dtype=np.float64).reshape(2, m),
+                "T": np.array(T, dtype=np.float64).reshape(m), "n": np.array(n, dtype=np.float64).reshape(ns, m),
+                "h": np.zeros(m), "MWave": np.zeros(m), "kappa": np.zeros(m), "mu": np.zeros(m),
+                "Yv": np.zeros((ns, m)), "vhi": np.zeros((ns, m)), "iters": np.zeros(m, dtype=np.int32)}
+        order = ["p", "Y", "T", "n", "h", "MWave", "kappa", "mu", "Yv", "vhi", "iters"]
+
+        def fn(*ptr):
+            code = self.lib.cea_solve_tp(self.h, m, *ptr, None)
+            if code:
+                raise RuntimeError("cea_solve_tp failed: %d" % code)
+        return self._host_call(fn, order, arrs)

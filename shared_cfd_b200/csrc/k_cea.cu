@@ -541,6 +541,383 @@ __global__ void __launch_bounds__(128, MINB) k_cea(const CeaTab<NS, NE, NSEC>* _
     }
 }
 
+// LU.f90 on a register matrix (partial pivoting, singular below 1e-30), row
+// swaps as unconditional selects; x = A^-1 b.  Returns false when singular.
+template <int M>
+__device__ __forceinline__ bool lu_solve_reg(double (&A)[M][M], double (&bd)[M], double (&x)[M]) {
+    bool sing = false;
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        double p = fabs(A[k][k]);
+        int ip = k;
+#pragma unroll
+        for (int i = k + 1; i < M; ++i) {
+            const double d = fabs(A[i][k]);
+            if (p < d) {
+                p = d;
+                ip = i;
+            }
+        }
+        if (p < 1e-30) sing = true;
+#pragma unroll
+        for (int i = k + 1; i < M; ++i) {
+            const bool sw = i == ip;
+#pragma unroll
+            for (int j = 0; j < M; ++j) {
+                const double a = A[k][j], b = A[i][j];
+                A[k][j] = sw ? b : a;
+                A[i][j] = sw ? a : b;
+            }
+            const double a = bd[k], b = bd[i];
+            bd[k] = sw ? b : a;
+            bd[i] = sw ? a : b;
+        }
+        const double inv = 1.0 / A[k][k];
+#pragma unroll
+        for (int i = k + 1; i < M; ++i) A[i][k] = A[i][k] * inv;
+#pragma unroll
+        for (int j = k + 1; j < M; ++j) {
+            const double a = A[k][j];
+#pragma unroll
+            for (int i = k + 1; i < M; ++i) A[i][j] = A[i][j] - a * A[i][k];
+        }
+    }
+    double cc[M];
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        cc[k] = bd[k];
+#pragma unroll
+        for (int j = 0; j < k; ++j) cc[k] = cc[k] - A[k][j] * cc[j];
+    }
+    x[M - 1] = cc[M - 1] / A[M - 1][M - 1];
+#pragma unroll
+    for (int k = M - 2; k >= 0; --k) {
+        double v = cc[k];
+#pragma unroll
+        for (int j = k + 1; j < M; ++j) v = v - A[k][j] * x[j];
+        x[k] = v / A[k][k];
+    }
+    return !sing;
+}
+
+struct HpTpOut {
+    double* h;  // tp: mixture enthalpy
+    double* mwave;
+    double* kappa;
+    double* mu;
+    double* Yv;
+    double* vhi;
+    int32_t* iters;
+};
+
+// cea_hp (HP) and cea_tp (sub_chem.f90:1652-2248), one cell per thread.  The
+// unknowns are pi_0..pi_{ne-1}, ln sn (slot NE) and for hp ln T (slot NE+1);
+// as in k_cea, dropped and unused element slots are identity rows.  The
+// singular-matrix retry, unbounded in the reference, counts towards the
+// 500-iteration limit.
+template <int NS, int NE, int NSEC, bool EXACT, bool HP>
+__global__ void __launch_bounds__(128, 2) k_cea_hptp(const CeaTab<NS, NE, NSEC>* __restrict__ gtab, int64_t ncell,
+                                                    const double* __restrict__ p_in, const double* __restrict__ Y_in,
+                                                    const double* __restrict__ h_in, double* __restrict__ T_io,
+                                                    double* __restrict__ n_io, HpTpOut out,
+                                                    unsigned long long* __restrict__ fails) {
+    using Tab = CeaTab<NS, NE, NSEC>;
+    extern __shared__ double smem_tab[];
+    {
+        const double* src = reinterpret_cast<const double*>(gtab);
+        for (int k = threadIdx.x; k < (int)(sizeof(Tab) / sizeof(double)); k += blockDim.x) smem_tab[k] = src[k];
+    }
+    __syncthreads();
+    const Tab& t = *reinterpret_cast<const Tab*>(smem_tab);
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    const int ns = EXACT ? NS : t.ns, ne = EXACT ? NE : t.ne, nt = t.nt;
+    constexpr int M = HP ? NE + 2 : NE + 1;
+    constexpr int SN = NE, LT = NE + 1;
+
+    const double Y0 = Y_in[c], Y1 = Y_in[ncell + c];
+    const double H = HP ? h_in[c] : 0.0;
+    double T = T_io[c];
+    double n[NS], logn[NS], vhrt[NS], dl[NS];
+#pragma unroll
+    for (int j = 0; j < NS; ++j) n[j] = j < ns ? n_io[(int64_t)j * ncell + c] : 0.0;
+
+    const double logP = log(p_in[c] / PST);
+    double b0[NE], keep[NE];
+#pragma unroll
+    for (int i = 0; i < NE; ++i) {
+        b0[i] = i < ne ? Y0 * t.b0f[i] + Y1 * t.b0o[i] : 0.0;  // not masked in hp / tp
+        keep[i] = 1.0;
+    }
+    double b0max = b0[0];
+#pragma unroll
+    for (int i = 1; i < NE; ++i)
+        if (i < ne && b0[i] > b0max) b0max = b0[i];
+    double sn = 0.0;
+#pragma unroll
+    for (int j = 0; j < NS; ++j)
+        if (j < ns) sn += n[j];
+    double b0sn = sn;  // b0(ne+1)
+    const int mode = Y0 < Y_EPS ? 1 : (Y1 < Y_EPS ? 2 : 0);
+    if (mode) {
+#pragma unroll
+        for (int j = 0; j < NS; ++j)
+            if (j < ns) n[j] = n[j] * (mode == 1 ? t.masko[j] : t.maskf[j]);
+#pragma unroll
+        for (int i = 0; i < NE; ++i) keep[i] = i < ne ? (mode == 1 ? t.keepo[i] : t.keepf[i]) : 1.0;
+    }
+    const double tinyn = TSIZE * sn;
+    const double logtinyn = log(tinyn);
+    const double tinytinyn = TTSIZE * sn;
+    const double logtinytinyn = log(tinytinyn);
+
+    double logT = log(T);
+    double vh[9];
+    v_hrt(T, logT, vh);
+    double b[NE], bsn = sn, bh = 0.0;  // b(1:ne), b(ne+1), b(ne+2)
+#pragma unroll
+    for (int i = 0; i < NE; ++i) b[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < NS; ++j) {
+        vhrt[j] = 0.0;
+        logn[j] = logtinyn;
+        if (j < ns && n[j] > tinyn) {
+            if (HP) vhrt[j] = dot9(t.co[j][section<Tab, NSEC>(t, j, T)], vh);
+            logn[j] = log(n[j]);
+#pragma unroll
+            for (int i = 0; i < NE; ++i)
+                if (i < ne) b[i] += t.ac[i][j] * n[j];
+            bh += vhrt[j] * n[j];
+        }
+    }
+    bool flag = true;
+#pragma unroll
+    for (int i = 0; i < NE; ++i)
+        if (i < ne && b0[i] > EPS && fabs(b0[i] - b[i]) > b0max * EPS) flag = false;
+    if (HP && fabs(H - bh * RU * T) > EPS * fabs(H)) flag = false;
+
+    int counter = 0;
+    if (!flag) {
+        counter = 1;
+        for (;;) {
+            double A[M][M], bd[M], vpi[M];
+#pragma unroll
+            for (int i = 0; i < M; ++i)
+#pragma unroll
+                for (int j = 0; j < M; ++j) A[i][j] = 0.0;
+#pragma unroll
+            for (int i = 0; i < NE; ++i) {
+                b[i] = 0.0;
+                bd[i] = b0[i];
+            }
+            bd[SN] = b0sn - bsn;
+            if constexpr (HP) bd[LT] = H / (RU * T) - bh;
+            double vm[9], vc[9];
+            v_murt(T, logT, vm);
+            if (HP) v_cpr(T, vc);
+            const double lb0sn = log(b0sn);
+            double aSL = 0.0, aLL = 0.0;
+#pragma unroll
+            for (int k = 0; k < NS; ++k) {
+                if (k >= ns) continue;
+                const int s = section<Tab, NSEC>(t, k, T);
+                dl[k] = dot9(t.co[k][s], vm) + logn[k] - lb0sn + logP;
+                if (n[k] > tinyn) {
+                    const double vmurtn = dl[k] * n[k];
+#pragma unroll
+                    for (int i = 0; i < NE; ++i) {
+                        if (i >= ne) continue;
+                        const double aik = t.ac[i][k];
+#pragma unroll
+                        for (int j = i; j < NE; ++j)
+                            if (j < ne) A[i][j] += aik * t.ac[j][k] * n[k];
+                        A[i][SN] += aik * n[k];
+                        if constexpr (HP) A[i][LT] += aik * vhrt[k] * n[k];
+                        b[i] += aik * n[k];
+                        bd[i] += aik * (vmurtn - n[k]);
+                    }
+                    if constexpr (HP) {
+                        aSL += n[k] * vhrt[k];
+                        aLL += n[k] * (vhrt[k] * vhrt[k] + dot9(t.co[k][s], vc));
+                        bd[LT] += vmurtn * vhrt[k];
+                    }
+                    bd[SN] += vmurtn;
+                }
+            }
+            A[SN][SN] = bsn - b0sn;
+            if constexpr (HP) {
+                A[SN][LT] = aSL;
+                A[LT][LT] = aLL;
+            }
+#pragma unroll
+            for (int i = 0; i < M; ++i)
+#pragma unroll
+                for (int j = i + 1; j < M; ++j) A[j][i] = A[i][j];
+#pragma unroll
+            for (int r = 0; r < NE; ++r) {
+                if (r < ne && keep[r] != 0.0) continue;
+#pragma unroll
+                for (int j = 0; j < M; ++j) {
+                    A[r][j] = 0.0;
+                    A[j][r] = 0.0;
+                }
+                A[r][r] = 1.0;
+                bd[r] = 0.0;
+            }
+            if (!lu_solve_reg<M>(A, bd, vpi)) {
+                sn = 0.0;
+                bh = 0.0;
+#pragma unroll
+                for (int j = 0; j < NS; ++j) {
+                    if (j >= ns) continue;
+                    n[j] = n[j] + INITIAL_EPS;
+                    logn[j] = logtinytinyn;
+                    if (n[j] < tinytinyn)
+                        n[j] = tinytinyn;
+                    else
+                        logn[j] = log(n[j]);
+                    if (n[j] > tinyn) {
+                        if (HP) {
+                            vhrt[j] = dot9(t.co[j][section<Tab, NSEC>(t, j, T)], vh);
+                            bh += vhrt[j] * n[j];
+                        }
+                        sn += n[j];
+                    }
+                }
+                bsn = sn;
+                counter = counter + 1;
+                if (counter > MAX_ITER) break;
+                continue;
+            }
+#pragma unroll
+            for (int r = 0; r < NE; ++r)
+                if (r < ne && keep[r] == 0.0) vpi[r] = -1e300;
+            const double dlsn = vpi[SN];
+            const double dlogT = HP ? vpi[LT] : 0.0;
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                if (j >= ns) continue;
+                double x = 0.0;
+#pragma unroll
+                for (int i = 0; i < NE; ++i)
+                    if (i < ne) x += t.ac[i][j] * vpi[i];
+                dl[j] = HP ? -dl[j] + x + dlsn + vhrt[j] * dlogT : -dl[j] + x + dlsn;
+            }
+            double lambda1 = 0.0, lambda2 = 1e300;
+            const double logsn = lb0sn;
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                if (j >= ns) continue;
+                if (logn[j] - logsn > -18.420681)
+                    lambda1 = fmax(lambda1, fabs(dl[j]));
+                else if (dl[j] > 0.0)
+                    lambda2 = fmin(lambda2, fabs((-logn[j] + logsn - 9.2103404) / (dl[j] - dlsn)));
+            }
+            if (HP)
+                lambda1 = 2.0 / fmax(fmax(fmax(5.0 * fabs(dlogT), 5.0 * fabs(dlsn)), fabs(lambda1)), 2.0);
+            else
+                lambda1 = 2.0 / fmax(fmax(5.0 * fabs(dlsn), fabs(lambda1)), 2.0);
+            const double om = fmin(1.0, fmin(lambda1, lambda2));
+            b0sn = b0sn * exp(om * dlsn);
+            if (HP) {
+                T = T * exp(om * dlogT);
+                logT = log(T);
+                v_hrt(T, logT, vh);
+            }
+            sn = 0.0;
+            bh = 0.0;
+            double dnmax = 0.0;
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                if (j >= ns) continue;
+                n[j] = n[j] * exp(om * dl[j]);
+                logn[j] = logtinytinyn;
+                if (n[j] < tinytinyn)
+                    n[j] = tinytinyn;
+                else
+                    logn[j] = log(n[j]);
+                if (n[j] > tinyn) {
+                    if (HP) {
+                        vhrt[j] = dot9(t.co[j][section<Tab, NSEC>(t, j, T)], vh);
+                        bh += vhrt[j] * n[j];
+                    }
+                    sn += n[j];
+                    const double x = fabs(dl[j]) * n[j];
+                    if (dnmax < x) dnmax = x;
+                }
+            }
+            bsn = sn;
+            flag = true;
+            if (fabs(dnmax) > EPS * sn) flag = false;
+#pragma unroll
+            for (int i = 0; i < NE; ++i)
+                if (i < ne && b0[i] > EPS && fabs(b0[i] - b[i]) > b0max * EPS) flag = false;
+            if (fabs(dlsn) > EPS || fabs(b0sn - bsn) > EPS * fabs(sn)) flag = false;
+            if (HP && (fabs(dlogT) > EPS || fabs(H - bh * RU * T) > EPS * fabs(H))) flag = false;
+            if (counter > MAX_ITER) flag = true;
+            if (flag) break;
+            ++counter;
+        }
+    }
+    if (counter > MAX_ITER) atomicAdd(&fails[0], 1ull);
+    if (HP) T_io[c] = T;
+#pragma unroll
+    for (int j = 0; j < NS; ++j)
+        if (j < ns) n_io[(int64_t)j * ncell + c] = n[j];
+    if (out.iters) out.iters[c] = counter;
+    if (out.mwave) out.mwave[c] = 1e3 / sn;
+    double vc[9];
+    v_cpr(T, vc);
+    double kap = 0.0;
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+        if (i < ns && n[i] > tinyn) kap += n[i] * dot9(t.co[i][section<Tab, NSEC>(t, i, T)], vc);
+    if (out.kappa) out.kappa[c] = kap / (kap - sn);
+    v_hrt(T, logT, vh);
+    const double rt3 = RU * 1e3 * T;
+    double hsum = 0.0;
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        if (i >= ns) continue;
+        const double dh = dot9(t.co[i][section<Tab, NSEC>(t, i, T)], vh);
+        if (out.vhi) out.vhi[(int64_t)i * ncell + c] = rt3 / t.mw[i] * dh;
+        hsum += n[i] * dh;
+        if (out.Yv) out.Yv[(int64_t)i * ncell + c] = n[i] * t.mw[i] * 1e-3;
+    }
+    if (!HP && out.h) out.h[c] = hsum * RU * T;
+    if (out.mu) {
+        const double tt = 1.0 / (T * T);
+        double sq[NS], rs[NS], nfit[NS];
+#pragma unroll
+        for (int i = 0; i < NS; ++i) {
+            sq[i] = rs[i] = nfit[i] = 0.0;
+            if (i >= nt) continue;
+            const int s = tsection(t.tthi[i], t.ttlo[i], t.ntsec[i], T);
+            const double* a = t.trans[i][s];
+            const double muN = exp(a[0] * logT + a[1] * (tt * T) + a[2] * tt + a[3] * 1.0);
+            sq[i] = sqrt(muN);
+            rs[i] = rsqrt(muN);
+#pragma unroll
+            for (int k = 0; k < NS; ++k)
+                if (k == t.tr2th[i]) nfit[i] = n[k];
+        }
+        double mu = 0.0;
+#pragma unroll
+        for (int i = 0; i < NS; ++i) {
+            if (i >= nt) continue;
+            double denom = 0.0;
+#pragma unroll
+            for (int j = 0; j < NS; ++j) {
+                if (j >= nt) continue;
+                const double f = 1.0 + sq[i] * rs[j] * t.wmw[i][j];
+                denom += nfit[j] * (0.25 * (f * f) * t.wsq[i][j]);
+            }
+            mu += nfit[i] * (sq[i] * sq[i]) / denom;
+        }
+        out.mu[c] = mu * 1e-7;
+    }
+}
+
 template <class Tab>
 void fill_tab(Tab& t, const scfd_cea_data& d, const double* b0f, const double* b0o, const double* yfe,
               const double* yoe, const double* maskf, const double* masko, const double* keepf,
@@ -624,6 +1001,26 @@ int cea_launch(scfd_cea* h, int64_t ncell, const double* rho, const double* Y, c
         k_cea<SCFD_CEA_MAX_SPECIES, SCFD_CEA_MAX_ELEMENTS, SCFD_CEA_MAX_SECTIONS, false, 1>
             <<<(unsigned)blocks, threads, sizeof(TabBig), st>>>((const TabBig*)h->d_tab, ncell, rho, Y, e, T, n,
                                                                  out, h->d_fail);
+    return cudaGetLastError() == cudaSuccess ? 0 : SCFD_E_CUDA;
+}
+
+template <bool HP>
+int cea_hptp_launch(scfd_cea* h, int64_t ncell, const double* p, const double* Y, const double* hh, double* T,
+                    double* n, const HpTpOut& out, cudaStream_t st) {
+    if (ncell == 0) return 0;
+    const int threads = 128;
+    const int64_t blocks = (ncell + threads - 1) / threads;
+    if (blocks > 0x7fffffff) return SCFD_E_ARG;
+    if (h->kind == KIND_9_3)
+        k_cea_hptp<9, 3, 3, true, HP><<<(unsigned)blocks, threads, sizeof(TabH2Air), st>>>(
+            (const TabH2Air*)h->d_tab, ncell, p, Y, hh, T, n, out, h->d_fail);
+    else if (h->kind == KIND_SMALL)
+        k_cea_hptp<12, 4, 3, false, HP><<<(unsigned)blocks, threads, sizeof(TabSmall), st>>>(
+            (const TabSmall*)h->d_tab, ncell, p, Y, hh, T, n, out, h->d_fail);
+    else
+        k_cea_hptp<SCFD_CEA_MAX_SPECIES, SCFD_CEA_MAX_ELEMENTS, SCFD_CEA_MAX_SECTIONS, false, HP>
+            <<<(unsigned)blocks, threads, sizeof(TabBig), st>>>((const TabBig*)h->d_tab, ncell, p, Y, hh, T, n, out,
+                                                                 h->d_fail);
     return cudaGetLastError() == cudaSuccess ? 0 : SCFD_E_CUDA;
 }
 
@@ -795,7 +1192,9 @@ int scfd_cea_create(const scfd_cea_data* data, scfd_cea** out) {
         nf[j] = nf[j] + INITIAL_EPS;
         no[j] = no[j] + INITIAL_EPS;
     }
-    // cell 0: fuel (Y = 1, 0); cell 1: oxidizer (Y = 0, 1)
+    // cell 0: fuel (Y = 1, 0); cell 1: oxidizer (Y = 0, 1).  'uv': cea at the
+    // stream's rho and e; 'hp': cea_hp at its p and h = e + p/rho
+    // (sub_chem.f90:1196-1228)
     std::vector<double> hbuf(2 * (6 + 3 * ns + 3 + 2), 0.0);
     double* rho = hbuf.data();
     double* Y = rho + 2;
@@ -805,14 +1204,14 @@ int scfd_cea_create(const scfd_cea_data* data, scfd_cea** out) {
     double* mwv = n + 2 * ns;
     double* kap = mwv + 2;
     double* mu = kap + 2;
+    const double Es[2] = {Ef, Eo}, ps[2] = {d.pf, d.po};
     rho[0] = rhof;
     rho[1] = rhoo;
     Y[0] = 1.0;
     Y[1] = 0.0;
     Y[2] = 0.0;
     Y[3] = 1.0;
-    E[0] = Ef;
-    E[1] = Eo;
+    for (int s2 = 0; s2 < 2; ++s2) E[s2] = d.init_hp ? Es[s2] + ps[s2] / rho[s2] : Es[s2];
     T[0] = d.Tf;
     T[1] = d.To;
     for (int j = 0; j < ns; ++j) {
@@ -822,16 +1221,24 @@ int scfd_cea_create(const scfd_cea_data* data, scfd_cea** out) {
     const size_t nb = hbuf.size() * sizeof(double);
     double* dbuf = nullptr;
     int32_t* dit = nullptr;
-    if ((e = cudaMalloc(&dbuf, nb + 2 * sizeof(int32_t))) != cudaSuccess) return fail(e);
-    dit = (int32_t*)((char*)dbuf + nb);
+    if ((e = cudaMalloc(&dbuf, nb + 2 * sizeof(double) + 2 * sizeof(int32_t))) != cudaSuccess) return fail(e);
+    double* dp = (double*)((char*)dbuf + nb);
+    dit = (int32_t*)(dp + 2);
     int32_t it[2] = {0, 0};
     e = cudaMemcpy(dbuf, hbuf.data(), nb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dp, ps, sizeof(ps), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
         const size_t off_mw = (size_t)(mwv - hbuf.data());
-        CellOut o{dbuf + off_mw, dbuf + off_mw + 2, dbuf + off_mw + 4, nullptr, nullptr, nullptr, dit};
         const size_t off_T = (size_t)(T - hbuf.data()), off_n = (size_t)(n - hbuf.data());
-        if (cea_launch(h, 2, dbuf, dbuf + 2, dbuf + 6, dbuf + off_T, dbuf + off_n, o, 0) != 0)
-            e = cudaGetLastError();
+        int rc;
+        if (d.init_hp) {
+            HpTpOut o{nullptr, dbuf + off_mw, dbuf + off_mw + 2, dbuf + off_mw + 4, nullptr, nullptr, dit};
+            rc = cea_hptp_launch<true>(h, 2, dp, dbuf + 2, dbuf + 6, dbuf + off_T, dbuf + off_n, o, 0);
+        } else {
+            CellOut o{dbuf + off_mw, dbuf + off_mw + 2, dbuf + off_mw + 4, nullptr, nullptr, nullptr, dit};
+            rc = cea_launch(h, 2, dbuf, dbuf + 2, dbuf + 6, dbuf + off_T, dbuf + off_n, o, 0);
+        }
+        if (rc != 0) e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpy(hbuf.data(), dbuf, nb, cudaMemcpyDeviceToHost);
         if (e == cudaSuccess) e = cudaMemcpy(it, dit, sizeof(it), cudaMemcpyDeviceToHost);
     }
@@ -845,18 +1252,24 @@ int scfd_cea_create(const scfd_cea_data* data, scfd_cea** out) {
         return SCFD_E_SINGULAR;
     }
     scfd_cea_stream* st[2] = {&inf.fuel, &inf.oxidizer};
-    const double Es[2] = {Ef, Eo};
-    for (int s = 0; s < 2; ++s) {
-        scfd_cea_stream& o = *st[s];
-        o.rho = rho[s];
-        o.T = T[s];
-        o.e = Es[s];
-        o.mw = mwv[s];
-        o.kappa = kap[s];
-        o.mu = mu[s];
-        o.p = o.rho * RU * 1e3 / o.mw * o.T;
-        o.h = o.e + o.p / o.rho;
-        for (int j = 0; j < ns; ++j) o.n[j] = n[2 * j + s];
+    for (int s2 = 0; s2 < 2; ++s2) {
+        scfd_cea_stream& o = *st[s2];
+        o.T = T[s2];
+        o.mw = mwv[s2];
+        o.kappa = kap[s2];
+        o.mu = mu[s2];
+        if (d.init_hp) {
+            o.p = ps[s2];
+            o.h = E[s2];
+            o.rho = o.p / (RU * 1e3 / o.mw * o.T);
+            o.e = o.h - o.p / o.rho;
+        } else {
+            o.rho = rho[s2];
+            o.e = Es[s2];
+            o.p = o.rho * RU * 1e3 / o.mw * o.T;
+            o.h = o.e + o.p / o.rho;
+        }
+        for (int j = 0; j < ns; ++j) o.n[j] = n[2 * j + s2];
     }
     inf.iters_fuel = it[0];
     inf.iters_oxidizer = it[1];
@@ -890,6 +1303,28 @@ int scfd_cea_solve(scfd_cea* h, int64_t ncell, const double* rho, const double* 
     h->last = st;
     const CellOut o{mwave, kappa, mu, Yv, vhi, DHi, iters};
     return cea_launch(h, ncell, rho, Y, e, T, n, o, st);
+}
+
+int scfd_cea_solve_hp(scfd_cea* h, int64_t ncell, const double* p, const double* Y, const double* hh, double* T,
+                      double* n, double* mwave, double* kappa, double* mu, double* Yv, double* vhi, int32_t* iters,
+                      void* stream) {
+    if (!h || ncell < 0) return SCFD_E_ARG;
+    if (ncell > 0 && (!p || !Y || !hh || !T || !n)) return SCFD_E_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    h->last = st;
+    const HpTpOut o{nullptr, mwave, kappa, mu, Yv, vhi, iters};
+    return cea_hptp_launch<true>(h, ncell, p, Y, hh, T, n, o, st);
+}
+
+int scfd_cea_solve_tp(scfd_cea* h, int64_t ncell, const double* p, const double* Y, const double* T, double* n,
+                      double* hh, double* mwave, double* kappa, double* mu, double* Yv, double* vhi, int32_t* iters,
+                      void* stream) {
+    if (!h || ncell < 0) return SCFD_E_ARG;
+    if (ncell > 0 && (!p || !Y || !T || !n)) return SCFD_E_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    h->last = st;
+    const HpTpOut o{hh, mwave, kappa, mu, Yv, vhi, iters};
+    return cea_hptp_launch<false>(h, ncell, p, Y, nullptr, const_cast<double*>(T), n, o, st);
 }
 
 int scfd_cea_status(scfd_cea* h, int64_t* counts) {

@@ -216,3 +216,53 @@ def test_empty_batch_and_bad_arguments(model, orc, data):
     for j in range(9):
         bad.nf[j] = 0.0
     assert orc.cea_create(C.byref(bad), C.byref(h)) == abi.E_ARG
+
+
+def uv_states(model, m=300, seed=13):
+    """Equilibrium states from cea (uv): rho, Y, e, T, n, p, h."""
+    inf = model.info()
+    rho, Y, e, T = cea.random_states(inf, m, seed=seed)
+    out = model.solve(rho, Y, e, T, model.initial_n(m))
+    p = rho * RU * 1e3 / out["MWave"] * out["T"]
+    return rho, Y, e, out, p, e + p / rho
+
+
+def test_hp_recovers_the_uv_equilibrium(model):
+    """cea_hp at the p and h of a cea (uv) equilibrium, from a different start,
+    returns the same T and composition (sub_chem.f90:1652-1962)."""
+    rho, Y, e, uv, p, h = uv_states(model)
+    mixed = (Y[0] >= 1e-6) & (Y[1] >= 1e-6)
+    out = model.solve_hp(p[mixed], Y[:, mixed], h[mixed], np.full(mixed.sum(), 1200.0),
+                         model.initial_n(int(mixed.sum())))
+    assert out["not_converged"] == 0
+    np.testing.assert_allclose(out["T"], uv["T"][mixed], rtol=1e-7)
+    sn = uv["n"][:, mixed].sum(axis=0)
+    assert np.max(np.abs(out["n"] - uv["n"][:, mixed]) / sn) < 1e-7
+    np.testing.assert_allclose(out["kappa"], uv["kappa"][mixed], rtol=1e-6)
+    np.testing.assert_allclose(out["mu"], uv["mu"][mixed], rtol=1e-6)
+
+
+def test_tp_recovers_the_uv_equilibrium_and_its_enthalpy(model):
+    """cea_tp at the p and T of a cea (uv) equilibrium returns its composition
+    and h = e + p/rho (sub_chem.f90:1963-2248)."""
+    rho, Y, e, uv, p, h = uv_states(model, seed=14)
+    mixed = (Y[0] >= 1e-6) & (Y[1] >= 1e-6)
+    out = model.solve_tp(p[mixed], Y[:, mixed], uv["T"][mixed], model.initial_n(int(mixed.sum())))
+    assert out["not_converged"] == 0
+    sn = uv["n"][:, mixed].sum(axis=0)
+    assert np.max(np.abs(out["n"] - uv["n"][:, mixed]) / sn) < 1e-7
+    scale = np.abs(h[mixed]) + RU * uv["T"][mixed] * sn
+    assert np.max(np.abs(out["h"] - h[mixed]) / scale) < 1e-7
+
+
+def test_hp_stream_states(orc):
+    """initialize_cea('hp'): the streams at their own p and h stay at 300 K,
+    1e5 Pa and reproduce the 'uv' states."""
+    with cea.Cea(cea.h2_air_data(init_hp=True), lib=orc) as a, cea.Cea(cea.h2_air_data(), lib=orc) as b:
+        x, y = a.info(), b.info()
+        for s in ("fuel", "oxidizer"):
+            u, v = getattr(x, s), getattr(y, s)
+            assert u.p == pytest.approx(1e5, rel=1e-12)
+            assert u.T == pytest.approx(v.T, rel=1e-8)
+            for k in ("rho", "e", "h", "mw", "kappa", "mu"):
+                assert getattr(u, k) == pytest.approx(getattr(v, k), rel=1e-7), (s, k)
