@@ -286,7 +286,8 @@ def reactor_workload():
             (REACTOR_N, REACTOR_DT_CALL, REACTOR_T_END))
 
 
-def cpu_reactors(cores, n=REACTOR_N):
+def cpu_reactors(cores, n=None):
+    n = REACTOR_N if n is None else n
     from shared_cfd_b200.reactors import Reactors
     so = os.path.join(ROOT, "oracle", "_build", "liborc.so")
     if not os.path.exists(so):
@@ -674,6 +675,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sharded", action="store_true", help="block-sharded path also at N = 1 (needs torchrun)")
     ap.add_argument("--cea-cells", type=int, default=0, help="cells of --config cea (default 2^22)")
+    ap.add_argument("--reactors-n", type=int, default=0, help="reactors of --config reactors (default 8192)")
+    ap.add_argument("--reactors-t-end", type=float, default=0.0, help="end time of --config reactors (default 2e-3 s)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -681,6 +684,11 @@ def main():
     cores = os.cpu_count() or 1
 
     if args.config == "reactors":
+        global REACTOR_N, REACTOR_T_END
+        if args.reactors_n > 0:
+            REACTOR_N = args.reactors_n
+        if args.reactors_t_end > 0.0:
+            REACTOR_T_END = args.reactors_t_end
         return run_reactors(args, rank, cores)
     if args.config == "adjoint":
         return run_adjoint(args, rank, cores)

@@ -94,7 +94,7 @@ __host__ __device__ inline int warp_mem_doubles(int ns, int nr) {
 
 // Fex_var of the state n (shared memory) by one warp: species thermo and
 // reaction rates across lanes, per-species sums in the serial order.
-__device__ void warp_fex(const DevChem& ch, const RateLists& rl, const double* n, double* dndtp, double* dndtm,
+__device__ __noinline__ void warp_fex(const DevChem& ch, const RateLists& rl, const double* n, double* dndtp, double* dndtm,
                          WarpMem& w, int lane) {
     const int ns = ch.ns, nr = ch.nr;
     double sn = 0.0;
@@ -143,7 +143,7 @@ __device__ void warp_fex(const DevChem& ch, const RateLists& rl, const double* n
 // by one warp: species thermo and reactions across lanes, the per-species
 // sums in the reference's serial order (net lists), the T row on lane j.
 // dndt[0..ns] and, for Jex, J (row-major N x N) are written to shared memory.
-__device__ void warp_jex(const DevChem& ch, const RateLists& rl, const double* n, double* dndt, double* J,
+__device__ __noinline__ void warp_jex(const DevChem& ch, const RateLists& rl, const double* n, double* dndt, double* J,
                          WarpMem& w, int lane) {
     const int ns = ch.ns, nr = ch.nr, N = ns + 1;
     const bool jac = J != nullptr;
