@@ -65,7 +65,14 @@ enum { SCFD_DT_GLOBAL = 0, SCFD_DT_LOCAL = 1, SCFD_DT_FIXED = 2 }; /* checkout_f
 /* checkout_flow.py:134-181 (the values of its time-scheme line); DUAL is the
  * Weiss-Smith preconditioned dual time of store/time_scheme/dual/2d (2d, global
  * or fixed dt, non-reacting: checkout_flow.py:159-168) */
-enum { SCFD_SCHEME_EULER = 0, SCFD_SCHEME_LUSGS = 2, SCFD_SCHEME_NR = 3, SCFD_SCHEME_DUAL = 5 };
+enum {
+    SCFD_SCHEME_EULER = 0,
+    SCFD_SCHEME_LUSGS = 2,
+    SCFD_SCHEME_NR = 3,
+    SCFD_SCHEME_PRECON = 4,        /* time_scheme/precon/2d: preconditioned NR inner loop, local dt */
+    SCFD_SCHEME_DUAL = 5,
+    SCFD_SCHEME_PRECON_LUSGS = 6   /* time_scheme/preconLU-SGS/2d: preconditioned LU-SGS, local dt */
+};
 enum { SCFD_RECON_UPWIND = 0, SCFD_RECON_MUSCL = 1 };           /* checkout_flow.py:183-194 */
 enum { SCFD_THERMO_IDEAL = 0, SCFD_THERMO_CHEMKIN_COLD = 1, SCFD_THERMO_CHEMKIN_REACTIVE = 2 };
 enum { SCFD_MU_REFERENCE = 0, SCFD_MU_SUTHERLAND = 1 };        /* ideal gas viscosity law */

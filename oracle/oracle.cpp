@@ -1415,10 +1415,17 @@ void calc_next_step_euler(orc_ctx& c) {  // store/time_scheme/euler/time_euler_v
 
 // set_ABpm: LU-SGS/q2d/sch_lusgs.raw.f90:1-149 (alpha with Vol/dt) and
 // NR/q2d/sch_NR.raw.f90:1-149 (alpha with 3Vol/(2dt)); dpdq on q2d only.
+// set_ABpm of LU-SGS and NR, and of the precon schemes
+// (time_scheme/precon/2d/sch_precon.raw.f90:1-202, preconLU-SGS/2d the same
+// with alpha from Vol/dt): low-Mach reference velocity Ur, preconditioned
+// spectral radii, the local time step written to dt_mat, pre1 = phh (Y, u, v,
+// H) with phh = -1/(c^2 + 1/phi), pre2 = (g1 Vs/2 + DHi, -g1 u, -g1 v, g1), and
+// the Jacobians premultiplied by I + pre1 pre2^T.
 void set_ABpm(orc_ctx& c) {
     const int nY = c.nY, D = c.D;
-    const bool nr = c.d.scheme == SCFD_SCHEME_NR;
+    const bool nr = c.d.scheme == SCFD_SCHEME_NR || c.d.scheme == SCFD_SCHEME_PRECON;
     const bool q2d = c.d.dim == SCFD_DIM_Q2D;
+    const bool pc = c.d.scheme == SCFD_SCHEME_PRECON || c.d.scheme == SCFD_SCHEME_PRECON_LUSGS;
     for (int p = 1; p <= c.np; ++p) {
         if (!c.own(p)) continue;
 #pragma omp parallel for
@@ -1433,6 +1440,28 @@ void set_ABpm(orc_ctx& c) {
                 double unA = c.vnci(1, i, j, p) * u + c.vnci(2, i, j, p) * v;
                 double unB = c.vncj(1, i, j, p) * u + c.vncj(2, i, j, p) * v;
                 double nuA = std::fabs(unA) + cs, nuB = std::fabs(unB) + cs;
+                if (pc) {
+                    const double Vv = c.w(c.indxMu, i, j, p) / rho / std::min(c.dsci(i, j, p), c.dscj(i, j, p));
+                    const double Ur = std::min(std::max(Vv, std::sqrt(Vs)), cs);
+                    c.phi(i, j, p) = 1.0 / sq(Ur) - 1.0 / sq(cs);
+                    const double alp = 0.5 * (1.0 - sq(Ur / cs));
+                    double ud = unA * (1.0 - alp), cd = std::sqrt(sq(alp) * sq(unA) + sq(Ur));
+                    nuA = std::fabs(ud) + cd;
+                    ud = unB * (1.0 - alp);
+                    cd = std::sqrt(sq(alp) * sq(unB) + sq(Ur));
+                    nuB = std::fabs(ud) + cd;
+                    const double uds = nuA * (c.dsi(i, j, p) + c.dsi(i - 1, j, p)) + nuB * (c.dsj(i, j, p) + c.dsj(i, j - 1, p));
+                    c.dt_mat(i, j, p) = c.d.cfl * c.Vol(i, j, p) / std::max(uds, c.w(c.indxMu, i, j, p) / rho);
+                    const double phh = -1.0 / (sq(cs) + 1.0 / c.phi(i, j, p));
+                    for (int k = 1; k <= nY; ++k) c.pre1(k, i, j, p) = phh * c.w(4 + k, i, j, p);
+                    c.pre1(nY + 1, i, j, p) = phh * u;
+                    c.pre1(nY + 2, i, j, p) = phh * v;
+                    c.pre1(nY + 3, i, j, p) = phh * H;
+                    for (int k = 1; k <= nY; ++k) c.pre2(k, i, j, p) = 0.5 * gmmad * Vs + c.DHi(k, i, j, p);
+                    c.pre2(nY + 1, i, j, p) = -gmmad * u;
+                    c.pre2(nY + 2, i, j, p) = -gmmad * v;
+                    c.pre2(nY + 3, i, j, p) = gmmad;
+                }
                 if (q2d) {
                     for (int k = 1; k <= nY; ++k) c.dpdq(k, i, j, p) = 0.5 * gmmad * Vs + c.DHi(k, i, j, p);
                     c.dpdq(nY + 1, i, j, p) = -gmmad * u;
@@ -1469,6 +1498,18 @@ void set_ABpm(orc_ctx& c) {
                     b(nY + 1, k) = tB[nY];
                     b(nY + 2, k) = tB[nY + 1] + c.DHi(k, i, j, p);
                     b(nY + 3, k) = tB[nY + 2] + c.DHi(k, i, j, p) * v;
+                }
+                if (pc) {  // multiply preM (sch_precon.raw.f90:148-166)
+                    for (int k = 1; k <= D; ++k) {
+                        double tmp = 0.0;
+                        for (int l = 1; l <= D; ++l) tmp = tmp + c.pre2(l, i, j, p) * a(l, k);
+                        for (int l = 1; l <= D; ++l) a(l, k) = a(l, k) + c.pre1(l, i, j, p) * tmp;
+                    }
+                    for (int k = 1; k <= D; ++k) {
+                        double tmp = 0.0;
+                        for (int l = 1; l <= D; ++l) tmp = tmp + c.pre2(l, i, j, p) * b(l, k);
+                        for (int l = 1; l <= D; ++l) b(l, k) = b(l, k) + c.pre1(l, i, j, p) * tmp;
+                    }
                 }
                 for (int cc = 1; cc <= D; ++cc)
                     for (int rr = 1; rr <= D; ++rr) {
@@ -1711,7 +1752,8 @@ void dual_sweeps(orc_ctx& c, double& res_out, double& omega_out) {
 // (global) omega.  Returns 0 or SCFD_E_OMEGA.
 void lusgs_sweeps(orc_ctx& c, double& res_out, double& omega_out) {
     const int nY = c.nY, D = c.D;
-    const bool nr = c.d.scheme == SCFD_SCHEME_NR;
+    const bool nr = c.d.scheme == SCFD_SCHEME_NR || c.d.scheme == SCFD_SCHEME_PRECON;
+    const bool pc = c.d.scheme == SCFD_SCHEME_PRECON || c.d.scheme == SCFD_SCHEME_PRECON_LUSGS;
     const bool q2d = c.d.dim == SCFD_DIM_Q2D;
     auto& Dq = c.Dq;
     double omega = 1e300;
@@ -1721,11 +1763,17 @@ void lusgs_sweeps(orc_ctx& c, double& res_out, double& omega_out) {
         int ni = c.ni[p - 1], nj = c.nj[p - 1];
 #pragma omp parallel for
         for (int j = 1; j <= nj; ++j)
-            for (int i = 1; i <= ni; ++i)
-                for (int k = 1; k <= D; ++k) {
-                    double s = rhs_k(c, k, i, j, p);
-                    Dq(k, i, j, p) = nr ? s - c.Vol(i, j, p) * c.dqdt(k, i, j, p) : s;
+            for (int i = 1; i <= ni; ++i) {
+                double sm[SCFD_MAX_SPECIES + 3];
+                for (int k = 1; k <= D; ++k) sm[k - 1] = rhs_k(c, k, i, j, p);
+                if (pc) {  // Dq = Dq_small + pre1 (pre2 . Dq_small) (time_precon_viscous.f90:24)
+                    double t = 0.0;
+                    for (int k = 1; k <= D; ++k) t = t + c.pre2(k, i, j, p) * sm[k - 1];
+                    for (int k = 1; k <= D; ++k) sm[k - 1] = sm[k - 1] + c.pre1(k, i, j, p) * t;
                 }
+                for (int k = 1; k <= D; ++k)
+                    Dq(k, i, j, p) = nr ? sm[k - 1] - c.Vol(i, j, p) * c.dqdt(k, i, j, p) : sm[k - 1];
+            }
         for (int j = 0; j <= nj; ++j)
             for (int k = 1; k <= D; ++k) Dq(k, 0, j, p) = 0.0;
         for (int i = 0; i <= ni; ++i)
@@ -1818,7 +1866,7 @@ int calc_next_step_implicit(orc_ctx& c, int step_internal) {
         return nr_apply(c, step_internal, res, omega);
     }
     lusgs_sweeps(c, res, omega);
-    if (c.d.scheme != SCFD_SCHEME_NR) return 0;
+    if (c.d.scheme != SCFD_SCHEME_NR && c.d.scheme != SCFD_SCHEME_PRECON) return 0;
     return nr_apply(c, step_internal, res, omega);
 }
 
@@ -1830,9 +1878,11 @@ void set_ABpm_scheme(orc_ctx& c) {
         set_ABpm(c);
 }
 
-// dual time (NR and the preconditioned dual) share the main loop of
-// NR/q2d/main.main.raw.f90 and dual/2d/main.main.raw.f90
-bool dual_time(const orc_ctx& c) { return c.d.scheme == SCFD_SCHEME_NR || c.d.scheme == SCFD_SCHEME_DUAL; }
+// dual time (NR, the preconditioned dual and precon) share the main loop of
+// NR/q2d/main.main.raw.f90, dual/2d/main.main.raw.f90 and precon/2d/main.main.raw.f90
+bool dual_time(const orc_ctx& c) {
+    return c.d.scheme == SCFD_SCHEME_NR || c.d.scheme == SCFD_SCHEME_DUAL || c.d.scheme == SCFD_SCHEME_PRECON;
+}
 
 void copy_arr(FArr& dst, const FArr& src) { dst.v = src.v; }
 
@@ -2118,13 +2168,17 @@ int orc_create(const scfd_desc* d, orc_ctx** out) {
     if (d->abi_version != SCFD_ABI_VERSION) return SCFD_E_ARG;
     if (d->nplane < 1 || d->nplane > SCFD_MAX_PLANES || d->ny < 1 || d->ny > SCFD_MAX_SPECIES) return SCFD_E_ARG;
     if (d->scheme != SCFD_SCHEME_EULER && d->scheme != SCFD_SCHEME_LUSGS && d->scheme != SCFD_SCHEME_NR &&
-        d->scheme != SCFD_SCHEME_DUAL)
+        d->scheme != SCFD_SCHEME_DUAL && d->scheme != SCFD_SCHEME_PRECON && d->scheme != SCFD_SCHEME_PRECON_LUSGS)
         return SCFD_E_UNSUPPORTED;
     if (d->scheme == SCFD_SCHEME_DUAL) {  // checkout_flow.py:159-168; no reacting variant of dual
         if (d->dim != SCFD_DIM_2D || d->dt_mode == SCFD_DT_LOCAL || d->thermo == SCFD_THERMO_CHEMKIN_REACTIVE)
             return SCFD_E_UNSUPPORTED;
         if (!(d->cfl_tau > 0.0)) return SCFD_E_ARG;
     }
+    // precon / preconLU-SGS: 2d only, local time step (checkout_flow.py:154-160,171-177)
+    if ((d->scheme == SCFD_SCHEME_PRECON || d->scheme == SCFD_SCHEME_PRECON_LUSGS) &&
+        (d->dim != SCFD_DIM_2D || d->dt_mode != SCFD_DT_LOCAL || d->thermo == SCFD_THERMO_CHEMKIN_REACTIVE))
+        return SCFD_E_UNSUPPORTED;
     auto* c = new orc_ctx();
     c->d = *d;
     c->np = d->nplane;
@@ -2174,8 +2228,9 @@ int orc_create(const scfd_desc* d, orc_ctx** out) {
     c->x.init({{0, NI + 1}, {0, NJ + 1}, {1, np}});
     c->r.init({{0, NI + 1}, {0, NJ + 1}, {1, np}});
     c->dt_mat.init({{1, NI}, {1, NJ}, {1, np}});
-    bool impl = d->scheme == SCFD_SCHEME_LUSGS || d->scheme == SCFD_SCHEME_NR || d->scheme == SCFD_SCHEME_DUAL;
-    if (d->scheme == SCFD_SCHEME_DUAL) {
+    bool impl = d->scheme == SCFD_SCHEME_LUSGS || d->scheme == SCFD_SCHEME_NR || d->scheme == SCFD_SCHEME_DUAL ||
+                d->scheme == SCFD_SCHEME_PRECON || d->scheme == SCFD_SCHEME_PRECON_LUSGS;
+    if (d->scheme == SCFD_SCHEME_DUAL || d->scheme == SCFD_SCHEME_PRECON || d->scheme == SCFD_SCHEME_PRECON_LUSGS) {
         c->pre1.init({{1, D}, {1, NI}, {1, NJ}, {1, np}});
         c->pre2.init({{1, D}, {1, NI}, {1, NJ}, {1, np}});
         c->pre_sca.init({{1, 4}, {1, NI}, {1, NJ}, {1, np}});

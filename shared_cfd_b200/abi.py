@@ -23,7 +23,7 @@ STATUS_NAMES = {
 
 DIM_2D, DIM_Q2D = 0, 1
 DT_GLOBAL, DT_LOCAL, DT_FIXED = 0, 1, 2
-SCHEME_EULER, SCHEME_LUSGS, SCHEME_NR, SCHEME_DUAL = 0, 2, 3, 5
+SCHEME_EULER, SCHEME_LUSGS, SCHEME_NR, SCHEME_PRECON, SCHEME_DUAL, SCHEME_PRECON_LUSGS = 0, 2, 3, 4, 5, 6
 RECON_UPWIND, RECON_MUSCL = 0, 1
 THERMO_IDEAL, THERMO_CHEMKIN_COLD, THERMO_CHEMKIN_REACTIVE = 0, 1, 2
 MU_REFERENCE, MU_SUTHERLAND = 0, 1

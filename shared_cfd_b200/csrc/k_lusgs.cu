@@ -144,6 +144,9 @@ __global__ void __launch_bounds__(128) k_sweep(View v, StripList sl, double* xfe
     const bool q2d = v.dim == SCFD_DIM_Q2D;
     const bool nr = dual_time_scheme(v.scheme);
     const bool dual = v.scheme == SCFD_SCHEME_DUAL;
+    // precon / preconLU-SGS: the split Jacobians are (I + phh p1 p2^T)(n1 A + n2 B)/2
+    // +/- nu/2 (sch_precon.raw.f90:148-186), the product of jac_out_dual with s2 = phh
+    const bool pc = precon_scheme(v.scheme);
     for (;;) {
         int sid = 0;
         if (lane == 0) sid = atomicAdd(ticket, 1);
@@ -260,6 +263,8 @@ __global__ void __launch_bounds__(128) k_sweep(View v, StripList sl, double* xfe
                 cj.dsa = RT(v.dsci[c]); cj.dsb = RT(v.dscj[c]);
                 if (dual)
                     jac_out_dual<RT, DMAX, DIR == 0>(nY, cj, s2, Y, DH, x, outA, outB);
+                else if (pc)
+                    jac_out_dual<RT, DMAX, DIR == 0>(nY, cj, RT(v.pre[c]), Y, DH, x, outA, outB);
                 else
                     jac_out<RT, DMAX, DIR == 0>(nY, cj, Y, DH, x, outA, outB);
                 if (DIR == 0 || nr || !lusgs_update) {
@@ -343,7 +348,7 @@ int launch_sweep(const View& v, cudaStream_t s, int dir, double* xfer, int* prog
     StripList f{(const int2*)strip_tab_f, nstrips_fwd}, b{(const int2*)strip_tab_b, nstrips_bwd};
     const bool mixed = v.precision == SCFD_PREC_MIXED;
     const int upd = dual_time_scheme(v.scheme) ? 0 : 1;
-    const bool dual = v.scheme == SCFD_SCHEME_DUAL;
+    const bool dual = v.scheme == SCFD_SCHEME_DUAL || precon_scheme(v.scheme);  // generic sweeps only
     if (!dual && dir == 0 && launch_sweep2(v, s, 0, f.strips, f.n, xfer, progress, tickets, partials, upd)) return 1;
     if (!dual && dir == 1 &&
         launch_sweep2(v, s, 1, b.strips, b.n, xfer, progress + nstrips_fwd, tickets + 1, partials, upd))

@@ -276,6 +276,61 @@ __global__ void __launch_bounds__(NT) k_residual(View v) {
     }
     const double vol = v.Vol[c];
     const bool first = v.sc->first_dual != 0;
+    if (MODE == RES_PRECON || MODE == RES_PRECON_LUSGS) {
+        // set_ABpm of time_scheme/precon/2d (sch_precon.raw.f90:28-77, 194-197):
+        // low-Mach reference velocity, preconditioned spectral radii, the local
+        // time step (written to dt_mat: set_dqdt and alpha use it), phh of
+        // pre1 = phh (Y, u, v, H); then Dq = R + pre1 (pre2 . R) [- Vol dqdt]
+        // (time_precon_viscous.f90:18-27)
+        const double rho = v.w[c], u = v.w[N + c], vv = v.w[2 * N + c], pr = v.w[3 * N + c];
+        const double gamm = v.w[(D + 1) * N + c], H = v.w[(D + 2) * N + c];
+        const double mu = v.w[(D + 4) * N + c], dsa = v.dsci[c], dsb = v.dscj[c];
+        const double cs = sqrt(gamm * pr / rho);
+        const double unA = v.vnci[c] * u + v.vnci[N + c] * vv;
+        const double unB = v.vncj[c] * u + v.vncj[N + c] * vv;
+        const double Vs = u * u + vv * vv;
+        const double Vv = mu / rho / fmin(dsa, dsb);
+        const double Ur = fmin(fmax(Vv, sqrt(Vs)), cs);
+        const double phi = 1.0 / (Ur * Ur) - 1.0 / (cs * cs);
+        const double alp = 0.5 * (1.0 - (Ur / cs) * (Ur / cs));
+        double ud = unA * (1.0 - alp), cd = sqrt(alp * alp * (unA * unA) + Ur * Ur);
+        const double nuA = fabs(ud) + cd;
+        ud = unB * (1.0 - alp);
+        cd = sqrt(alp * alp * (unB * unB) + Ur * Ur);
+        const double nuB = fabs(ud) + cd;
+        const long long cim = cidx(v.P, p, i - 1, j), cjm = cidx(v.P, p, i, j - 1);
+        const double uds = nuA * (v.dsi[c] + v.dsi[cim]) + nuB * (v.dsj[c] + v.dsj[cjm]);
+        const double dt = v.cfl * vol / fmax(uds, mu / rho);
+        v.dt_mat[c] = dt;
+        const double phh = -1.0 / (cs * cs + 1.0 / phi);
+        const double tmp = MODE == RES_PRECON ? 3.0 * vol / (2.0 * dt) + dsa * nuA + dsb * nuB
+                                              : vol / dt + dsa * nuA + dsb * nuB;
+        v.alpha[c] = 1.0 / tmp;
+        v.nuA[c] = nuA;
+        v.nuB[c] = nuB;
+        v.pre[c] = phh;
+        const double g1 = gamm - 1.0;
+        double R[kMaxSpecies + 3];
+        double t = 0.0;
+        for (int k = 0; k < D; ++k) {
+            const double src = k == nY + 1 ? area * (sq_my + svq_my) : area * 0.0;
+            R[k] = (double)fim[k] - (double)fip[k] + (double)fjm[k] - (double)fjp[k] + src;
+            const double p2 = k < nY ? 0.5 * g1 * Vs + v.DHi[k * N + c]
+                                     : (k == nY ? -g1 * u : (k == nY + 1 ? -g1 * vv : g1));
+            t = t + p2 * R[k];
+        }
+        for (int k = 0; k < D; ++k) {
+            const double p1 = k < nY ? phh * v.w[(4 + k) * N + c] : phh * (k == nY ? u : (k == nY + 1 ? vv : H));
+            double rhs = R[k] + p1 * t;
+            if (MODE == RES_PRECON) {
+                const double qk = v.q[k * N + c], qpk = v.qp[k * N + c];
+                const double dqdt = first ? (qk - qpk) / dt : (3.0 * qk - 4.0 * qpk + v.qpp[k * N + c]) / (2.0 * dt);
+                rhs = rhs - vol * dqdt;
+            }
+            v.Dq[k * N + c] = rhs;
+        }
+        return;
+    }
     for (int k = 0; k < D; ++k) {
         const double src = k == nY + 1 ? area * (sq_my + svq_my) : area * 0.0;
         double rhs = (double)fim[k] - (double)fip[k] + (double)fjm[k] - (double)fjp[k] + src;
@@ -365,7 +420,9 @@ static void launch_t(const View& v, cudaStream_t s) {
 // need_coeffs: the caller's sweep reads alpha/nuA/nuB from the cell arrays,
 // which only this generic kernel writes.
 int launch_residual(const View& v, cudaStream_t s, int mode, bool need_coeffs) {
-    if (mode != RES_DUAL && !need_coeffs && launch_residual2(v, s, mode)) return 1;
+    if (mode != RES_DUAL && mode != RES_PRECON && mode != RES_PRECON_LUSGS && !need_coeffs &&
+        launch_residual2(v, s, mode))
+        return 1;
     const bool mixed = v.precision == SCFD_PREC_MIXED;
     if (mode == RES_EULER) {
         if (mixed) launch_t<float, RES_EULER>(v, s); else launch_t<double, RES_EULER>(v, s);
@@ -373,6 +430,10 @@ int launch_residual(const View& v, cudaStream_t s, int mode, bool need_coeffs) {
         if (mixed) launch_t<float, RES_LUSGS>(v, s); else launch_t<double, RES_LUSGS>(v, s);
     } else if (mode == RES_DUAL) {
         if (mixed) launch_t<float, RES_DUAL>(v, s); else launch_t<double, RES_DUAL>(v, s);
+    } else if (mode == RES_PRECON) {
+        if (mixed) launch_t<float, RES_PRECON>(v, s); else launch_t<double, RES_PRECON>(v, s);
+    } else if (mode == RES_PRECON_LUSGS) {
+        if (mixed) launch_t<float, RES_PRECON_LUSGS>(v, s); else launch_t<double, RES_PRECON_LUSGS>(v, s);
     } else {
         if (mixed) launch_t<float, RES_NR>(v, s); else launch_t<double, RES_NR>(v, s);
     }

@@ -443,6 +443,8 @@ struct Seq {
     }
     void residual(int mode) {
         if (mode == RES_NR && c->d.scheme == SCFD_SCHEME_DUAL) mode = RES_DUAL;
+        if (mode == RES_NR && c->d.scheme == SCFD_SCHEME_PRECON) mode = RES_PRECON;
+        if (mode == RES_LUSGS && c->d.scheme == SCFD_SCHEME_PRECON_LUSGS) mode = RES_PRECON_LUSGS;
         const bool coeffs = mode != RES_EULER && !c->use_sw3 && !c->use_sw4;
         n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, mode, coeffs); });
     }
@@ -572,7 +574,11 @@ int scfd_create(const scfd_desc* d, scfd_ctx** out) {
     if (d->abi_version != SCFD_ABI_VERSION) return SCFD_E_ARG;
     if (d->nplane < 1 || d->nplane > SCFD_MAX_PLANES || d->ny < 1 || d->ny > SCFD_MAX_SPECIES) return SCFD_E_ARG;
     if (d->scheme != SCFD_SCHEME_EULER && d->scheme != SCFD_SCHEME_LUSGS && d->scheme != SCFD_SCHEME_NR &&
-        d->scheme != SCFD_SCHEME_DUAL)
+        d->scheme != SCFD_SCHEME_DUAL && !precon_scheme(d->scheme))
+        return SCFD_E_UNSUPPORTED;
+    // precon / preconLU-SGS: 2d only, local time step (checkout_flow.py:154-160,171-177)
+    if (precon_scheme(d->scheme) &&
+        (d->dim != SCFD_DIM_2D || d->dt_mode != SCFD_DT_LOCAL || d->thermo == SCFD_THERMO_CHEMKIN_REACTIVE))
         return SCFD_E_UNSUPPORTED;
     if (d->scheme == SCFD_SCHEME_DUAL) {  // checkout_flow.py:159-168; no reacting variant of dual
         if (d->dim != SCFD_DIM_2D || d->dt_mode == SCFD_DT_LOCAL || d->thermo == SCFD_THERMO_CHEMKIN_REACTIVE)
@@ -768,7 +774,8 @@ int scfd_commit(scfd_ctx* c) {
     const ChemTables tabs = c->have_chem ? ChemTables(c->chem) : ChemTables();
     const int nrec = 64 * c->np;
     // strip records for the TMA-streamed sweeps
-    const bool dual = c->d.scheme == SCFD_SCHEME_DUAL;
+    // the dual and precon schemes take the generic residual and sweeps
+    const bool dual = c->d.scheme == SCFD_SCHEME_DUAL || precon_scheme(c->d.scheme);
     const size_t blk3 = impl && !dual ? sweep3_record_elems(nY, mixed) : 0;
     const size_t esz3 = mixed ? sizeof(float) : sizeof(double);
     const char* sweep_env = std::getenv("SCFD_SWEEP");
@@ -1151,7 +1158,8 @@ static int autotune(scfd_ctx* c) {
     std::string rep = "{\"enabled\": true";
     // residual: the fused kernel of the strip-record path (not the generic one)
     const int mode = c->d.scheme == SCFD_SCHEME_EULER ? RES_EULER : c->d.scheme == SCFD_SCHEME_LUSGS ? RES_LUSGS : RES_NR;
-    const bool fused = c->d.scheme != SCFD_SCHEME_DUAL && (mode == RES_EULER || c->use_sw3 || c->use_sw4) &&
+    const bool fused = c->d.scheme != SCFD_SCHEME_DUAL && !precon_scheme(c->d.scheme) &&
+                       (mode == RES_EULER || c->use_sw3 || c->use_sw4) &&
                        (c->nY == 1 || c->nY == 8 || c->nY == 9) && c->P.nact > 0;
     const char* force = std::getenv("SCFD_RES_TILE");  // pins the tile (index), e.g. for profiling
     int tx[8], ty[8];

@@ -206,12 +206,18 @@ int launch_adj_objective(const View& v, cudaStream_t s, const long long* cells, 
                          double* lam, int grad_only);
 
 // residual modes (RES_DUAL: NR's right-hand side multiplied by Gamma^-1 and the
-// coefficients of the preconditioned dual time)
-enum { RES_EULER = 0, RES_LUSGS = 1, RES_NR = 2, RES_DUAL = 3 };
+// coefficients of the preconditioned dual time; RES_PRECON / RES_PRECON_LUSGS:
+// the preconditioned local time step, spectral radii and alpha of the precon
+// schemes and their right-hand side multiplied by I + phh p1 p2^T)
+enum { RES_EULER = 0, RES_LUSGS = 1, RES_NR = 2, RES_DUAL = 3, RES_PRECON = 4, RES_PRECON_LUSGS = 5 };
 
-// NR and the preconditioned dual time share the dual-time main loop
+// NR, the preconditioned dual time and precon share the dual-time main loop
 __host__ __device__ inline bool dual_time_scheme(int scheme) {
-    return scheme == SCFD_SCHEME_NR || scheme == SCFD_SCHEME_DUAL;
+    return scheme == SCFD_SCHEME_NR || scheme == SCFD_SCHEME_DUAL || scheme == SCFD_SCHEME_PRECON;
+}
+// the two schemes of time_scheme/precon and time_scheme/preconLU-SGS
+__host__ __device__ inline bool precon_scheme(int scheme) {
+    return scheme == SCFD_SCHEME_PRECON || scheme == SCFD_SCHEME_PRECON_LUSGS;
 }
 
 }  // namespace scfd
