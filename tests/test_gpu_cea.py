@@ -183,9 +183,10 @@ def compare_hptp(a, b, keys):
     assert np.all(np.abs(a["vhi"] - b["vhi"]) <= tol * vs)
 
 
-@pytest.mark.parametrize("species", [None, ["H2", "O2", "H2O", "H", "O", "OH", "HO2", "N2"]])
+@pytest.mark.parametrize("species", [None, ["H2", "O2", "H2O", "H", "O", "OH", "HO2", "N2"], "hon17"])
 def test_hp_and_tp_match_restatement(gpu, orc, species):
-    d = cea.h2_air_data(species=species)
+    # the exact 9-species, the 12-species and the generic 32-species kernels
+    d = cea.hon17_data() if species == "hon17" else cea.h2_air_data(species=species)
     with cea.Cea(d, lib=gpu) as g, cea.Cea(d, lib=orc) as o:
         inf = o.info()
         rho, Y, e, T = cea.random_states(inf, 2048, seed=17)

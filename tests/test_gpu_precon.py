@@ -41,3 +41,23 @@ def test_precon_mixed_precision_is_close(gpu, orc):
     case.desc.precision = abi.PREC_MIXED
     a = run_case(case, gpu, 3)
     assert rel_l2(case, a["q"], b["q"]) <= 1e-4
+
+
+@pytest.mark.parametrize("scheme", [abi.SCHEME_PRECON, abi.SCHEME_PRECON_LUSGS])
+def test_precon_sharded_equals_unsharded_gpu(gpu, scheme):
+    from shared_cfd_b200.sharded import ShardedSolver, lockstep
+    case = precon_case(scheme, orientation=1, inner=6)
+    ref = run_case(case, gpu, 3)
+    ranks = [ShardedSolver(case, [0, 1], lib=gpu, rank=r, nranks=2) for r in range(2)]
+    try:
+        for s in ranks:
+            s.upload()
+            s.prepare(1)
+        for n in range(3):
+            lockstep(ranks, n + 1)
+        for r, s in enumerate(ranks):
+            q = s.download()[0]
+            assert np.array_equal(case.interior(q, r), case.interior(ref["q"], r))
+    finally:
+        for s in ranks:
+            s.close()

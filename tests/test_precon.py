@@ -81,3 +81,26 @@ def test_unsupported_combinations_are_refused(orc, lib_name):
                 case.desc.dim = abi.DIM_Q2D
             ctx = C.c_void_p()
             assert lib.create(C.byref(case.desc), C.byref(ctx)) == abi.E_UNSUPPORTED, (scheme, change)
+
+
+@pytest.mark.parametrize("scheme", [abi.SCHEME_PRECON, abi.SCHEME_PRECON_LUSGS])
+def test_precon_sharded_equals_unsharded(orc, scheme):
+    """Block sharding (scfd_dstep on two in-process ranks): the preconditioned
+    local dt, alpha and right-hand side are per cell, so each rank's planes get
+    the unsharded bits."""
+    from shared_cfd_b200.sharded import ShardedSolver, lockstep
+    case = precon_case(scheme, orientation=1, inner=6)
+    ref = run_case(case, orc, 3)
+    ranks = [ShardedSolver(case, [0, 1], lib=orc, rank=r, nranks=2) for r in range(2)]
+    try:
+        for s in ranks:
+            s.upload()
+            s.prepare(1)
+        for n in range(3):
+            lockstep(ranks, n + 1)
+        for r, s in enumerate(ranks):
+            q = s.download()[0]
+            assert np.array_equal(case.interior(q, r), case.interior(ref["q"], r))
+    finally:
+        for s in ranks:
+            s.close()
