@@ -178,10 +178,19 @@ __global__ void __launch_bounds__(1024) k_pack(View v, const int2* blk, const in
     T* out = rec + rec_off[b.x] + (long long)b.y * L::STEP;
     const int nt = min(32, ni + 31 - b.y);
     using V = typename Vec16<T>::type;
+    // the next group's fields are loaded before this group's barrier and
+    // transpose, so that their global loads overlap it
+    T cur[G], nxt[G];
+#pragma unroll
+    for (int e = 0; e < G; ++e) cur[e] = T(field(e));
 #pragma unroll
     for (int g = 0; g < NG; ++g) {
+        if (g + 1 < NG) {
 #pragma unroll
-        for (int e = 0; e < G; ++e) tile[e][l][tt] = T(field(g * G + e));
+            for (int e = 0; e < G; ++e) nxt[e] = T(field((g + 1) * G + e));
+        }
+#pragma unroll
+        for (int e = 0; e < G; ++e) tile[e][l][tt] = cur[e];
         __syncthreads();
         const int wl = threadIdx.x, wt = threadIdx.y;
         if (wt < nt) {
@@ -191,6 +200,8 @@ __global__ void __launch_bounds__(1024) k_pack(View v, const int2* blk, const in
             *reinterpret_cast<V*>(out + ((long long)wt * NG + g) * 32 * G + wl * G) = *reinterpret_cast<V*>(vals);
         }
         __syncthreads();
+#pragma unroll
+        for (int e = 0; e < G; ++e) cur[e] = nxt[e];
     }
 }
 
