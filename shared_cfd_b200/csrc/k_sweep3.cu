@@ -485,20 +485,26 @@ __global__ void __launch_bounds__(1024) k_unpack(View v, const int2* blk, const 
     const T* in = rec + rec_off[b.x] + (long long)b.y * L::STEP;
     const int nt = min(32, ni + 31 - b.y);
     const long long N = v.ncell;
+    // read (step y, lane x) coalesced, write cells (step x, lane y); component
+    // k+1's record value and the cell's q are loaded before component k's
+    // barriers, so that the loads overlap them
+    const bool rd = (int)threadIdx.y < nt;
+    const long long rbase = (long long)threadIdx.y * NG * 32 * G + threadIdx.x * G;
+    const int tt = threadIdx.x, l = threadIdx.y;
+    const int t = b.y + tt, cc = t - l, j = 32 * s + 1 + l;
+    const bool wr = tt < nt && cc >= 0 && cc < ni && j <= nj;
+    const long long c = wr ? cidx(v.P, p, cc + 1, j) : 0;
+    double nxt = rd ? double(in[rbase]) : 0.0;
+    double qn = wr ? v.q[c] : 0.0;
     for (int k = 0; k < D; ++k) {
-        // read (step y, lane x) coalesced, write cells (step x, lane y)
-        if ((int)threadIdx.y < nt)
-            tile[threadIdx.y][threadIdx.x] = double(in[((long long)threadIdx.y * NG + k / G) * 32 * G + threadIdx.x * G + k % G]);
-        __syncthreads();
-        const int tt = threadIdx.x, l = threadIdx.y;
-        const int t = b.y + tt, cc = t - l, j = 32 * s + 1 + l;
-        if (tt < nt && cc >= 0 && cc < ni && j <= nj) {
-            const long long c = cidx(v.P, p, cc + 1, j);
-            if (nr_mode)
-                v.q[k * N + c] = v.q[k * N + c] + om * tile[tt][l];
-            else
-                v.q[k * N + c] = v.q[k * N + c] + tile[tt][l];
+        const double cur = nxt, qk = qn;
+        if (k + 1 < D) {
+            nxt = rd ? double(in[rbase + (long long)((k + 1) / G) * 32 * G + (k + 1) % G]) : 0.0;
+            qn = wr ? v.q[(k + 1) * N + c] : 0.0;
         }
+        if (rd) tile[threadIdx.y][threadIdx.x] = cur;
+        __syncthreads();
+        if (wr) v.q[k * N + c] = nr_mode ? qk + om * tile[tt][l] : qk + tile[tt][l];
         __syncthreads();
     }
 }
