@@ -178,16 +178,19 @@ __global__ void __launch_bounds__(1024) k_pack(View v, const int2* blk, const in
     T* out = rec + rec_off[b.x] + (long long)b.y * L::STEP;
     const int nt = min(32, ni + 31 - b.y);
     using V = typename Vec16<T>::type;
-    // the next group's fields are loaded before this group's barrier and
-    // transpose, so that their global loads overlap it
-    T cur[G], nxt[G];
+    // the fields of the next two groups are loaded before this group's barrier
+    // and transpose, so that their global loads overlap it
+    T cur[G], nxt[G], nx2[G];
 #pragma unroll
-    for (int e = 0; e < G; ++e) cur[e] = T(field(e));
+    for (int e = 0; e < G; ++e) {
+        cur[e] = T(field(e));
+        nxt[e] = NG > 1 ? T(field(G + e)) : T(0);
+    }
 #pragma unroll
     for (int g = 0; g < NG; ++g) {
-        if (g + 1 < NG) {
+        if (g + 2 < NG) {
 #pragma unroll
-            for (int e = 0; e < G; ++e) nxt[e] = T(field((g + 1) * G + e));
+            for (int e = 0; e < G; ++e) nx2[e] = T(field((g + 2) * G + e));
         }
 #pragma unroll
         for (int e = 0; e < G; ++e) tile[e][l][tt] = cur[e];
@@ -201,7 +204,10 @@ __global__ void __launch_bounds__(1024) k_pack(View v, const int2* blk, const in
         }
         __syncthreads();
 #pragma unroll
-        for (int e = 0; e < G; ++e) cur[e] = nxt[e];
+        for (int e = 0; e < G; ++e) {
+            cur[e] = nxt[e];
+            nxt[e] = nx2[e];
+        }
     }
 }
 
