@@ -12,7 +12,9 @@
 // until the element balance, the energy and the largest |dln n_j| n_j agree to
 // 1e-9 (500 iterations at most).  The equilibrium state then gives the mixture
 // weight, gamma = cp/(cp - R), the species enthalpies vhi, the DHi terms and
-// the Wilke-mixed viscosity.
+// the Wilke-mixed viscosity.  k_cea_hptp restates cea_hp and cea_tp
+// (sub_chem.f90:1652-2248) the same way, with ln sum(n) (and for hp ln T) among
+// the unknowns.
 //
 // Layout: one thread per cell; the species vectors are register arrays of a
 // compile-time length (exactly 9 species / 3 elements for the hydrogen-air
