@@ -505,16 +505,17 @@ int  scfd_cea_status(scfd_cea* cea, int64_t* counts);
  * for callers that cannot call cudaMalloc, e.g. a solver whose device arrays
  * come from its own OpenACC / CUDA Fortran data regions or memory pool).
  * d_q and d_qp are DEVICE arrays in the layout of scfd_upload,
- * q(1:dimq,-1:nimax+2,-1:njmax+2,Nplane); *d_rms (device) receives
- * sqrt(sum (q(E)-qp(E))^2) / ncells over the interior cells
- * (store/core/check_convergence.f90:17-28).  Enqueued on `stream` (a
- * cudaStream_t, or NULL); the caller synchronises.  No context is needed.
- * Scratch is a static device array of SCFD_NOALLOC_MAX_BLOCKS doubles that
- * every GPU loading the library keeps until exit; its address is looked up on
- * the first call on each device, so make that first call before any stream
- * capture.  Calls that overlap on the GPU share the scratch and race.
- * Returns SCFD_E_ARG for a bad descriptor or more planes than the scratch
- * holds. */
+ * q(1:dimq,-1:nimax+2,-1:njmax+2,Nplane); *d_rms (device) receives the square
+ * root of the sum, over the interior cells, of the squared change of the
+ * energy component between qp and q, divided by the number of interior cells.
+ * Enqueued on `stream` (a cudaStream_t, or NULL); the caller synchronises.  No
+ * context is needed.  Scratch is a static device array of
+ * SCFD_NOALLOC_MAX_BLOCKS doubles that every GPU loading the library keeps
+ * until exit; its address is looked up on the first call on each device, so
+ * make that first call before any stream capture, and do not reset the device
+ * (cudaDeviceReset) between calls.  Calls that overlap on the GPU share the
+ * scratch and race.  Returns SCFD_E_ARG for a bad descriptor or more than
+ * SCFD_MAX_PLANES planes. */
 int  scfd_rms_noalloc(const scfd_desc* desc, const double* d_q, const double* d_qp, double* d_rms,
                       void* stream);
 

@@ -120,7 +120,7 @@ int launch_rms(const View& v, cudaStream_t s, double* partial, double* out) {
         ++n;
     }
     double cells = 0.0;
-    for (int p = 0; p < v.P.np; ++p) cells = cells + (double)(v.P.ni[p] * v.P.nj[p]);
+    for (int p = 0; p < v.P.np; ++p) cells = cells + (double)v.P.ni[p] * v.P.nj[p];
     k_rms_final<<<1, 1, 0, s>>>(partial, gx * v.P.nact, cells, out);
     return n + 1;
 }

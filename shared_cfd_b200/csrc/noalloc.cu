@@ -13,8 +13,11 @@
 // the symbol is only a host-side stand-in, so its device address is looked up
 // with cudaGetSymbolAddress once per device, on the first call made while that
 // device is current; that first call should therefore come before any stream
-// capture.  All calls share the array: calls that overlap on the GPU (from
-// different streams or threads) race.  Every partial used by a call is written
+// capture.  The cached address belongs to the device's primary context: after
+// cudaDeviceReset (or anything else that destroys that context) the module is
+// loaded again at a new address, so do not reset a device between calls.  All
+// calls share the array: calls that overlap on the GPU (from different streams
+// or threads) race.  Every partial used by a call is written
 // by that call before it is read, so nothing has to be cleared.
 #include <cuda_runtime.h>
 
@@ -29,6 +32,8 @@ static __device__ __align__(256) double g_rms_partials[SCFD_NOALLOC_MAX_BLOCKS];
 namespace {
 
 constexpr int kBlocksPerPlane = SCFD_NOALLOC_MAX_BLOCKS / SCFD_MAX_PLANES;  // 64
+static_assert(SCFD_MAX_PLANES * kBlocksPerPlane <= SCFD_NOALLOC_MAX_BLOCKS,
+              "the scratch must hold the partial sums of every plane");
 
 struct RefLayout {
     int np, dimq, ix, jx;  // ix = nimax+4, jx = njmax+4
@@ -95,7 +100,7 @@ extern "C" int scfd_rms_noalloc(const scfd_desc* d, const double* d_q, const dou
     if (!d || !d_q || !d_qp || !d_rms) return SCFD_E_ARG;
     if (d->abi_version != SCFD_ABI_VERSION || d->ny < 1 || d->ny > SCFD_MAX_SPECIES) return SCFD_E_ARG;
     // the scratch holds kBlocksPerPlane partial sums for at most SCFD_MAX_PLANES planes
-    if (d->nplane < 1 || d->nplane * kBlocksPerPlane > SCFD_NOALLOC_MAX_BLOCKS) return SCFD_E_ARG;
+    if (d->nplane < 1 || d->nplane > SCFD_MAX_PLANES) return SCFD_E_ARG;
     RefLayout L{};
     L.np = d->nplane;
     L.dimq = d->ny + 3;
@@ -107,7 +112,7 @@ extern "C" int scfd_rms_noalloc(const scfd_desc* d, const double* d_q, const dou
         L.nj[p] = d->nj[p];
         nimax = d->ni[p] > nimax ? d->ni[p] : nimax;
         njmax = d->nj[p] > njmax ? d->nj[p] : njmax;
-        cells = cells + (double)(d->ni[p] * d->nj[p]);
+        cells = cells + (double)d->ni[p] * d->nj[p];
     }
     L.ix = nimax + 4;
     L.jx = njmax + 4;

@@ -51,11 +51,9 @@ struct scfd_ctx {
     int nops = 0;
     double* d_bcval = nullptr;
     int valstride = SCFD_BC_MAXVAL + 2;
-    // strip-record sweeps: one lane per cell (sw3) or a quad per cell (sw4)
+    // strip-record sweeps (k_sweep3.cu)
     bool use_sw3 = false;
     Sweep3 sw3{};
-    bool use_sw4 = false;
-    Sweep4 sw4{};
     // chemistry
     unsigned long long* d_counter = nullptr;
     // rms
@@ -445,18 +443,10 @@ struct Seq {
         if (mode == RES_NR && c->d.scheme == SCFD_SCHEME_DUAL) mode = RES_DUAL;
         if (mode == RES_NR && c->d.scheme == SCFD_SCHEME_PRECON) mode = RES_PRECON;
         if (mode == RES_LUSGS && c->d.scheme == SCFD_SCHEME_PRECON_LUSGS) mode = RES_PRECON_LUSGS;
-        const bool coeffs = mode != RES_EULER && !c->use_sw3 && !c->use_sw4;
+        const bool coeffs = mode != RES_EULER && !c->use_sw3;
         n += timed(c, SCFD_K_RESIDUAL, [&] { return launch_residual(v, s, mode, coeffs); });
     }
     void sweeps() {
-        if (c->use_sw4) {
-            const Sweep4& w4 = c->sw4;
-            cudaMemsetAsync(w4.progress, 0, sizeof(int) * (2 * w4.ntasks + 2), s);
-            n += timed(c, SCFD_K_PACK, [&] { return launch_sweep4(v, s, w4, 0, 0); });
-            n += timed(c, SCFD_K_SWEEP_FWD, [&] { return launch_sweep4(v, s, w4, 1, 0); });
-            n += timed(c, SCFD_K_SWEEP_BWD, [&] { return launch_sweep4(v, s, w4, 2, 0); });
-            return;
-        }
         if (c->nsf == 0) return;  // a rank without planes
         launch_sweep_reset(s, c->d_progress, c->d_tickets, c->nsf, c->nsb);
         if (c->use_sw3) {
@@ -475,17 +465,12 @@ struct Seq {
         });
     }
     // the per-strip (res, omega) partials of the last backward sweep
-    const double* partials() const { return c->use_sw4 ? c->sw4.partials : c->use_sw3 ? c->sw3.partials : c->d_partials; }
-    int nstrips() const { return c->use_sw4 ? c->sw4.nstrips : c->use_sw3 ? c->sw3.nstrips : c->nsb; }
+    const double* partials() const { return c->use_sw3 ? c->sw3.partials : c->d_partials; }
+    int nstrips() const { return c->use_sw3 ? c->sw3.nstrips : c->nsb; }
     // q update after the sweeps: NR relaxes with the omega reduced from
     // `part` (nparts strip partials); LU-SGS (inner = 1) adds Dq
     void update(int inner, const double* part, int nparts) {
-        if (c->use_sw4) {
-            Sweep4 w4 = c->sw4;
-            w4.partials = const_cast<double*>(part);
-            w4.nstrips = nparts;
-            n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep4(v, s, w4, 3, inner); });
-        } else if (c->use_sw3) {
+        if (c->use_sw3) {
             if (c->nsf == 0) return;
             Sweep3 w3 = c->sw3;
             w3.partials = const_cast<double*>(part);
@@ -778,39 +763,10 @@ int scfd_commit(scfd_ctx* c) {
     const bool dual = c->d.scheme == SCFD_SCHEME_DUAL || precon_scheme(c->d.scheme);
     const size_t blk3 = impl && !dual ? sweep3_record_elems(nY, mixed) : 0;
     const size_t esz3 = mixed ? sizeof(float) : sizeof(double);
-    const char* sweep_env = std::getenv("SCFD_SWEEP");
     const bool legacy = std::getenv("SCFD_SWEEP_LEGACY") != nullptr;
     const char* graph_env = std::getenv("SCFD_GRAPH");
     c->use_graph = !(graph_env && std::strcmp(graph_env, "0") == 0);
-    int qc4 = 0;
-    const size_t blk4 = impl && !dual ? sweep4_record_elems(nY, mixed, &qc4) : 0;
-    c->use_sw4 = blk4 > 0 && !legacy && sweep_env && std::strcmp(sweep_env, "4") == 0 && c->owner.empty();
-    c->use_sw3 = blk3 > 0 && !legacy && !c->use_sw4;
-    // quad-per-cell sweeps: strips of R rows, tasks of up to WPC strips
-    std::vector<long long> rec_off4;
-    std::vector<int> strips4, blks4, tasksf4, tasksb4;
-    long long rec_total4 = 0;
-    int ntasks4 = 0;
-    if (c->use_sw4) {
-        const int R = sweep4_rows(), WPC = sweep4_strips_per_task(mixed), pad = sweep4_pad_steps();
-        const int SB = sweep4_steps_per_block();
-        int fs = 0;
-        for (int pl = 0; pl < c->np; ++pl) {
-            const int ns = (c->P.nj[pl] + R - 1) / R, steps = c->P.ni[pl] + R - 1;
-            const int fs_plane = fs;
-            for (int st4 = 0; st4 < ns; ++st4, ++fs) {
-                rec_off4.push_back(rec_total4 + (long long)pad * blk4);
-                rec_total4 += (long long)(steps + 2 * pad) * blk4;
-                strips4.insert(strips4.end(), {pl, st4, 0, 0});
-                for (int t0 = 0; t0 < steps; t0 += SB) blks4.insert(blks4.end(), {fs, t0});
-            }
-            std::vector<int> tk;
-            for (int g0 = 0; g0 < ns; g0 += WPC) tk.insert(tk.end(), {pl, g0, std::min(WPC, ns - g0), fs_plane + g0});
-            tasksf4.insert(tasksf4.end(), tk.begin(), tk.end());
-            for (int k = (int)tk.size() / 4 - 1; k >= 0; --k) tasksb4.insert(tasksb4.end(), tk.begin() + 4 * k, tk.begin() + 4 * k + 4);
-        }
-        ntasks4 = (int)tasksf4.size() / 4;
-    }
+    c->use_sw3 = blk3 > 0 && !legacy;
     std::vector<long long> rec_off;
     std::vector<int> blks3, tabf3, tabb3;
     long long rec_total = 0;
@@ -858,11 +814,6 @@ int scfd_commit(scfd_ctx* c) {
     bytes += tabs.bytes();
     const size_t nref = (size_t)(c->nimax + 4) * (c->njmax + 4) * c->np;
     bytes += need<double>((size_t)std::max(std::max(W, D), nY) * nref);
-    if (c->use_sw4)
-        bytes += need<char>(rec_total4 * esz3) + need<long long>(rec_off4.size()) + need<int>(strips4.size()) +
-                 need<int>(blks4.size()) + 2 * need<int>(tasksf4.size()) +
-                 need<char>((size_t)ntasks4 * (c->nimax + 8) * qc4 * esz3) + need<int>(2 * ntasks4 + 2) +
-                 need<double>(2 * strips4.size() / 4);
     if (c->use_sw3)
         bytes += need<char>(rec_total * esz3) + need<long long>(rec_off.size()) + need<int>(blks3.size()) +
                  need<int>(tabf3.size()) + need<int>(tabb3.size());
@@ -942,34 +893,6 @@ int scfd_commit(scfd_ctx* c) {
         w3.progress = c->d_progress;
         w3.tickets = c->d_tickets;
         w3.partials = c->d_partials;
-        CK(cudaStreamSynchronize(c->stream));
-    }
-    if (c->use_sw4) {
-        Sweep4& w4 = c->sw4;
-        w4.rec = carve<char>(p, rec_total4 * esz3);
-        long long* ro = carve<long long>(p, rec_off4.size());
-        int* sp = carve<int>(p, strips4.size());
-        int* bk = carve<int>(p, blks4.size());
-        int* tf = carve<int>(p, tasksf4.size());
-        int* tb = carve<int>(p, tasksb4.size());
-        w4.xfer = carve<char>(p, (size_t)ntasks4 * (c->nimax + 8) * qc4 * esz3);
-        w4.progress = carve<int>(p, 2 * ntasks4 + 2);
-        w4.tickets = w4.progress + 2 * ntasks4;
-        w4.partials = carve<double>(p, 2 * strips4.size() / 4);
-        CK(cudaMemcpyAsync(ro, rec_off4.data(), rec_off4.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(sp, strips4.data(), strips4.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(bk, blks4.data(), blks4.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(tf, tasksf4.data(), tasksf4.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(tb, tasksb4.data(), tasksb4.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        w4.rec_off = ro;
-        w4.strips = reinterpret_cast<const int4*>(sp);
-        w4.nstrips = (int)strips4.size() / 4;
-        w4.blk = reinterpret_cast<const int2*>(bk);
-        w4.nblk = (int)blks4.size() / 2;
-        w4.tasks_f = reinterpret_cast<const int4*>(tf);
-        w4.tasks_b = reinterpret_cast<const int4*>(tb);
-        w4.ntasks = ntasks4;
-        w4.xstride = (long long)(c->nimax + 8) * qc4;
         CK(cudaStreamSynchronize(c->stream));
     }
     if (p > c->arena + c->arena_bytes) return c->fail(SCFD_E_CUDA, "arena overflow");
@@ -1159,7 +1082,7 @@ static int autotune(scfd_ctx* c) {
     // residual: the fused kernel of the strip-record path (not the generic one)
     const int mode = c->d.scheme == SCFD_SCHEME_EULER ? RES_EULER : c->d.scheme == SCFD_SCHEME_LUSGS ? RES_LUSGS : RES_NR;
     const bool fused = c->d.scheme != SCFD_SCHEME_DUAL && !precon_scheme(c->d.scheme) &&
-                       (mode == RES_EULER || c->use_sw3 || c->use_sw4) &&
+                       (mode == RES_EULER || c->use_sw3) &&
                        (c->nY == 1 || c->nY == 8 || c->nY == 9) && c->P.nact > 0;
     const char* force = std::getenv("SCFD_RES_TILE");  // pins the tile (index), e.g. for profiling
     int tx[8], ty[8];

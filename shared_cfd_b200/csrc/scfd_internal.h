@@ -147,29 +147,6 @@ struct Sweep3 {
 size_t sweep3_record_elems(int ny, bool mixed);  // elements per step block, 0 if none
 int sweep3_pad_steps();                          // zero step blocks before and after each strip
 int launch_sweep3(const View& v, cudaStream_t s, const Sweep3& w, int what, int inner);
-// Quad-per-cell LU-SGS with warp-to-warp hand-off (k_sweep4.cu), nY in {1, 8, 9}.
-struct Sweep4 {
-    void* rec;                 // strip records (float on the mixed path)
-    const long long* rec_off;  // per strip: element offset of step 0
-    const int4* strips;        // per strip (plane, strip index in plane, 0, 0)
-    int nstrips;
-    const int2* blk;           // pack/unpack blocks: (strip, first step)
-    int nblk;
-    const int4* tasks_f;       // forward tasks (plane, first strip, strips, index of the first strip)
-    const int4* tasks_b;       // backward order
-    int ntasks;
-    void* xfer;                // per task hand-off columns
-    long long xstride;         // elements per task
-    int* progress;             // 2*ntasks, followed by the 2 tickets
-    int* tickets;
-    double* partials;          // 2*nstrips
-};
-int sweep4_rows();
-int sweep4_strips_per_task(bool mixed);
-int sweep4_pad_steps();
-int sweep4_steps_per_block();
-size_t sweep4_record_elems(int ny, bool mixed, int* qc);  // elements per step block, 0 if none
-int launch_sweep4(const View& v, cudaStream_t s, const Sweep4& w, int what, int inner);
 int launch_nr_update(const View& v, cudaStream_t s, const double* partials, int nstrips, int inner);
 int launch_chem_impl(const View& v, cudaStream_t s, int max_substeps, unsigned long long* counter, int nsm);
 int launch_step_end(const View& v, cudaStream_t s, double warn, double err);

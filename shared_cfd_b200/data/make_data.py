@@ -117,4 +117,6 @@ def nasa_tables(ref, species, prefix):
         f.write("\n".join(out) + "\n")
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: %s" % "python shared_cfd_b200/data/make_data.py /path/to/shared_cfd")
+    main(sys.argv[1])

@@ -140,12 +140,32 @@ class ShardedSolver(Solver):
         """Kernels launched by the last run() (scfd_launch_count covers one step)."""
         return self._run_launches
 
-    def rms(self):
-        """The global RMS: the library returns this rank's share."""
+    def rms(self, combine="global"):
+        """The convergence RMS of the sharded case.
+
+        The library returns this rank's share sqrt(tmp_r) / N, with tmp_r the
+        rank's sum of squared energy changes and N the cells of the whole case.
+
+        combine="global" (default): sqrt(sum_r tmp_r) / N, the value of the same
+        case run unsharded on one GPU, independent of the rank count.
+
+        combine="reference": sum_r sqrt(tmp_r) / n_r with n_r the rank's own
+        cells, what check_convergence.f90:17-33 MPI_Reduce-sums over the
+        reference's ranks.  With R equal ranks it is R**1.5 times the global
+        value, so a min_RMS threshold taken from an R-rank run of the reference
+        corresponds to min_RMS / R**1.5 in the global form."""
         import torch
         import torch.distributed as dist
         local = Solver.rms(self)
         dev = "cuda" if self._device else "cpu"
+        if combine == "reference":
+            own = self.owned_cells
+            part = local * self.case.ncells / own if own else 0.0
+            t = torch.tensor([part], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, group=self.group)
+            return float(t.item())
+        if combine != "global":
+            raise ValueError("combine must be 'global' or 'reference'")
         t = torch.tensor([local * local], dtype=torch.float64, device=dev)
         dist.all_reduce(t, group=self.group)
         return float(np.sqrt(t.item()))

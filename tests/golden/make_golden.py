@@ -1,7 +1,7 @@
 """Generate the committed golden fixtures from a checkout of the reference
 (read-only).  Run from the repository root:
 
-    python tests/golden/make_golden.py [/path/to/shared_cfd]
+    python tests/golden/make_golden.py /path/to/shared_cfd
 
 forward_step_bd.npz / forward_step_expected.json
     Boundary node coordinates of the four forward-step samples
@@ -102,4 +102,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: %s" % "python tests/golden/make_golden.py /path/to/shared_cfd")
+    main(sys.argv[1])

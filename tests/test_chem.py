@@ -84,7 +84,8 @@ def test_no27_state_known_answer_oracle(orc_raw):
     assert (e.max(axis=1) < 1e-11).mean() > 0.65
 
 
-@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="reference checkout not present")
+@pytest.mark.skipif(not REFERENCE or not os.path.isdir(REFERENCE),
+                    reason="SCFD_REFERENCE does not name a reference checkout")
 def test_parser_reproduces_frozen_mechanism():
     core = os.path.join(REFERENCE, "store/therm_lib/chemkin/core")
     s27 = os.path.join(REFERENCE, "sample/no27.chemkin_reaction")

@@ -95,7 +95,8 @@ def test_restart_truncated_is_rejected(tmp_path):
         F.read_restart(str(tmp_path / "cut.bin"), 4, [(3, 2)])
 
 
-@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="reference checkout not present")
+@pytest.mark.skipif(not REFERENCE or not os.path.isdir(REFERENCE),
+                    reason="SCFD_REFERENCE does not name a reference checkout")
 def test_no27_restart_bin_bytes_round_trip():
     p = os.path.join(REFERENCE, "sample/no27.chemkin_reaction/restart.bin")
     step, tt, cells = F.read_restart(p, 11, [(223, 99)])

@@ -128,14 +128,13 @@ def test_launch_count_positive(gpu):
     s.close()
 
 
-SWEEP_ENV = {"lane": {}, "quad": {"SCFD_SWEEP": "4"}, "legacy": {"SCFD_SWEEP_LEGACY": "1"}}
+SWEEP_ENV = {"lane": {}, "legacy": {"SCFD_SWEEP_LEGACY": "1"}}
 
 
 @pytest.mark.parametrize("path", sorted(SWEEP_ENV))
 def test_sweep_paths_agree(gpu, orc, path, monkeypatch):
-    """All three sweep implementations match the restatement: lane-per-cell
-    strip records streamed by bulk copies (default), quad-per-cell strips with
-    warp-to-warp hand-off, and the generic per-lane gather."""
+    """Both sweep implementations match the restatement: strip records
+    streamed by bulk copies (default) and the generic per-lane gather."""
     for k, val in SWEEP_ENV[path].items():
         monkeypatch.setenv(k, val)
     case = cases.perturb(cases.forward_step(2, n=20, scheme=abi.SCHEME_LUSGS, dt_mode=abi.DT_LOCAL, viscous=1,
@@ -146,9 +145,9 @@ def test_sweep_paths_agree(gpu, orc, path, monkeypatch):
 
 @pytest.mark.parametrize("path", sorted(SWEEP_ENV))
 def test_sweep_many_tasks_ragged(gpu, orc, path, monkeypatch):
-    """One plane of 150 rows: 19 eight-row strips in three tasks (the last with
-    three strips, its last strip six rows high), so the hand-off crosses CTAs
-    through global memory as well as warps through shared memory."""
+    """One plane of 150 rows: several strips, the last of them ragged, so the
+    wavefront hands the top row of each strip to the next and ends in a
+    partial strip."""
     for k, val in SWEEP_ENV[path].items():
         monkeypatch.setenv(k, val)
     case = cases.perturb(cases.flat_plate(40, 150), seed=5)
@@ -157,7 +156,7 @@ def test_sweep_many_tasks_ragged(gpu, orc, path, monkeypatch):
 
 def test_reacting_step_two_tasks_per_plane(gpu, orc):
     """Reacting NR q2d step at a quarter of the resolution per direction:
-    128-row planes run as two tasks of eight strips."""
+    128- and 64-row planes, several strips per plane."""
     case = cases.reacting_step(scale=0.25, inner=3)
     _parity(case, gpu, orc, 1)
 

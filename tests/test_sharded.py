@@ -118,6 +118,19 @@ def test_sharded_rms_is_the_global_rms(orc):
         one.step(1)
         parts = [Solver.rms(s) for s in ranks]
         assert np.sqrt(sum(x * x for x in parts)) == pytest.approx(one.rms(), rel=1e-13)
+        # the reference's combination (check_convergence.f90:17-33): each rank's
+        # sqrt(sum) over its own cell count, summed over ranks
+        ncell = case.ncells
+        want = 0.0
+        for s, part in zip(ranks, parts):
+            want += part * ncell / s.owned_cells
+        q, _, _, _ = one.download()
+        qp = one.download_qp()
+        direct = 0.0
+        for p in range(len(case.planes)):
+            d = case.interior(q, p)[:, :, case.D - 1] - case.interior(qp, p)[:, :, case.D - 1]
+            direct += np.sqrt((d * d).sum()) / (case.ni[p] * case.nj[p])
+        assert want == pytest.approx(direct, rel=1e-12)
     finally:
         for s in ranks + [one]:
             s.close()

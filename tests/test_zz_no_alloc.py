@@ -55,6 +55,8 @@ def test_rms_noalloc_rejects_more_planes_than_its_scratch(gpu):
     d = abi.Desc()
     d.abi_version = abi.ABI_VERSION
     d.ny = 1
-    d.nplane = abi.MAX_PLANES + 1
     one = C.c_double()
-    assert f(C.byref(d), C.c_void_p(1), C.c_void_p(1), C.byref(one), None) == abi.E_ARG
+    # 0x04000001 * 64 wraps to 64 in 32-bit arithmetic: the check must not multiply
+    for n in (abi.MAX_PLANES + 1, 0x04000001, -1, 0):
+        d.nplane = n
+        assert f(C.byref(d), C.c_void_p(1), C.c_void_p(1), C.byref(one), None) == abi.E_ARG
