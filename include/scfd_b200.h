@@ -163,6 +163,9 @@ typedef struct scfd_chem {
     double  rtol, atol;                      /* control_chem.inp tolerances        */
 } scfd_chem;
 
+/* inner iterations recorded per step by scfd_inner_log */
+#define SCFD_INNER_LOG 128
+
 typedef struct scfd_stats {
     double  dt_grbl;               /* global dt of the step (global / fixed mode) */
     double  tt;                    /* accumulated physical time                   */
@@ -220,6 +223,15 @@ int  scfd_run(scfd_ctx* ctx, int step, int nsteps, scfd_stats* stats);
 /* RMS of check_convergence (store/core/check_convergence.f90:17-28):
  * sqrt(sum (q(E)-qp(E))^2) / ncells over all planes. */
 int  scfd_rms(scfd_ctx* ctx, double* rms);
+/* The inner-iteration record of the last NR / dual / precon step, as the
+ * reference writes internal_res.dat with "InternalLoop OutOmega"
+ * (store/time_scheme/NR/q2d/time_NR_viscous.f90:87-95): for inner iteration
+ * k = 1..n, omega[k-1] is the relaxation factor from the Dqrate limiter before
+ * the omega_max cap (1e300 when no species decreases) and res[k-1] the residual
+ * sum (res/res1 is the reference's third column).  Writes min(n, inner
+ * iterations of the step, SCFD_INNER_LOG) entries and returns that count (< 0:
+ * an SCFD_E_* code, negated).  Either pointer may be NULL. */
+int  scfd_inner_log(scfd_ctx* ctx, double* omega, double* res, int n);
 /* Copies the state back in the reference layout; any pointer may be NULL. */
 int  scfd_download(scfd_ctx* ctx, double* q, double* w, double* vhi, double* tt);
 /* Same as download but for qp (the previous step's q). */

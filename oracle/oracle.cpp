@@ -104,6 +104,9 @@ struct orc_ctx {
     FArr pre1, pre2, pre_sca, phi;  // store/time_scheme/dual/2d/var_dual.f90
     bool first_dual = true;
     double res1 = 0.0, res = 0.0, omega_last = 0.0;
+    // omega before the omega_max cap and res of every inner iteration of the
+    // last step (internal_res.dat, time_NR_viscous.f90:87-95)
+    double il_omega[SCFD_INNER_LOG] = {}, il_res[SCFD_INNER_LOG] = {};
     long long chem_attempts = 0, chem_fallback = 0;
     int status = SCFD_OK;
     // block sharding (scfd_set_partition): planes owned by this rank, the
@@ -1844,6 +1847,10 @@ void lusgs_sweeps(orc_ctx& c, double& res_out, double& omega_out) {
 // time_NR_viscous.f90:75-108.  omega is the smallest candidate (the running
 // minimum of the reference falls below omega_min exactly when it does).
 int nr_apply(orc_ctx& c, int step_internal, double res, double omega) {
+    if (step_internal >= 1 && step_internal <= SCFD_INNER_LOG) {
+        c.il_omega[step_internal - 1] = omega;
+        c.il_res[step_internal - 1] = res;
+    }
     if (omega < c.d.omega_min) return SCFD_E_OMEGA;
     if (step_internal == 1) c.res1 = res;
     c.res = res;
@@ -2364,6 +2371,19 @@ int orc_run(orc_ctx* c, int stepno, int nsteps, scfd_stats* st) {
         if (s) return s;
     }
     return 0;
+}
+
+int orc_inner_log(orc_ctx* c, double* omega, double* res, int n) {  // time_NR_viscous.f90:87-95
+    if (!c || !c->committed || n < 0) return -SCFD_E_ARG;
+    const bool dual_time = c->d.scheme == SCFD_SCHEME_NR || c->d.scheme == SCFD_SCHEME_DUAL ||
+                           c->d.scheme == SCFD_SCHEME_PRECON;
+    if (!dual_time) return 0;
+    const int m = std::min(std::min(n, std::max(0, c->d.num_internal_loop - 1)), SCFD_INNER_LOG);
+    for (int k = 0; k < m; ++k) {
+        if (omega) omega[k] = c->il_omega[k];
+        if (res) res[k] = c->il_res[k];
+    }
+    return m;
 }
 
 int orc_rms(orc_ctx* c, double* rms) {  // store/core/check_convergence.f90:17-32

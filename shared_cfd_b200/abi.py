@@ -11,6 +11,7 @@ MAX_SPECIES = 32
 MAX_REACTIONS = 256
 MAX_TRANS_SEC = 5
 BC_MAXVAL = 2 * MAX_SPECIES + 8
+INNER_LOG = 128
 
 # status codes
 OK, E_ARG, E_CUDA, E_TNEWTON, E_CHEM, E_OMEGA, E_RESRATE, E_NAN, E_SPIN, E_CONNECT, E_IO, E_STATE, \
@@ -236,6 +237,7 @@ SIGNATURES = {
     "step": (C.c_int, [_P, C.c_int, C.POINTER(Stats)]),
     "run": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(Stats)]),
     "rms": (C.c_int, [_P, _D]),
+    "inner_log": (C.c_int, [_P, _D, _D, C.c_int]),
     "download": (C.c_int, [_P, _D, _D, _D, _D]),
     "download_qp": (C.c_int, [_P, _D]),
     "write_restart": (C.c_int, [_P, C.c_char_p, C.c_int]),

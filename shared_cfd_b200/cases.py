@@ -230,11 +230,27 @@ def control_chem_text(po, To, ox, pf, Tf, fuel, rtol=1e-6, atol=1e-6):
             "Absolute Torelance VODE : %-15.7e\n" % atol)
 
 
-def h2air_mechanism(seed=20240607, po=1e5, To=1500.0, pf=1e5, Tf=300.0, **kw):
-    """(Mechanism, fuel/oxidiser states) after the reference's set-up."""
+def with_trace(comp, trace):
+    """A control_chem.inp composition (mole ratios) in which every species of
+    SPECIES9 that the stream lacks appears at `trace` times the stream's total
+    ratio."""
+    if trace <= 0.0:
+        return dict(comp)
+    tot = sum(comp.values())
+    out = dict(comp)
+    for sp in SPECIES9:
+        out.setdefault(sp, trace * tot)
+    return out
+
+
+def h2air_mechanism(seed=20240607, po=1e5, To=1500.0, pf=1e5, Tf=300.0, trace=0.0, **kw):
+    """(Mechanism, fuel/oxidiser states) after the reference's set-up.  trace > 0
+    lists every absent species in both stream compositions of control_chem.inp
+    at that mole ratio (relative to the stream), so no species starts at zero."""
     m = CH.parse_chem(seeded_chem_inp(seed, **kw), open(os.path.join(DATA, "elements_mw.dat")).read())
     CH.parse_trans(open(os.path.join(DATA, "h2air9_trans.dat")).read(), m)
-    comp = CH.parse_control_chem(control_chem_text(po, To, {"O2": 1, "N2": 3.76}, pf, Tf, {"H2": 1}), m)
+    comp = CH.parse_control_chem(control_chem_text(po, To, with_trace({"O2": 1, "N2": 3.76}, trace), pf, Tf,
+                                                   with_trace({"H2": 1}, trace)), m)
     fo = CH.fuel_oxidizer(m, comp, len(m.species))
     return m, fo
 
@@ -253,7 +269,8 @@ def moving_state(st, u, v, D):
     return q, w
 
 
-def reacting_step(scale=1.0, seed=20240607, precision=abi.PREC_FP64, inner=20, dt=1e-7, mech_kw=None):
+def reacting_step(scale=1.0, seed=20240607, precision=abi.PREC_FP64, inner=20, dt=1e-7, mech_kw=None, trace=0.0,
+                  omega_max=0.1, checks="relaxed"):
     """Axisymmetric backward-facing step with a central H2 jet.
 
     Blocks (x axial, r radial, axis r=0; at scale 1 the cell counts are exact):
@@ -264,7 +281,16 @@ def reacting_step(scale=1.0, seed=20240607, precision=abi.PREC_FP64, inner=20, d
     Air (O2:N2 = 1:3.76) enters block 1 at 1500 K, M = 2; H2 enters block 3
     at 300 K and 1200 m/s through the step face r < 0.005; r in [0.005, 0.01]
     of the step face and r = 0.01 upstream are no-slip walls; r = 0.02 is a
-    slip wall; r = 0 is the axis; x = 0.04 is a supersonic outflow."""
+    slip wall; r = 0 is the axis; x = 0.04 is a supersonic outflow.
+
+    trace: mole ratio of every absent species in both streams (h2air_mechanism).
+    omega_max: control.inp "InternalLoop Omega Max".
+    checks: "reference" keeps the shipped "InternalLoop Omega Min" (1e-3) and
+    "ResRateErr" (1e-3) of NR/q2d/control.part.inp, so a step whose omega
+    falls below 1e-3 or whose inner residual does not drop three orders stops
+    with E_OMEGA / E_RESRATE as the reference stops; "relaxed" lowers Omega Min
+    to 1e-8 and turns ResRateErr off (the impulsive start from the uniform
+    initial state needs both)."""
     n = lambda k: max(4, int(round(k * scale)))
     n512, n256 = n(512), n(256)
     h1, h, H, Lu, Lx = 0.005, 0.010, 0.020, 0.02, 0.04
@@ -276,19 +302,18 @@ def reacting_step(scale=1.0, seed=20240607, precision=abi.PREC_FP64, inner=20, d
     planes = [rect_plane(xu, r_out), rect_plane(xd, r_out), rect_plane(xd, r_core), rect_plane(xd, r_wake)]
     # the connectivity generator compares text-parsed coordinates
     planes = F.roundtrip_plot3d_values(planes)
-    m, fo = h2air_mechanism(seed, **(mech_kw or {}))
+    m, fo = h2air_mechanism(seed, trace=trace, **(mech_kw or {}))
     ns = len(m.species)
     d = base_desc(ny=ns, dim=abi.DIM_Q2D, dt_mode=abi.DT_FIXED, scheme=abi.SCHEME_NR, viscous=1,
                   thermo=abi.THERMO_CHEMKIN_REACTIVE)
     d.dt_fixed = dt
     d.num_internal_loop = inner + 1
-    # control.inp "InternalLoop ResRateErr": the impulsive start cannot drop the
-    # inner residual 3 orders within 20 relaxed (omega <= 0.1) iterations, so the
-    # ratio is reported (res_warn) but does not stop the run.
-    d.res_rate_err = 1e300
-    # "InternalLoop Omega Min": positivity limiting keeps omega near 1e-3 while
-    # the jet starts; the floor is lowered so that it cannot stop the run.
-    d.omega_min = 1e-8
+    d.omega_max = omega_max
+    if checks == "relaxed":
+        d.res_rate_err = 1e300
+        d.omega_min = 1e-8
+    elif checks != "reference":
+        raise ValueError("checks must be 'reference' or 'relaxed'")
     d.precision = precision
     cut, _ = F.connectivity(planes)
     case = Case(planes, d, cut=cut, chem=CH.to_struct(m))

@@ -380,6 +380,7 @@ __global__ void k_nr_update(View v, const double* partials, int nstrips, int inn
             if (inner == 1) v.sc->res1 = res;
             v.sc->res = res;
             v.sc->omega = omf;
+            log_inner(v.sc, inner, om, res);
         }
     }
     __syncthreads();

@@ -86,6 +86,7 @@ __global__ void k_res_import(View v, const double* red, int inner) {
     if (inner == 1) sc->res1 = red[0];
     sc->res = red[0];
     sc->omega = fmin(v.omega_max, red[1]);
+    log_inner(sc, inner, red[1], red[0]);
 }
 
 __global__ void k_status_export(View v, double* red) { red[0] = -(double)v.sc->status; }

@@ -477,6 +477,7 @@ __global__ void __launch_bounds__(1024) k_unpack(View v, const int2* blk, const 
                 if (inner == 1) v.sc->res1 = res;
                 v.sc->res = res;
                 v.sc->omega = om;
+                log_inner(v.sc, inner, o, res);
             }
         }
         s_om = om;

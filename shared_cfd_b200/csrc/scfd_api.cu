@@ -1637,6 +1637,18 @@ int scfd_rms(scfd_ctx* c, double* rms) {
     return (*rms != *rms) ? SCFD_E_NAN : 0;
 }
 
+int scfd_inner_log(scfd_ctx* c, double* omega, double* res, int n) {
+    if (!c || !c->committed || n < 0) return -SCFD_E_ARG;
+    if (!dual_time_scheme(c->d.scheme)) return 0;
+    if (int st = sync_scalars(c)) return -st;
+    int m = std::min(std::min(n, std::max(0, c->d.num_internal_loop - 1)), SCFD_INNER_LOG);
+    for (int k = 0; k < m; ++k) {
+        if (omega) omega[k] = c->h_sc->il_omega[k];
+        if (res) res[k] = c->h_sc->il_res[k];
+    }
+    return m;
+}
+
 int scfd_download(scfd_ctx* c, double* q, double* w, double* vhi, double* tt) {
     if (!c || !c->committed) return SCFD_E_ARG;
     int st;

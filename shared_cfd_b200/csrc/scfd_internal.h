@@ -79,7 +79,19 @@ struct DevScalars {
     long long chem_attempts;
     long long chem_fallback;
     unsigned long long spin_abort;  // non-zero once a bounded wait gave up
+    // per inner iteration of the last step (internal_res.dat of
+    // time_NR_viscous.f90:87-95): omega from the Dqrate limiter before the
+    // omega_max cap, and the residual sum
+    double il_omega[SCFD_INNER_LOG];
+    double il_res[SCFD_INNER_LOG];
 };
+// records the inner iteration's omega candidate and residual (inner >= 1)
+__device__ __forceinline__ void log_inner(DevScalars* sc, int inner, double omega_raw, double res) {
+    if (inner >= 1 && inner <= SCFD_INNER_LOG) {
+        sc->il_omega[inner - 1] = omega_raw;
+        sc->il_res[inner - 1] = res;
+    }
+}
 
 // All device pointers of a context; passed by value to the kernels.
 struct View {

@@ -170,6 +170,19 @@ class Solver:
         self._check(self.lib.rms(self.ctx, C.byref(r)), "rms")
         return r.value
 
+    def inner_log(self):
+        """(omega, res) per inner iteration of the last step, as arrays: omega
+        from the Dqrate limiter before the omega_max cap (1e300 when no species
+        decreases), res the residual sum (res / res[0] is the reference's
+        internal_res.dat ratio)."""
+        n = abi.INNER_LOG
+        om = np.zeros(n)
+        res = np.zeros(n)
+        m = self.lib.inner_log(self.ctx, abi.dptr(om), abi.dptr(res), n)
+        if m < 0:
+            self._check(-m, "inner_log")
+        return om[:m], res[:m]
+
     def download(self):
         c = self.case
         q = np.zeros_like(c.q)

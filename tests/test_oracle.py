@@ -84,3 +84,23 @@ def test_omega_floor_is_reported(orc):
     st = s.step(1, check=False)
     s.close()
     assert st.status == abi.E_OMEGA
+
+
+def test_inner_log_records_every_inner_iteration(orc):
+    """The internal_res.dat record (time_NR_viscous.f90:87-95): one omega and
+    residual per inner iteration; the first residual is res1, the last is res,
+    and the applied omega is the last candidate capped at omega_max."""
+    from shared_cfd_b200.solver import Solver
+    case = cases.reacting_step(scale=1.0 / 64.0, inner=4)
+    s = Solver(case, lib=orc)
+    try:
+        s.upload()
+        s.prepare(1)
+        st = s.step(1)
+        om, res = s.inner_log()
+    finally:
+        s.close()
+    assert len(om) == len(res) == 4
+    assert res[0] == st.res1 and res[-1] == st.res
+    assert min(case.desc.omega_max, om[-1]) == st.omega
+    assert np.all(om > 0.0) and np.all(res > 0.0)
