@@ -62,8 +62,23 @@ def shard_pieces(config, world):
     return (world + 1) // 2 if config == "reacting_step" else world
 
 
+def unit_of(config):
+    return "Mcell-step/s" if config == "sod" else "Mcell-iter/s"
+
+
+def unit_of_case(case):
+    return "Mcell-step/s" if case.desc.scheme == abi.SCHEME_EULER else "Mcell-iter/s"
+
+
 def iters_per_step(case):
     return max(1, case.desc.num_internal_loop - 1) if case.desc.scheme == abi.SCHEME_NR else 1
+
+
+METRIC = {
+    "reacting_step": "Mcell-iter/s of the reacting-step NR dual-time step (cells x inner iterations per second)",
+    "flat_plate": "Mcell-iter/s of the flat-plate LU-SGS step (cells x iterations per second)",
+    "sod": "Mcell-step/s of the Sod explicit step (cells x steps per second)",
+}
 
 
 def workload_name(config, scale):
@@ -245,11 +260,12 @@ def cpu_reference(config, scale, steps, cores, threads=None):
     s.upload()
     s.prepare(1)
     t0 = time.perf_counter()
-    s.run(1, steps)
+    st = s.run(1, steps, check=False)
     dt = time.perf_counter() - t0
+    q = s.download()[0]
     s.close()
     units = case.ncells * iters_per_step(case) * steps
-    return units / dt / 1e6, dt, case
+    return units / dt / 1e6, dt, case, q, st.status
 
 
 def l2_note(case):
@@ -702,14 +718,14 @@ def main():
         if rank != 0:
             return 0
         steps = max(1, args.steps)
-        val, dt, case = cpu_reference(args.config, args.scale, steps, cores)
-        unit = "Mcell-iter/s"
-        line = {"impl": "reference", "metric": "Mcell-iter/s (plain FP64)", "value": val, "unit": unit,
+        val, dt, case, _, _ = cpu_reference(args.config, args.scale, steps, cores)
+        unit = unit_of(args.config)
+        line = {"impl": "reference", "metric": METRIC[args.config], "value": val, "unit": unit,
                 "n_gpus": args.gpus, "steps": steps, "warmup": 0, "ms_per_step": 1e3 * dt / steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded)",
                 "config": {"workload": workload_name(args.config, args.scale), "cells": case.ncells,
-                           "inner_iterations": iters_per_step(case)},
+                           "inner_iterations": iters_per_step(case), "controls": controls_note(case)},
                 "cpu_baseline": {"value": val, "unit": unit, "cores": cores, "kind": "port",
                                  "sample": "%d physical step(s) of the full workload on %d OpenMP threads "
                                            "(C++ FP64 restatement of the reference)" % (steps, cores)},
@@ -745,10 +761,11 @@ def main():
         build.build()
     barrier()
 
+    unit = unit_of(args.config)
     res = {}
     solvers = {}
     pieces = shard_pieces(args.config, world)
-    for prec, tag in ((abi.PREC_MIXED, "mixed"), (abi.PREC_FP64, "fp64")):
+    for prec, tag in ((abi.PREC_FP64, "fp64"), (abi.PREC_MIXED, "mixed")):
         case = make_case(args.config, args.scale, prec)
         if sharded:
             case = cases.split_planes_i(case, pieces)
@@ -762,50 +779,119 @@ def main():
         ms = max_over_ranks(ms)
         # strong scaling under sharding: the ranks share one workload
         units = case.ncells * iters_per_step(case) * args.steps * (1 if sharded else world)
+        om, rr = s.inner_log() if case.desc.scheme == abi.SCHEME_NR else (np.zeros(0), np.zeros(0))
         res[tag] = {"ms": ms, "value": units / (ms * 1e-3) / 1e6, "launches": nl, "clocks": clk,
-                    "autotune": s.tuning(),
-                    "status": st.status, "res_warn": st.res_warn, "omega": st.omega,
-                    "chem_attempts": st.chem_attempts, "chem_fallback": st.chem_fallback_cells}
+                    "autotune": s.tuning(), "status": st.status, "res_warn": st.res_warn, "omega": st.omega,
+                    "chem_attempts": st.chem_attempts, "chem_fallback": st.chem_fallback_cells,
+                    "inner_omega": [float(x) for x in om], "inner_res_ratio": [float(x / rr[0]) for x in rr]}
         solvers[tag] = (s, case)
-        log("%s: %.2f ms/step  %.1f Mcell-iter/s  status %d" % (tag, ms / args.steps, res[tag]["value"], st.status))
+        log("%s: %.2f ms/step  %.1f %s  status %d" % (tag, ms / args.steps, res[tag]["value"], unit, st.status))
 
-    # accuracy of the mixed path against the FP64 path after the same steps
-    qm, _, _, _ = solvers["mixed"][0].gather() if sharded else solvers["mixed"][0].download()
-    qd, _, _, _ = solvers["fp64"][0].gather() if sharded else solvers["fp64"][0].download()
-    case = solvers["fp64"][1]
+    peak, peak_kind = measured_peaks()
+    prof, roof = {}, {}
+    for tag in ("fp64", "mixed"):
+        s_k, case_k = solvers[tag]
+        cells_here = s_k.owned_cells if sharded else case_k.ncells
+        prof[tag] = kernel_profile(s_k, args.steps, case_k, tag == "mixed", cells_here)
+        roof[tag] = roofline_of(prof[tag], args.config, tag == "mixed", cells_here, peak, peak_kind)
+
+    # end to end through the C ABI with host buffers, both precisions
+    e2e = {tag: e2e_run(*solvers[tag], args.steps, sharded, world, barrier, max_over_ranks, torch, dev)
+           for tag in ("fp64", "mixed")}
+
+    # the CPU restatement on the same workload: the timed baseline, and the
+    # oracle state both GPU paths are compared with after the same steps
+    cpu, acc = None, None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, dt, _, q_orc, orc_status = cpu_reference(args.config, args.scale, args.cpu_steps, cores)
+            cpu = {"value": v, "unit": unit, "cores": cores, "kind": "port",
+                   "sample": "%d physical step(s) of the full workload (%.1f s) on %d OpenMP threads, "
+                             "C++ FP64 restatement" % (args.cpu_steps, dt, cores)}
+            # one core, on a quarter-resolution sample of the same case (1/16 of the cells)
+            v1, dt1, c1, _, _ = cpu_reference(args.config, args.scale * 0.25, 1, cores, threads=1)
+            cpu["single_core"] = {"value": v1, "unit": unit, "cores": 1,
+                                  "sample": "1 physical step of the workload at quarter resolution per "
+                                            "direction (%d cells, %.1f s) on 1 thread" % (c1.ncells, dt1)}
+            acc = accuracy_vs_oracle(args, q_orc, orc_status)
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": unit, "cores": cores, "kind": "port", "sample": "failed: %s" % e}
+
+    # the mixed path against the FP64 path after the timed steps
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from helpers import rel_l2
-    l2_mixed = rel_l2(case, qm, qd)
+    qm = solvers["mixed"][0].gather()[0] if sharded else solvers["mixed"][0].download()[0]
+    qd = solvers["fp64"][0].gather()[0] if sharded else solvers["fp64"][0].download()[0]
+    l2_mixed_fp64 = rel_l2(solvers["fp64"][1], qm, qd)
 
-    # per-kernel device times (separate, profiled pass of the mixed path)
-    s_m, case_m = solvers["mixed"]
-    cells_here = s_m.owned_cells if sharded else case_m.ncells
-    prof = kernel_profile(s_m, args.steps, case_m, True, cells_here)
-    prof64 = kernel_profile(solvers["fp64"][0], args.steps, case, False, cells_here)
-    peak, peak_kind = measured_peaks()
+    if rank == 0:
+        d, m = res["fp64"], res["mixed"]
+        case = solvers["fp64"][1]
+        line = {
+            "metric": METRIC[args.config],
+            "value": d["value"], "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": d["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": workload_name(args.config, args.scale), "cells": case.ncells,
+                       "inner_iterations": iters_per_step(case),
+                       "parallelism": ("%d GPU(s), block-sharded: %d planes (blocks cut along i into %d), "
+                                       "NCCL all-gather of halo cells and all-reduce of dt/res/omega/status"
+                                       % (world, len(case.planes), pieces)) if sharded else "1 GPU",
+                       "l2": l2_note(case), "controls": controls_note(case)},
+            "e2e": e2e["fp64"], "gpu_launches": d["launches"], "clocks": d["clocks"],
+            "roofline": roof["fp64"], "cpu_baseline": cpu,
+            "accuracy": acc,
+            "status": {"code": d["status"], "res_warn": d["res_warn"], "omega": d["omega"],
+                       "chem_attempts": d["chem_attempts"], "chem_fallback_cells": d["chem_fallback"],
+                       "last_step_inner_omega": d["inner_omega"], "last_step_inner_res_ratio": d["inner_res_ratio"]},
+            "mixed": {"value": m["value"], "unit": unit, "ms_per_step": m["ms"] / args.steps,
+                      "over_fp64": m["value"] / d["value"], "e2e": e2e["mixed"], "gpu_launches": m["launches"],
+                      "clocks": m["clocks"], "roofline": roof["mixed"], "l2_vs_fp64_gpu": l2_mixed_fp64,
+                      "dtype": "f32 reconstruction, fluxes and sweeps; f64 thermo, chemistry, sums, updates",
+                      "status": {"code": m["status"], "omega": m["omega"],
+                                 "last_step_inner_omega": m["inner_omega"]}},
+            "autotune": {"fp64": d["autotune"], "mixed": m["autotune"]},
+            "kernels_fp64": {k: {kk: v[kk] for kk in ("avg_ms", "launches", "total_ms", "gbs") if kk in v}
+                             for k, v in prof["fp64"].items()},
+            "kernels_mixed": {k: {kk: v[kk] for kk in ("avg_ms", "launches", "total_ms", "gbs") if kk in v}
+                              for k, v in prof["mixed"].items()},
+        }
+        print(json.dumps(line), flush=True)
+    for s, _ in solvers.values():
+        s.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def roofline_of(prof, config, mixed, cells_here, peak, peak_kind):
+    """Roofline of the dominant HBM-touching kernel of one precision's profile,
+    and the same for the face-flux kernel."""
     hbm = {k: v for k, v in prof.items() if v["bytes_per_launch"] > 0 and v["kind"] != abi.K_CHEM}
     top = max(prof.items(), key=lambda kv: kv[1]["total_ms"])
     dom = max(hbm.items(), key=lambda kv: kv[1]["total_ms"]) if hbm else top
     ach = dom[1]["bytes_per_launch"] / (dom[1]["avg_ms"] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom[0], "achieved": ach, "peak": peak, "unit": "GB/s",
                 "frac": ach / peak, "peak_source": peak_kind,
-                "traffic": traffic_per_launch(args.config, True, dom[1]["kind"], cells_here),
+                "traffic": traffic_per_launch(config, mixed, dom[1]["kind"], cells_here),
                 "traffic_source": NCU_TRAFFIC_NOTE,
                 "algorithmic_bytes_per_launch": dom[1]["bytes_per_launch"],
                 "avg_launch_ms": dom[1]["avg_ms"], "top_kernel_by_time": top[0]}
-    # the face-flux kernel (MUSCL + SLAU + viscous fluxes + RHS) on the same roofline
     if "residual" in prof:
         r = prof["residual"]
         ach_r = r["bytes_per_launch"] / (r["avg_ms"] * 1e-3) / 1e9
         roofline["flux_kernel"] = {"kernel": "residual", "achieved": ach_r, "frac": ach_r / peak,
-                                   "traffic": traffic_per_launch(args.config, True, abi.K_RESIDUAL, cells_here),
+                                   "traffic": traffic_per_launch(config, mixed, abi.K_RESIDUAL, cells_here),
                                    "avg_launch_ms": r["avg_ms"]}
-    for v in list(prof.values()) + list(prof64.values()):
+    for v in prof.values():
         if v["bytes_per_launch"]:
             v["gbs"] = v["bytes_per_launch"] / (v["avg_ms"] * 1e-3) / 1e9
+    return roofline
 
-    # end to end through the C ABI with host buffers
-    s_e, case_e = solvers["mixed"]
+
+def e2e_run(s_e, case_e, steps, sharded, world, barrier, max_over_ranks, torch, dev):
+    """The metric through scfd_upload / scfd_step / scfd_download with host
+    buffers every step (the reference-layout arrays cross PCIe)."""
     q = np.ascontiguousarray(case_e.q)
     w = np.ascontiguousarray(case_e.w)
     vhi = np.ascontiguousarray(case_e.vhi)
@@ -815,67 +901,48 @@ def main():
     barrier()
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    for k in range(args.steps):
+    for k in range(steps):
         s_e._check(lib.upload(s_e.ctx, abi.dptr(q), abi.dptr(w), abi.dptr(vhi), 0.0), "upload")
         if sharded:
-            s_e.dstep(k + 1)
+            s_e.dstep(k + 1, check=False)
         else:
             st = abi.Stats()
             lib.step(s_e.ctx, k + 1, C.byref(st))
         s_e._check(lib.download(s_e.ctx, abi.dptr(qout), None, None, C.byref(ttc)), "download")
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    units = case_e.ncells * iters_per_step(case_e) * args.steps * (1 if sharded else world)
-    e2e = {"value": units / e2e_s / 1e6, "unit": "Mcell-iter/s",
-           "h2d_bytes_per_step": int(q.nbytes + w.nbytes + vhi.nbytes), "d2h_bytes_per_step": int(qout.nbytes)}
+    units = case_e.ncells * iters_per_step(case_e) * steps * (1 if sharded else world)
+    return {"value": units / e2e_s / 1e6, "unit": unit_of_case(case_e),
+            "h2d_bytes_per_step": int(q.nbytes + w.nbytes + vhi.nbytes), "d2h_bytes_per_step": int(qout.nbytes)}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            v, dt, _ = cpu_reference(args.config, args.scale, args.cpu_steps, cores)
-            cpu = {"value": v, "unit": "Mcell-iter/s", "cores": cores, "kind": "port",
-                   "sample": "%d physical step(s) of the full workload (%.1f s) on %d OpenMP threads, "
-                             "C++ FP64 restatement" % (args.cpu_steps, dt, cores)}
-            # one core, on a quarter-resolution sample of the same case (1/16 of the cells)
-            v1, dt1, c1 = cpu_reference(args.config, args.scale * 0.25, 1, cores, threads=1)
-            cpu["single_core"] = {"value": v1, "unit": "Mcell-iter/s", "cores": 1,
-                                  "sample": "1 physical step of the workload at quarter resolution per "
-                                            "direction (%d cells, %.1f s) on 1 thread" % (c1.ncells, dt1)}
-        except Exception as e:  # noqa: BLE001
-            cpu = {"value": None, "unit": "Mcell-iter/s", "cores": cores, "kind": "port", "sample": "failed: %s" % e}
 
-    if rank == 0:
-        m = res["mixed"]
-        line = {
-            "metric": "Mcell-iter/s (mixed FP32/FP64; plain FP64 in fp64_value)",
-            "value": m["value"], "unit": "Mcell-iter/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": m["ms"] / args.steps, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic (seeded)",
-            "config": {"workload": workload_name(args.config, args.scale), "cells": case.ncells,
-                       "inner_iterations": iters_per_step(case),
-                       "parallelism": ("%d GPU(s), block-sharded: %d planes (blocks cut along i into %d), "
-                                       "NCCL all-gather of halo cells and all-reduce of dt/res/omega/status"
-                                       % (world, len(case.planes), pieces)) if sharded else "1 GPU",
-                       "l2": l2_note(case)},
-            "fp64_value": res["fp64"]["value"], "fp64_ms_per_step": res["fp64"]["ms"] / args.steps,
-            "mixed_over_fp64": m["value"] / res["fp64"]["value"],
-            "l2_mixed_vs_fp64": l2_mixed,
-            "e2e": e2e, "gpu_launches": m["launches"],
-            "autotune": {"mixed": m["autotune"], "fp64": res["fp64"]["autotune"]},
-            "clocks": m["clocks"], "roofline": roofline, "cpu_baseline": cpu,
-            "status": {"mixed": m["status"], "fp64": res["fp64"]["status"], "res_warn": m["res_warn"],
-                       "omega": m["omega"], "omega_fp64": res["fp64"]["omega"],
-                       "chem_attempts": m["chem_attempts"], "chem_fallback_cells": m["chem_fallback"]},
-            "kernels_mixed": {k: {kk: v[kk] for kk in ("avg_ms", "launches", "total_ms", "gbs") if kk in v}
-                              for k, v in prof.items()},
-            "kernels_fp64": {k: {kk: v[kk] for kk in ("avg_ms", "launches", "total_ms", "gbs") if kk in v}
-                             for k, v in prof64.items()},
-        }
-        print(json.dumps(line), flush=True)
-    for s, _ in solvers.values():
+def accuracy_vs_oracle(args, q_orc, orc_status):
+    """Relative L2 (all conserved variables, and the largest per-component
+    value) of the GPU FP64 and mixed paths against the CPU restatement after the
+    same args.cpu_steps steps from the same initial state."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import rel_l2, rel_l2_per_component
+    from shared_cfd_b200.solver import Solver
+    out = {"steps": args.cpu_steps, "oracle_status": orc_status}
+    for prec, tag in ((abi.PREC_FP64, "fp64"), (abi.PREC_MIXED, "mixed")):
+        case = make_case(args.config, args.scale, prec)
+        s = Solver(case)
+        s.upload()
+        s.prepare(1)
+        st = s.run(1, args.cpu_steps, check=False)
+        q = s.download()[0]
         s.close()
-    if dist is not None:
-        dist.destroy_process_group()
-    return 0
+        out[tag + "_vs_oracle"] = rel_l2(case, q, q_orc)
+        out[tag + "_vs_oracle_per_component_max"] = rel_l2_per_component(case, q, q_orc)[0]
+        out[tag + "_status"] = st.status
+    return out
+
+
+def controls_note(case):
+    d = case.desc
+    if d.scheme != abi.SCHEME_NR:
+        return None
+    return {"omega_max": d.omega_max, "omega_min": d.omega_min, "dqrate_max": d.dq_max,
+            "res_rate_err": d.res_rate_err if d.res_rate_err < 1e299 else "off"}
 
 
 if __name__ == "__main__":
