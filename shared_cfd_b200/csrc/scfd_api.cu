@@ -51,9 +51,9 @@ struct scfd_ctx {
     int nops = 0;
     double* d_bcval = nullptr;
     int valstride = SCFD_BC_MAXVAL + 2;
-    // strip-record sweeps (k_sweep3.cu)
+    // cluster-wavefront sweeps over strip records (k_wave.cu)
     bool use_sw3 = false;
-    Sweep3 sw3{};
+    Wave sw3{};
     // chemistry
     unsigned long long* d_counter = nullptr;
     // rms
@@ -450,9 +450,9 @@ struct Seq {
         if (c->nsf == 0) return;  // a rank without planes
         launch_sweep_reset(s, c->d_progress, c->d_tickets, c->nsf, c->nsb);
         if (c->use_sw3) {
-            n += timed(c, SCFD_K_PACK, [&] { return launch_sweep3(v, s, c->sw3, 0, 0); });
-            n += timed(c, SCFD_K_SWEEP_FWD, [&] { return launch_sweep3(v, s, c->sw3, 1, 0); });
-            n += timed(c, SCFD_K_SWEEP_BWD, [&] { return launch_sweep3(v, s, c->sw3, 2, 0); });
+            n += timed(c, SCFD_K_PACK, [&] { return launch_wave(v, s, c->sw3, 0, 0); });
+            n += timed(c, SCFD_K_SWEEP_FWD, [&] { return launch_wave(v, s, c->sw3, 1, 0); });
+            n += timed(c, SCFD_K_SWEEP_BWD, [&] { return launch_wave(v, s, c->sw3, 2, 0); });
             return;
         }
         n += timed(c, SCFD_K_SWEEP_FWD, [&] {
@@ -472,10 +472,10 @@ struct Seq {
     void update(int inner, const double* part, int nparts) {
         if (c->use_sw3) {
             if (c->nsf == 0) return;
-            Sweep3 w3 = c->sw3;
+            Wave w3 = c->sw3;
             w3.partials = const_cast<double*>(part);
             w3.nstrips = nparts;
-            n += timed(c, SCFD_K_UPDATE, [&] { return launch_sweep3(v, s, w3, 3, inner); });
+            n += timed(c, SCFD_K_UPDATE, [&] { return launch_wave(v, s, w3, 3, inner); });
         } else if (dual_time_scheme(c->d.scheme)) {
             n += timed(c, SCFD_K_UPDATE, [&] { return launch_nr_update(v, s, part, nparts, inner); });
         }
@@ -758,42 +758,43 @@ int scfd_commit(scfd_ctx* c) {
     // chemistry tables, compact
     const ChemTables tabs = c->have_chem ? ChemTables(c->chem) : ChemTables();
     const int nrec = 64 * c->np;
-    // strip records for the TMA-streamed sweeps
+    // strip records for the cluster-wavefront sweeps
     // the dual and precon schemes take the generic residual and sweeps
     const bool dual = c->d.scheme == SCFD_SCHEME_DUAL || precon_scheme(c->d.scheme);
-    const size_t blk3 = impl && !dual ? sweep3_record_elems(nY, mixed) : 0;
+    const WaveSizes wz = impl && !dual ? wave_sizes(nY, mixed) : WaveSizes{0, 0, 0, 0};
     const size_t esz3 = mixed ? sizeof(float) : sizeof(double);
     const bool legacy = std::getenv("SCFD_SWEEP_LEGACY") != nullptr;
     const char* graph_env = std::getenv("SCFD_GRAPH");
     c->use_graph = !(graph_env && std::strcmp(graph_env, "0") == 0);
-    c->use_sw3 = blk3 > 0 && !legacy;
-    std::vector<long long> rec_off;
-    std::vector<int> blks3, tabf3, tabb3;
-    long long rec_total = 0;
+    const int ncl_max = wz.xs > 0 && !legacy ? wave_max_clusters(nY, mixed) : 0;
+    c->use_sw3 = wz.xs > 0 && !legacy && ncl_max > 0;
+    std::vector<long long> step_off;
+    std::vector<int> blks3, strips3, tasksf, tasksb;
+    long long steps_total = 0;
     if (c->use_sw3) {
+        const int pad = wave_pad_steps(), tpc = wave_strips_per_task();
         int fs = 0;
         for (int pl = 0; pl < c->np; ++pl) {
             if (!c->own(pl)) continue;
             const int ns = (c->P.nj[pl] + 31) / 32, steps = c->P.ni[pl] + 31;
+            const int fs_plane = fs;
             for (int st3 = 0; st3 < ns; ++st3, ++fs) {
-                const int pad = sweep3_pad_steps();
-                rec_off.push_back(rec_total + (long long)pad * blk3);
-                rec_total += (long long)(steps + 2 * pad) * blk3;
+                step_off.push_back(steps_total);
+                steps_total += steps + 2 * pad;
                 for (int t0 = 0; t0 < steps; t0 += 32) {
                     blks3.push_back(fs);
                     blks3.push_back(t0);
                 }
-                tabf3.insert(tabf3.end(), {pl, st3, fs, 0});
+                strips3.insert(strips3.end(), {pl, st3, fs, 0});
             }
-        }
-        int base3 = 0;
-        for (int pl = 0; pl < c->np; ++pl) {
-            if (!c->own(pl)) continue;
-            const int ns = (c->P.nj[pl] + 31) / 32;
-            for (int st3 = ns - 1; st3 >= 0; --st3) tabb3.insert(tabb3.end(), {pl, st3, base3 + st3, 0});
-            base3 += ns;
+            // tasks of up to tpc strips: forward from the bottom, backward from the top
+            for (int s0 = 0; s0 < ns; s0 += tpc) tasksf.insert(tasksf.end(), {pl, s0, std::min(tpc, ns - s0), fs_plane});
+            for (int s0 = ns - 1; s0 >= 0; s0 -= tpc) tasksb.insert(tasksb.end(), {pl, s0, std::min(tpc, s0 + 1), fs_plane});
         }
     }
+    const int ntasks = (int)tasksf.size() / 4;
+    const int hk = wave_handoff_chunk();
+    const long long xstride3 = (long long)((c->nimax + hk - 1) / hk) * hk * std::max(1, wz.d4);
     // arena size
     size_t bytes = 0;
     bytes += 3 * need<double>(D * N);                         // q, qp, qpp
@@ -815,8 +816,9 @@ int scfd_commit(scfd_ctx* c) {
     const size_t nref = (size_t)(c->nimax + 4) * (c->njmax + 4) * c->np;
     bytes += need<double>((size_t)std::max(std::max(W, D), nY) * nref);
     if (c->use_sw3)
-        bytes += need<char>(rec_total * esz3) + need<long long>(rec_off.size()) + need<int>(blks3.size()) +
-                 need<int>(tabf3.size()) + need<int>(tabb3.size());
+        bytes += need<char>(steps_total * wz.xs * esz3) + need<char>(steps_total * wz.cs * esz3) +
+                 need<long long>(step_off.size()) + need<int>(blks3.size()) + need<int>(strips3.size()) +
+                 need<int>(tasksf.size()) + need<int>(tasksb.size()) + need<double>((size_t)ntasks * xstride3);
     bytes += 64 * 256;
     c->arena_bytes = bytes;
     CK(cudaMalloc(&c->arena, bytes));
@@ -872,24 +874,30 @@ int scfd_commit(scfd_ctx* c) {
         CK(cudaEventCreateWithFlags(&c->ring_ev[b], cudaEventDisableTiming));
     }
     if (c->use_sw3) {
-        Sweep3& w3 = c->sw3;
-        w3.rec = carve<char>(p, rec_total * esz3);
-        long long* ro = carve<long long>(p, rec_off.size());
+        Wave& w3 = c->sw3;
+        w3.X = carve<char>(p, steps_total * wz.xs * esz3);
+        w3.C = carve<char>(p, steps_total * wz.cs * esz3);
+        long long* so = carve<long long>(p, step_off.size());
         int* bk = carve<int>(p, blks3.size());
-        int* tf = carve<int>(p, tabf3.size());
-        int* tb = carve<int>(p, tabb3.size());
-        CK(cudaMemcpyAsync(ro, rec_off.data(), rec_off.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+        int* sp = carve<int>(p, strips3.size());
+        int* tf = carve<int>(p, tasksf.size());
+        int* tb = carve<int>(p, tasksb.size());
+        w3.xfer = carve<double>(p, (size_t)ntasks * xstride3);
+        CK(cudaMemcpyAsync(so, step_off.data(), step_off.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
         CK(cudaMemcpyAsync(bk, blks3.data(), blks3.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(tf, tabf3.data(), tabf3.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(tb, tabb3.data(), tabb3.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-        w3.rec_off = ro;
+        CK(cudaMemcpyAsync(sp, strips3.data(), strips3.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(tf, tasksf.data(), tasksf.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(tb, tasksb.data(), tasksb.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+        w3.step_off = so;
         w3.blk = reinterpret_cast<const int2*>(bk);
         w3.nblk = (int)blks3.size() / 2;
-        w3.tab_f = reinterpret_cast<const int4*>(tf);
-        w3.tab_b = reinterpret_cast<const int4*>(tb);
+        w3.strips = reinterpret_cast<const int4*>(sp);
         w3.nstrips = c->nsf;
-        w3.xfer = c->d_xfer;
-        w3.xstride = (long long)(c->nimax + 8) * D;
+        w3.tasks_f = reinterpret_cast<const int4*>(tf);
+        w3.tasks_b = reinterpret_cast<const int4*>(tb);
+        w3.ntasks = ntasks;
+        w3.nclusters = std::min(ntasks, ncl_max);
+        w3.xstride = xstride3;
         w3.progress = c->d_progress;
         w3.tickets = c->d_tickets;
         w3.partials = c->d_partials;
@@ -1625,8 +1633,19 @@ int scfd_adjoint_run(scfd_ctx* c, const scfd_adj_desc* d, double* J, double* gra
 
 int scfd_tuning(scfd_ctx* c, char* json, int len) {
     if (!c || !json || len <= 0) return SCFD_E_ARG;
-    std::snprintf(json, (size_t)len, "%s", c->tune_report.c_str());
-    return (int)c->tune_report.size() < len ? 0 : SCFD_E_ARG;
+    // the autotuner's report plus the sweep implementation the context runs
+    std::string rep = c->tune_report;
+    char sw[160];
+    if (c->use_sw3)
+        std::snprintf(sw, sizeof(sw), "\"sweep\": {\"kind\": \"cluster wavefront\", \"tasks\": %d, \"clusters\": %d}",
+                      c->sw3.ntasks, c->sw3.nclusters);
+    else
+        std::snprintf(sw, sizeof(sw), "\"sweep\": {\"kind\": \"%s\"}",
+                      c->d.scheme == SCFD_SCHEME_EULER ? "none" : "generic");
+    const size_t close = rep.rfind('}');
+    if (close != std::string::npos) rep = rep.substr(0, close) + (rep.size() > 2 ? ", " : "") + sw + "}";
+    std::snprintf(json, (size_t)len, "%s", rep.c_str());
+    return (int)rep.size() < len ? 0 : SCFD_E_ARG;
 }
 
 int scfd_rms(scfd_ctx* c, double* rms) {

@@ -141,24 +141,35 @@ int launch_sweep(const View& v, cudaStream_t s, int dir, double* xfer, int* prog
                  int* tickets, int nstrips_fwd, int nstrips_bwd, const int* strip_tab_f, const int* strip_tab_b);
 bool launch_sweep2(const View& v, cudaStream_t s, int dir, const int2* strips, int n, double* xfer, int* prog,
                    int* ticket, double* partials, int upd);
-// Strip-record LU-SGS (k_sweep3.cu), available for nY in {1, 8, 9}.
-struct Sweep3 {
-    void* rec;                 // strip records (float on the mixed path)
-    const long long* rec_off;  // per forward strip
-    const int2* blk;           // pack/unpack blocks: (strip, first step)
+// Cluster-wavefront LU-SGS over strip records (k_wave.cu), for nY in {1, 8, 9}.
+struct Wave {
+    void* X;                    // records: x(1:D) per cell and step (float on the mixed path)
+    void* C;                    // records: the cells' coefficients
+    const long long* step_off;  // per forward strip: first step block of its records
+    const int4* strips;         // per forward strip (plane, s, strip, 0): pack / unpack
+    const int2* blk;            // pack/unpack blocks: (strip, first step)
     int nblk;
-    const int4* tab_f;         // forward strips (plane, s, strip, 0)
-    const int4* tab_b;         // backward order
     int nstrips;
-    double* xfer;
-    long long xstride;
-    int* progress;             // 2*nstrips
-    int* tickets;              // 2
-    double* partials;          // 2*nstrips
+    const int4* tasks_f;        // tasks of up to 8 strips (plane, first strip, strips, strip 0's index)
+    const int4* tasks_b;        // backward order
+    int ntasks;
+    int nclusters;              // clusters launched (at most ntasks)
+    void* xfer;                 // per task: published hand-off columns
+    long long xstride;          // elements per task
+    int* progress;              // 2*ntasks
+    int* tickets;               // 2
+    double* partials;           // 2*nstrips
 };
-size_t sweep3_record_elems(int ny, bool mixed);  // elements per step block, 0 if none
-int sweep3_pad_steps();                          // zero step blocks before and after each strip
-int launch_sweep3(const View& v, cudaStream_t s, const Sweep3& w, int what, int inner);
+struct WaveSizes {
+    int xs, cs, d4;  // elements of an X / C step block; padded hand-off column
+    size_t smem;     // dynamic shared memory of the sweep kernel
+};
+WaveSizes wave_sizes(int ny, bool mixed);  // xs = 0 if the species count has no sweep
+int wave_pad_steps();                      // zero step blocks before and after each strip
+int wave_strips_per_task();
+int wave_handoff_chunk();                  // hand-off columns per chunk
+int wave_max_clusters(int ny, bool mixed); // co-resident clusters of the sweep kernel (0: none)
+int launch_wave(const View& v, cudaStream_t s, const Wave& w, int what, int inner);
 int launch_nr_update(const View& v, cudaStream_t s, const double* partials, int nstrips, int inner);
 int launch_chem_impl(const View& v, cudaStream_t s, int max_substeps, unsigned long long* counter, int nsm);
 int launch_step_end(const View& v, cudaStream_t s, double warn, double err);

@@ -180,3 +180,78 @@ def test_graph_replay_matches_eager(gpu, monkeypatch):
         s.close()
     assert np.array_equal(out["eager"][0], out["graph"][0])
     assert out["eager"][1] == out["graph"][1]
+
+
+@pytest.mark.parametrize("nj", [300, 520])
+def test_sweep_tasks_hand_off_through_global_memory(gpu, orc, nj):
+    """Planes of 10 and 17 strips: the wavefront runs as tasks of up to 8
+    strips, so the top row of one task reaches the next through global memory
+    (forward upwards, backward downwards), with a ragged last strip and a
+    one-strip last task."""
+    case = cases.perturb(cases.flat_plate(24, nj), seed=nj)
+    _parity(case, gpu, orc, 3)
+    case.desc.precision = abi.PREC_MIXED
+    a = run_case(case, gpu, 3)
+    assert a["stats"].status == 0 and np.isfinite(a["q"]).all()
+
+
+def test_inner_log_matches_oracle(gpu, orc):
+    """omega (from the Dqrate limiter) and the residual of every inner iteration
+    of a reacting NR step agree with the restatement."""
+    case = cases.reacting_step(scale=1.0 / 32.0, inner=5)
+    logs = []
+    for lib in (gpu, orc):
+        s = Solver(case, lib=lib)
+        try:
+            s.upload()
+            s.prepare(1)
+            s.run(1, 2)
+            logs.append(s.inner_log())
+        finally:
+            s.close()
+    (om_g, res_g), (om_o, res_o) = logs
+    assert len(om_g) == len(om_o) == 5
+    np.testing.assert_allclose(om_g, om_o, rtol=1e-8)
+    np.testing.assert_allclose(res_g, res_o, rtol=1e-8)
+
+
+def test_reacting_step_full_size_one_step(gpu, orc):
+    """The reacting-step workload at its full size (786 432 cells, 512-row
+    planes run as two tasks each), one physical step of 20 inner iterations:
+    FP64 within 1e-10 of the restatement."""
+    case = cases.reacting_step(scale=1.0)
+    _parity(case, gpu, orc, 1)
+
+
+def test_flat_plate_full_config(gpu, orc):
+    """The flat-plate configuration as stated: 256x128 cells, LU-SGS with local
+    time stepping, 5000 iterations.  FP64 within 1e-10 of the restatement; the
+    mixed path's wall-normal profiles of u and T (at x = 0.05 m and 0.09 m)
+    within 1e-6 relative L2 of the restatement's."""
+    case = cases.flat_plate(256, 128)
+    a, b, _ = _parity(case, gpu, orc, 5000)
+    case.desc.precision = abi.PREC_MIXED
+    m = run_case(case, gpu, 5000)
+    assert m["stats"].status == 0
+    D = case.D
+    for x_frac in (0.5, 0.9):
+        i = int(x_frac * case.ni[0])
+        for name, f in (("u", lambda q: q[:, i, 1] / q[:, i, 0]),
+                        ("T", lambda q: (q[:, i, D - 1] - 0.5 * (q[:, i, 1] ** 2 + q[:, i, 2] ** 2) / q[:, i, 0])
+                         / q[:, i, 0])):
+            pm = f(case.interior(m["q"], 0))
+            pb = f(case.interior(b["q"], 0))
+            err = np.linalg.norm(pm - pb) / np.linalg.norm(pb)
+            assert err <= 1e-6, "%s profile at x/L %.1f: %g" % (name, x_frac, err)
+
+
+def test_reacting_step_runs_the_cluster_wavefront(gpu):
+    """Both precisions of the reacting step take the cluster-wavefront sweep
+    (not the generic fallback): 512-row planes in two tasks, 256-row in one."""
+    for prec in (abi.PREC_FP64, abi.PREC_MIXED):
+        s = Solver(cases.reacting_step(scale=1.0, precision=prec), lib=gpu)
+        try:
+            sw = s.tuning()["sweep"]
+        finally:
+            s.close()
+        assert sw["kind"] == "cluster wavefront" and sw["tasks"] == 6 and sw["clusters"] >= 1, sw
