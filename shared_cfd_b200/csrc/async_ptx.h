@@ -116,6 +116,20 @@ __device__ __forceinline__ void st_async16(unsigned raddr, double2 v, unsigned r
 __device__ __forceinline__ void mbar_arrive_cluster(unsigned rbar) {
     asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(rbar) : "memory");
 }
+// the same without release semantics (no fence): for a consumer telling a
+// producer that a buffer may be refilled, where the consumer's reads of it
+// have long completed when the producer next writes it
+__device__ __forceinline__ void mbar_arrive_cluster_relaxed(unsigned rbar) {
+    asm volatile("mbarrier.arrive.relaxed.cluster.shared::cluster.b64 _, [%0];" ::"r"(rbar) : "memory");
+}
+// bulk copy from this CTA's shared memory into another CTA's (shared::cluster
+// address), completing `bytes` of transaction count on the receiver's mbarrier
+__device__ __forceinline__ void bulk_s2dsmem(unsigned rdst, const void* src, unsigned bytes, unsigned rbar) {
+    asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     rdst),
+                 "r"(smem_u32(src)), "r"(bytes), "r"(rbar)
+                 : "memory");
+}
 __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }

@@ -14,10 +14,12 @@
 //
 // A task is up to 8 consecutive strips of one plane, run by one thread-block
 // cluster of 8 CTAs (CTA rank r on the task's strip r).  Strip r's lane 31
-// writes its row straight into CTA r + 1's hand-off ring with st.async (16-byte
-// stores into distributed shared memory that complete a transaction count on
-// an mbarrier of the receiving CTA), in chunks of HK columns; the receiver
-// releases each chunk with a remote arrive.  Between tasks of one plane the
+// stages its row in its own shared memory and, every HK columns, one bulk copy
+// moves the chunk into CTA r + 1's hand-off ring (distributed shared memory),
+// completing a transaction count on an mbarrier of the receiving CTA; the
+// receiver releases each chunk with a remote arrive.  A task with a successor
+// holds 8 strips, so only rank 7 ever publishes to global memory and ranks
+// 0-6 only to the next CTA.  Between tasks of one plane the
 // top row travels through global memory: the last CTA's helper warp copies it
 // out and publishes a progress counter (release), the next task's rank-0
 // helper polls it (acquire) and bulk-copies the chunk into its own ring.
@@ -300,8 +302,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
     // running uses (over all tasks of this cluster) of this CTA's rings
     unsigned rc = 0;  // record chunks
     unsigned xc = 0;  // hand-off chunks consumed from xin
-    unsigned pc = 0;  // chunks produced into the successor's xin
-    unsigned oc = 0;  // chunks produced into xout
+    unsigned pc = 0;  // chunks of this CTA's top row produced through xout
 
     for (;;) {
         if (threadIdx.x == 0 && rank == 0) {
@@ -366,7 +367,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                 }
                 RT* sx = ringX + slot * SPB * XS;
                 const RT* scf = ringC + slot * SPB * CSZ;
-#pragma unroll
+#pragma unroll 2
                 for (int u = 0; u < SPB; ++u) {
                     const int t = n * SPB + u;
                     const int pos = DIR == 0 ? u : SPB - 1 - u;
@@ -390,7 +391,9 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                     if (in_col && ((t % HK) == HK - 1 || t == ni - 1)) {
                         if (lane == 0) {
                             mbar_arrive_expect_tx(&xfull[hs], CHUNK_BYTES);  // its next use
-                            mbar_arrive_cluster(rel + hs * 8u);
+                            // the chunk is refilled 16 chunks later, long after lane 0's
+                            // reads of it completed: no release fence needed
+                            mbar_arrive_cluster_relaxed(rel + hs * 8u);
                         }
                         ++xc;
                     }
@@ -469,40 +472,35 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                             }
                         }
                     }
-                    // publish column cc of the top row (lane 31) to the strip above
+                    // publish column cc of the top row (lane 31) to the strip above: into
+                    // this CTA's xout ring; a whole chunk then goes by one bulk copy into
+                    // the next CTA's xin (or to the helper, for the next task)
                     const int cc = t - 31;
                     if ((pub_remote || pub_global) && cc >= 0 && cc < ni) {
-                        const unsigned cnt = pub_remote ? pc : oc;
-                        const unsigned ps = cnt % HS;
+                        const unsigned ps = pc % HS;
                         const int col = cc % HK;
                         const bool last = col == HK - 1 || cc == ni - 1;
                         bool okp = true;
                         if (lane == 31) {
-                            if (col == 0 && cnt >= HS)
-                                okp = wait_phase(pub_remote ? &pempty[ps] : &oemp[ps], ((cnt / HS) - 1u) & 1u, v, s_bail);
+                            if (col == 0 && pc >= HS)
+                                okp = wait_phase(pub_remote ? &pempty[ps] : &oemp[ps], ((pc / HS) - 1u) & 1u, v, s_bail);
                             if (okp) {
                                 RT vals[D4];
 #pragma unroll
                                 for (int k = 0; k < D4; ++k) vals[k] = k < D ? outB[k] : RT(0);
-                                if (pub_remote) {
-                                    const unsigned dst = dring + (unsigned)((ps * HK + col) * D4) * sizeof(RT);
+                                RT* dst = xout + (ps * HK + col) * D4;
 #pragma unroll
-                                    for (int g = 0; g < D4 / G; ++g)
-                                        st_async16(dst + g * 16, *reinterpret_cast<V*>(&vals[g * G]), dfull + ps * 8u);
-                                    // a partial last chunk is completed with zero columns
-                                    if (cc == ni - 1) {
-                                        const V z{};
-                                        for (int c2 = col + 1; c2 < HK; ++c2) {
-                                            const unsigned d2 = dring + (unsigned)((ps * HK + c2) * D4) * sizeof(RT);
-                                            for (int g = 0; g < D4 / G; ++g) st_async16(d2 + g * 16, z, dfull + ps * 8u);
-                                        }
+                                for (int g = 0; g < D4 / G; ++g)
+                                    reinterpret_cast<V*>(dst)[g] = *reinterpret_cast<V*>(&vals[g * G]);
+                                if (last) {
+                                    if (pub_remote) {
+                                        // columns past ni of a partial last chunk travel as they are
+                                        fence_proxy_async_smem();
+                                        bulk_s2dsmem(dring + ps * CHUNK_BYTES, xout + ps * HK * D4, CHUNK_BYTES,
+                                                     dfull + ps * 8u);
+                                    } else {
+                                        mbar_arrive(&oful[ps]);
                                     }
-                                } else {
-                                    RT* dst = xout + (ps * HK + col) * D4;
-#pragma unroll
-                                    for (int g = 0; g < D4 / G; ++g)
-                                        reinterpret_cast<V*>(dst)[g] = *reinterpret_cast<V*>(&vals[g * G]);
-                                    if (last) mbar_arrive(&oful[ps]);
                                 }
                             }
                         }
@@ -511,14 +509,8 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                             bail = true;
                             break;
                         }
-                        if (last) {
-                            if (pub_remote)
-                                ++pc;
-                            else
-                                ++oc;
-                        }
+                        if (last) ++pc;
                     }
-                    __syncwarp();
                 }
                 // the slot's results are visible to the helper's bulk store
                 fence_proxy_async_smem();
@@ -551,7 +543,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
             int* prog_out = a.progress + task;
             const RT* xsrc = reinterpret_cast<const RT*>(a.xfer) + (long long)(task > 0 ? task - 1 : 0) * a.xstride;
             RT* xdst = reinterpret_cast<RT*>(a.xfer) + (long long)task * a.xstride;
-            const unsigned rc0 = rc, xc0 = xc, oc0 = oc;
+            const unsigned rc0 = rc, xc0 = xc, pc0 = pc;
             int nl = 0, nst = 0, hin = 0, hout = 0;
             long long idle = 0;
             bool bail = false;
@@ -603,7 +595,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                 }
                 // this task's top row, published to the task above
                 if (pub_global && hout < nxc) {
-                    const unsigned g = oc0 + hout, hs = g % HS;
+                    const unsigned g = pc0 + hout, hs = g % HS;
                     int rd = 0;
                     if (lane == 0) rd = mbar_test_wait(&oful[hs], (g / HS) & 1u) ? 1 : 0;
                     if (__shfl_sync(0xffffffffu, rd, 0)) {
@@ -638,7 +630,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
             __syncwarp();
             rc = rc0 + nch;
             if (gin) xc = xc0 + nxc;
-            if (pub_global) oc = oc0 + nxc;
+            if (pub_global) pc = pc0 + nxc;
         }
         cluster_sync();  // the task is done in every CTA of the cluster
     }
