@@ -204,6 +204,66 @@ def gen_cond(g, grid_path, aboutnv):
     for name in ("fetchMPI.py", "mod_cond.py", "out_cond.py", "read_plot3d.py", "set_cond_var.py", "gen_cond.py"):
         if os.path.exists(g.path(name)):
             os.remove(g.path(name))
+    return tsm
+
+
+SIDES = ("SCFD_SIDE_ILO", "SCFD_SIDE_IHI", "SCFD_SIDE_JLO", "SCFD_SIDE_JHI")
+
+
+def gpu_files(g, sel, tsm, val_dt):
+    """The GPU architecture's generated files: scfd_gpu_driver.f90 with the
+    selections of checkout.inp, scfd_gpu_chem.f90 for the thermal model, and
+    scfd_gpu_bc.raw.f90, the boundary-descriptor template the user completes
+    into scfd_gpu_bc.f90 as condition.raw.f90 is completed into condition.f90."""
+    muscl = sel["recon"] == 1
+    fromto = [("GPU_MUSCL_USE", "use half_value, only: phi_mus, k_mus" if muscl else ""),
+              ("GPU_DIM", "0" if sel["dimension"] == "2d" else "1"),
+              ("GPU_DT_MODE", str(val_dt)),
+              ("GPU_SCHEME", str(sel["time_scheme"])),
+              ("GPU_RECON", str(sel["recon"])),
+              ("GPU_VISCOUS", str(sel["viscous"])),
+              ("GPU_THERMO", str(sel["thermal_model"])),
+              ("GPU_PHI", "phi_mus" if muscl else "0d0"),
+              ("GPU_KAPPA", "1.4d0"), ("GPU_RGAS", "287d0"), ("GPU_NU", "1.6d-5"),
+              ("GPU_K", "k_mus" if muscl else "0d0")]
+    g.raw2pro("scfd_gpu_driver.raw.f90", "scfd_gpu_driver.f90", fromto)
+    keep = "scfd_gpu_chem.chemkin.f90" if sel["thermal_model"] in (1, 2) else "scfd_gpu_chem.none.f90"
+    for name in ("scfd_gpu_chem.chemkin.f90", "scfd_gpu_chem.none.f90"):
+        if name == keep:
+            os.replace(g.path(name), g.path("scfd_gpu_chem.f90"))
+        else:
+            os.remove(g.path(name))
+    ranges = []
+    for p, sides in enumerate(tsm):
+        for cind in range(2):
+            for lu in range(2):
+                for a, b in sides[cind][lu]:
+                    ranges.append((p + 1, SIDES[2 * cind + lu], a, b))
+    lines = ["! Boundary descriptors of this case for scfd_set_bc: one per side range that",
+             "! no block interface covers (the ranges of condition.raw.f90).  Every entry",
+             "! starts as zero gradient (SCFD_BC_EXTRAP); set kind and value(:) to what the",
+             "! matching lines of condition.f90 write into the ghost cells (the SCFD_BC_*",
+             "! kinds of include/scfd_b200.h), then save this file as scfd_gpu_bc.f90.",
+             "module scfd_gpu_bc",
+             "   use iso_c_binding",
+             "   use scfd_b200_iface",
+             "   implicit none",
+             "contains",
+             "   subroutine scfd_gpu_bc_set(ctx)",
+             "      type(c_ptr),intent(in)::ctx"]
+    if ranges:
+        lines += ["      type(scfd_bc)::b(%d)" % len(ranges),
+                  "      integer(c_int)::ierr"]
+        for k, (p, side, a, b) in enumerate(ranges):
+            lines.append("      b(%d) = scfd_bc(%d, %s, %d, %d, SCFD_BC_EXTRAP, 0, 0d0)" % (k + 1, p, side, a, b))
+        lines += ["      ierr = scfd_set_bc(ctx, b, %d)" % len(ranges),
+                  "      if(ierr .ne. 0) then",
+                  "         print *,\"Error: scfd_set_bc returned status \",ierr",
+                  "         stop",
+                  "      end if"]
+    lines += ["   end subroutine scfd_gpu_bc_set", "end module scfd_gpu_bc", ""]
+    with open(g.path("scfd_gpu_bc.raw.f90"), "w") as fh:
+        fh.write("\n".join(lines))
 
 
 # ---- store/checkout/checkout_flow.py ---------------------------------------
@@ -305,6 +365,7 @@ def checkout_flow(root=".", inp="checkout.inp", log=print):
         if val not in (0, 1):
             raise CheckoutError("Odd Input at high order scheme! value is %d" % val)
         g.engage("high_order/" + ("upwind" if val == 0 else "muscl"))
+        recon = val
 
         log("***viscosity***")
         val_vis = read_control_next_int(fp, "viscosity")
@@ -345,6 +406,12 @@ def checkout_flow(root=".", inp="checkout.inp", log=print):
         else:
             raise CheckoutError("Odd Input at thermal model! value is %d" % val)
 
+    if sel["architecture"] == "GPU":
+        if sel["time_scheme"] == 1:
+            raise CheckoutError("the GPU architecture has no two-step Runge-Kutta (time scheme 1)")
+        if sel["thermal_model"] not in (0, 1, 2):
+            raise CheckoutError("the GPU architecture takes the ideal-gas and Chemkin thermal models (0-2)")
+    sel.update(viscous=val_vis, recon=recon)
     if val_vis == 0:
         g.engage("viscosity/non-viscous")
     else:
@@ -353,7 +420,9 @@ def checkout_flow(root=".", inp="checkout.inp", log=print):
     log("***generation of condition.raw.f90***")
     g.engage("cond/core")
     g.engage("cond/" + aboutnv)
-    gen_cond(g, gpath, aboutnv)
+    tsm = gen_cond(g, gpath, aboutnv)
+    if sel["architecture"] == "GPU":
+        gpu_files(g, sel, tsm, val_dt)
 
     # control.raw.inp, n_grid.f90, Makefile, main.f90 (checkout_flow.py:340-398)
     with open(g.path("control.raw.inp"), "w") as fh:

@@ -122,6 +122,11 @@ __device__ __forceinline__ void mbar_arrive_cluster(unsigned rbar) {
 __device__ __forceinline__ void mbar_arrive_cluster_relaxed(unsigned rbar) {
     asm volatile("mbarrier.arrive.relaxed.cluster.shared::cluster.b64 _, [%0];" ::"r"(rbar) : "memory");
 }
+// arrive with an expected transaction count on another CTA's mbarrier, no fence
+__device__ __forceinline__ void mbar_arrive_expect_tx_cluster_relaxed(unsigned rbar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.relaxed.cluster.shared::cluster.b64 _, [%0], %1;" ::"r"(rbar), "r"(bytes)
+                 : "memory");
+}
 // bulk copy from this CTA's shared memory into another CTA's (shared::cluster
 // address), completing `bytes` of transaction count on the receiver's mbarrier
 __device__ __forceinline__ void bulk_s2dsmem(unsigned rdst, const void* src, unsigned bytes, unsigned rbar) {

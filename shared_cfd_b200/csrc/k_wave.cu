@@ -246,10 +246,13 @@ __device__ __forceinline__ bool aborted(const View& v, const int* s_bail) {
     return *reinterpret_cast<const volatile int*>(s_bail) != 0 ||
            *reinterpret_cast<const volatile unsigned long long*>(&v.sc->spin_abort) != 0ull;
 }
-// bounded wait on a phase of a local mbarrier (cluster-scope acquire)
+// bounded wait on a phase of a local mbarrier.  Every phase these kernels wait
+// for completes on the waiting CTA's own barrier (bulk-copy transaction counts,
+// or arrivals that carry no data the waiter reads), so CTA-scope acquire is
+// enough.
 __device__ __forceinline__ bool wait_phase(unsigned long long* bar, unsigned par, const View& v, const int* s_bail) {
     long long spins = 0;
-    while (!mbar_try_wait_cluster(bar, par)) {
+    while (!mbar_try_wait(bar, par)) {
         if (++spins > kSpin || ((spins & 1023) == 0 && aborted(v, s_bail))) return false;
     }
     return true;
@@ -275,7 +278,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(xout + HS * HK * D4);
     unsigned long long* rfull = bars;          // record slot loaded (helper: expect_tx + bulk copies)
     unsigned long long* rdone = bars + PFB;    // record slot computed (compute warp arrive)
-    unsigned long long* xfull = bars + 2 * PFB;  // hand-off chunk arrived (armed by the consumer)
+    unsigned long long* xfull = bars + 2 * PFB;  // hand-off chunk arrived (producer's arrival + bytes)
     unsigned long long* pempty = xfull + HS;   // successor consumed a chunk this CTA produced
     unsigned long long* hempty = pempty + HS;  // this CTA consumed a chunk its helper fetched
     unsigned long long* oful = hempty + HS;    // xout chunk written (compute lane 31)
@@ -292,9 +295,6 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
         mbar_init_fence();
     }
     __syncthreads();
-    // every hand-off chunk is armed for its first use before any producer can write
-    if (threadIdx.x == 0)
-        for (int k = 0; k < HS; ++k) mbar_arrive_expect_tx(&xfull[k], CHUNK_BYTES);
     cluster_sync();
 
     const bool nr = v.scheme == SCFD_SCHEME_NR;
@@ -389,12 +389,9 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                         inB[k] = lane == 0 ? (in_col ? xi[k] : RT(0)) : sh;
                     }
                     if (in_col && ((t % HK) == HK - 1 || t == ni - 1)) {
-                        if (lane == 0) {
-                            mbar_arrive_expect_tx(&xfull[hs], CHUNK_BYTES);  // its next use
-                            // the chunk is refilled 16 chunks later, long after lane 0's
-                            // reads of it completed: no release fence needed
-                            mbar_arrive_cluster_relaxed(rel + hs * 8u);
-                        }
+                        // the chunk is refilled 16 chunks later, long after lane 0's reads
+                        // of it completed: no release fence needed
+                        if (lane == 0) mbar_arrive_cluster_relaxed(rel + hs * 8u);
                         ++xc;
                     }
                     // this lane's cell
@@ -494,8 +491,11 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                                     reinterpret_cast<V*>(dst)[g] = *reinterpret_cast<V*>(&vals[g * G]);
                                 if (last) {
                                     if (pub_remote) {
-                                        // columns past ni of a partial last chunk travel as they are
+                                        // the chunk's phase of the receiver's barrier completes with
+                                        // this arrival and the copy's bytes, in either order; columns
+                                        // past ni of a partial last chunk travel as they are
                                         fence_proxy_async_smem();
+                                        mbar_arrive_expect_tx_cluster_relaxed(dfull + ps * 8u, CHUNK_BYTES);
                                         bulk_s2dsmem(dring + ps * CHUNK_BYTES, xout + ps * HK * D4, CHUNK_BYTES,
                                                      dfull + ps * 8u);
                                     } else {
@@ -584,6 +584,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                         const bool free = g < HS || mbar_test_wait(&hempty[hs], ((g / HS) - 1u) & 1u);
                         if (free && ld_acquire_gpu(prog_in) >= hin + 1) {
                             fence_proxy_async_global();
+                            mbar_expect_tx(&xfull[hs], CHUNK_BYTES);
                             tma_bulk_g2s(xin + hs * HK * D4, xsrc + (long long)hin * HK * D4, CHUNK_BYTES, &xfull[hs]);
                             go = 1;
                         }
