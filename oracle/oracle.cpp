@@ -695,114 +695,58 @@ void track_ignition(Ignition& g, double tt, double T) {
     g.t_old = t;
 }
 
-// CHEMEQ2 tolerance y*rtol + rtol*1e-5 for the species (sub_chem.f90:1801), rtol*T for T
-double be_weight(int i, int ns, double yi, double rtol) {
-    return i < ns ? std::fabs(yi) * rtol + rtol * 1e-5 : std::fabs(yi) * rtol;
-}
+#include "dvode.h"
 
-bool lu_factor(double* M, int* piv, int N) {
-    for (int k = 0; k < N; ++k) {
-        int pk = k;
-        double best = std::fabs(M[k * N + k]);
-        for (int i = k + 1; i < N; ++i)
-            if (std::fabs(M[i * N + k]) > best) {
-                best = std::fabs(M[i * N + k]);
-                pk = i;
-            }
-        piv[k] = pk;
-        if (!(best > 0.0)) return false;
-        if (pk != k)
-            for (int j = 0; j < N; ++j) std::swap(M[k * N + j], M[pk * N + j]);
-        const double inv = 1.0 / M[k * N + k];
-        for (int i = k + 1; i < N; ++i) {
-            const double l = M[i * N + k] * inv;
-            M[i * N + k] = l;
-            for (int j = k + 1; j < N; ++j) M[i * N + j] = M[i * N + j] - l * M[k * N + j];
+// Rest of an interval after 10 CHEMEQ2 attempts, sub_chem.f90:1755-1775: DVODE
+// with MF = 21 on Fex and Jex (dvode.h) from (tt, y) to tout, rtol and atol
+// of control_chem.inp; ISTATE = -1 (MXSTEP steps taken before tout) restarts
+// it from where it stopped, at most max_recalc = 50 times
+// (mod_chem.raw.f90:27); any other failure is SCFD_E_CHEM (the reference
+// stops).  With `ign`, the ignition test runs after every accepted DVODE step.
+int dvode_rest(const scfd_chem& ch, double* y, double tt, double tout, long long& evals, Ignition* ign) {
+    const int N = ch.ns + 1;
+    struct Sys {
+        const scfd_chem& ch;
+        long long& evals;
+        int N;
+        void f(double, const double* yy, double* dy) {
+            fex_jex(ch, yy + 1, dy + 1, nullptr);
+            ++evals;
         }
-    }
-    return true;
-}
-
-void lu_solve(const double* M, const int* piv, int N, double* b) {
-    for (int k = 0; k < N; ++k)
-        if (piv[k] != k) std::swap(b[k], b[piv[k]]);
-    for (int i = 1; i < N; ++i)
-        for (int j = 0; j < i; ++j) b[i] = b[i] - M[i * N + j] * b[j];
-    for (int i = N - 1; i >= 0; --i) {
-        for (int j = i + 1; j < N; ++j) b[i] = b[i] - M[i * N + j] * b[j];
-        b[i] = b[i] / M[i * N + i];
-    }
-}
-
-// Rest of an interval after 10 CHEMEQ2 attempts (where sub_chem.f90:1755-1775
-// calls DVODE): substeps of the two-stage Rosenbrock method ROS2 (Verwer,
-// Spee, Blom, Hundsdorfer, SIAM J. Sci. Comput. 20, 1999), gamma = 1 + 1/sqrt(2),
-//     (I - gamma h J) k1 = f(y0),  (I - gamma h J) k2 = f(y0 + h k1) - 2 k1,
-//     y = y0 + 3/2 h k1 + 1/2 h k2,  error |h/2 (k1 + k2)|,
-// with f = Fex and J = Jex at y0 (the pair the reference hands DVODE, mf = 21)
-// and step factor 0.8/sqrt(err) in [0.2, 2].  y holds the accepted state at tt on entry and the state at tout
-// on return.  The same substeps as be_attempt of the CUDA path, in the same order.
-int implicit_rest(const scfd_chem& ch, double* y, double tt, double tout, double dt, double rtol,
-                  long long& attempts, int& substeps, int max_substeps, Ignition* ign, long long& evals,
-                  double& h_carry) {
-    const int ns = ch.ns, N = ns + 1;
-    const double gam = 1.7071067811865475;
-    double y0[SCFD_MAX_SPECIES + 1], f0[SCFD_MAX_SPECIES + 1], f[SCFD_MAX_SPECIES + 1],
-        k1[SCFD_MAX_SPECIES + 1], k2[SCFD_MAX_SPECIES + 1], M[(SCFD_MAX_SPECIES + 1) * (SCFD_MAX_SPECIES + 1)];
-    int piv[SCFD_MAX_SPECIES + 1];
-    for (int i = 0; i < N; ++i) y0[i] = y[i];
-    if (h_carry > 0.0) dt = h_carry;  // warm start from the previous call's last step
-    int rejects = 0;
+        void jac(double, const double* yy, dvode::State& s) {
+            double d[SCFD_MAX_SPECIES + 1], J[(SCFD_MAX_SPECIES + 1) * (SCFD_MAX_SPECIES + 1)];
+            fex_jex(ch, yy + 1, d, J);
+            ++evals;
+            for (int i = 0; i < N; ++i)
+                for (int j = 0; j < N; ++j) s.A(i + 1, j + 1) = J[i * N + j];
+        }
+    } sys{ch, evals, N};
+    dvode::State st;
+    double y1[SCFD_MAX_SPECIES + 2];
+    for (int i = 0; i < N; ++i) y1[i + 1] = y[i];
+    auto acc = [&](double tn, const double* yh1) {
+        if (ign) track_ignition(*ign, tn, yh1[N]);
+    };
+    double t = tt;
+    int nrecalc = 0;
     for (;;) {
-        ++attempts;
-        double h = dt;
-        if (tout - tt < h) h = tout - tt;
-        // M = I - gamma h J with Jex's exact Jacobian at y0; f0 = Fex(y0) (Jex's dndt)
-        fex_jex(ch, y0, f0, M);
-        for (int i = 0; i < N; ++i)
-            for (int j = 0; j < N; ++j) M[i * N + j] = (i == j ? 1.0 : 0.0) - gam * h * M[i * N + j];
-        double err = 1e300;
-        if (lu_factor(M, piv, N)) {
-            for (int i = 0; i < N; ++i) k1[i] = f0[i];
-            lu_solve(M, piv, N, k1);
-            for (int i = 0; i < N; ++i) y[i] = y0[i] + h * k1[i];
-            fex_jex(ch, y, f, nullptr);
-            for (int i = 0; i < N; ++i) k2[i] = f[i] - 2.0 * k1[i];
-            lu_solve(M, piv, N, k2);
-            err = 0.0;
-            for (int i = 0; i < N; ++i) {
-                y[i] = y0[i] + 1.5 * h * k1[i] + 0.5 * h * k2[i];
-                const double e = std::fabs(0.5 * h * (k1[i] + k2[i])) / be_weight(i, ns, y[i], rtol);
-                err = (e > err || e != e) ? e : err;
-            }
-        }
-        evals += 2;
-        if (!(err <= 1.0)) {
-            dt = h * (err == err && err < 1e300 ? std::max(0.2, 0.8 / std::sqrt(err)) : 0.25);
-            if (++rejects > 30) return SCFD_E_CHEM;
-            continue;
-        }
-        rejects = 0;
-        tt = tt + h;
-        for (int i = 0; i < N; ++i) y0[i] = y[i];
-        dt = h * std::min(2.0, std::max(0.2, 0.8 / std::sqrt(std::max(err, 1e-10))));
-        h_carry = dt;
-        if (ign) track_ignition(*ign, tt, y[ns]);
-        if (tout <= tt) return 0;
-        if (++substeps > max_substeps) return SCFD_E_CHEM;
+        const int istate = dvode::solve(st, sys, N, y1, t, tout, ch.rtol, ch.atol, acc);
+        if (istate > 0) break;
+        if (istate == -1 && ++nrecalc <= 50) continue;
+        for (int i = 0; i < N; ++i) y[i] = y1[i + 1];
+        return SCFD_E_CHEM;
     }
+    for (int i = 0; i < N; ++i) y[i] = y1[i + 1];
+    return 0;
 }
 
 // chemeq2, sub_chem.f90:1714-1819; returns 0, or SCFD_E_CHEM.  With `ign`,
 // the ignition test runs after every accepted substep; `evals` counts the
 // source-term evaluations.
 int chemeq2(const scfd_chem& ch, double* y, double tt, double tout, double rtol, long long& attempts,
-            bool& fell_back, int max_substeps, Ignition* ign = nullptr, long long* evals = nullptr,
-            double* h_carry = nullptr) {
+            bool& fell_back, int max_substeps, Ignition* ign = nullptr, long long* evals = nullptr) {
     long long ev_local = 0;
     long long& ev = evals ? *evals : ev_local;
-    double hc_local = 0.0;
-    double& hc = h_carry ? *h_carry : hc_local;
     const int ns = ch.ns;
     double y0[SCFD_MAX_SPECIES + 1], yp[SCFD_MAX_SPECIES + 1], p[SCFD_MAX_SPECIES + 1], q[SCFD_MAX_SPECIES + 1],
         p0[SCFD_MAX_SPECIES + 1], q0[SCFD_MAX_SPECIES + 1];
@@ -817,12 +761,11 @@ int chemeq2(const scfd_chem& ch, double* y, double tt, double tout, double rtol,
         for (;;) {
             for (int i = 0; i <= ns; ++i) y[i] = y0[i];
             countersum = countersum + 1;
-            // Reference: after 10 attempts the rest of the interval goes to DVODE
-            // (sub_chem.f90:1755-1775); here to the Rosenbrock substeps of
-            // implicit_rest (shared with the CUDA path), and the cell is counted.
+            // after 10 attempts the rest of the interval goes to DVODE
+            // (sub_chem.f90:1755-1775); the cell is counted
             if (countersum > 10) {
                 fell_back = true;
-                return implicit_rest(ch, y, tt, tout, dt, rtol, attempts, substeps, max_substeps, ign, ev, hc);
+                return dvode_rest(ch, y, tt, tout, ev, ign);
             }
             ++attempts;
             ev += 2;
@@ -2735,7 +2678,6 @@ int orc_reactors_launch(orc_reactors* r, const scfd_reactor_desc* d) {
         y[ns] = r->T0[k];
         Ignition g{r->T0[k], d->dT_ign, 0.0, r->T0[k], -1.0, false, 0.0};
         long long att = 0, ev = 0;
-        double hc = 0.0;  // Rosenbrock step carried from call to call
         bool fb = false, any_fb = false;
         int rc = 0;
         // successive reaction_chemeq2 calls over dt_call: moles floored at n_eps
@@ -2745,7 +2687,7 @@ int orc_reactors_launch(orc_reactors* r, const scfd_reactor_desc* d) {
             const double rest = d->t_end - tg;
             const double tout = (d->dt_call > 0.0 && d->dt_call < rest) ? d->dt_call : rest;
             g.t_off = tg;
-            rc = chemeq2(ch, y, 0.0, tout, ch.rtol, att, fb, maxsub, &g, &ev, &hc);
+            rc = chemeq2(ch, y, 0.0, tout, ch.rtol, att, fb, maxsub, &g, &ev);
             any_fb = any_fb || fb;
             if (rc) break;
             tg = tg + tout;

@@ -14,10 +14,10 @@
 //
 // A task is up to 8 consecutive strips of one plane, run by one thread-block
 // cluster of 8 CTAs (CTA rank r on the task's strip r).  Strip r's lane 31
-// stages its row in its own shared memory and, every HK columns, one bulk copy
-// moves the chunk into CTA r + 1's hand-off ring (distributed shared memory),
-// completing a transaction count on an mbarrier of the receiving CTA; the
-// receiver releases each chunk with a remote arrive.  A task with a successor
+// stages its row in its own shared memory; every HK columns the helper warp
+// moves the chunk with one bulk copy into CTA r + 1's hand-off ring
+// (distributed shared memory), completing a transaction count on an mbarrier
+// of the receiving CTA; the receiver releases each chunk with a remote arrive.  A task with a successor
 // holds 8 strips, so only rank 7 ever publishes to global memory and ranks
 // 0-6 only to the next CTA.  Between tasks of one plane the
 // top row travels through global memory: the last CTA's helper warp copies it
@@ -29,8 +29,8 @@
 // Each CTA has one compute warp and one helper warp.  The compute warp does
 // the wavefront only: no global loads, stores or fences in its step loop.  The
 // helper streams the strip's records through a ring of PFB slots (bulk copies
-// completing on mbarriers), writes the results back with bulk stores, and runs
-// the global hand-offs.  Every wait is bounded; a wait that gives up sets
+// completing on mbarriers), writes the results back with bulk stores, and moves
+// the hand-off chunks on (to the next CTA, or through global memory).  Every wait is bounded; a wait that gives up sets
 // SCFD_E_SPIN and the kernel winds down instead of hanging.
 //
 // Records (k_pack, in the cell order of the sweep):
@@ -343,8 +343,6 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
             const int lf = DIR == 0 ? lane : 31 - lane;  // this lane's slot in a step block
             // consumed chunks are released to the producer: the CTA below (remote) or this CTA's helper
             const unsigned rel = rank > 0 ? mapa(pempty, rank - 1) : mapa(hempty, rank);
-            const unsigned dring = pub_remote ? mapa(xin, rank + 1) : 0u;
-            const unsigned dfull = pub_remote ? mapa(xfull, rank + 1) : 0u;
             RT outA[D], outB[D];
 #pragma unroll
             for (int k = 0; k < D; ++k) {
@@ -489,18 +487,11 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
 #pragma unroll
                                 for (int g = 0; g < D4 / G; ++g)
                                     reinterpret_cast<V*>(dst)[g] = *reinterpret_cast<V*>(&vals[g * G]);
+                                // a whole chunk goes on to the helper, which moves it to the
+                                // next CTA (bulk copy) or to global memory
                                 if (last) {
-                                    if (pub_remote) {
-                                        // the chunk's phase of the receiver's barrier completes with
-                                        // this arrival and the copy's bytes, in either order; columns
-                                        // past ni of a partial last chunk travel as they are
-                                        fence_proxy_async_smem();
-                                        mbar_arrive_expect_tx_cluster_relaxed(dfull + ps * 8u, CHUNK_BYTES);
-                                        bulk_s2dsmem(dring + ps * CHUNK_BYTES, xout + ps * HK * D4, CHUNK_BYTES,
-                                                     dfull + ps * 8u);
-                                    } else {
-                                        mbar_arrive(&oful[ps]);
-                                    }
+                                    fence_proxy_async_smem();
+                                    mbar_arrive(&oful[ps]);
                                 }
                             }
                         }
@@ -547,7 +538,9 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
             int nl = 0, nst = 0, hin = 0, hout = 0;
             long long idle = 0;
             bool bail = false;
-            while (!bail && (nst < nch || (gin && hin < nxc) || (pub_global && hout < nxc))) {
+            const unsigned dring = pub_remote ? mapa(xin, rank + 1) : 0u;
+            const unsigned dfull = pub_remote ? mapa(xfull, rank + 1) : 0u;
+            while (!bail && (nst < nch || (gin && hin < nxc) || ((pub_remote || pub_global) && hout < nxc))) {
                 bool prog = false;
                 // record loads: the slot of chunk nl is free once chunk nl - PFB is stored
                 if (nl < nch && nl - PFB < nst) {
@@ -594,6 +587,23 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                         prog = true;
                     }
                 }
+                // this CTA's top row into the next CTA's xin: the chunk's phase of the
+                // receiver's barrier completes with this arrival and the copy's bytes, in
+                // either order; columns past ni of a partial last chunk travel as they are
+                if (pub_remote && hout < nxc) {
+                    const unsigned g = pc0 + hout, hs = g % HS;
+                    int rd = 0;
+                    if (lane == 0) rd = mbar_test_wait(&oful[hs], (g / HS) & 1u) ? 1 : 0;
+                    if (__shfl_sync(0xffffffffu, rd, 0)) {
+                        if (lane == 0) {
+                            fence_proxy_async_smem();
+                            mbar_arrive_expect_tx_cluster_relaxed(dfull + hs * 8u, CHUNK_BYTES);
+                            bulk_s2dsmem(dring + hs * CHUNK_BYTES, xout + hs * HK * D4, CHUNK_BYTES, dfull + hs * 8u);
+                        }
+                        ++hout;
+                        prog = true;
+                    }
+                }
                 // this task's top row, published to the task above
                 if (pub_global && hout < nxc) {
                     const unsigned g = pc0 + hout, hs = g % HS;
@@ -631,7 +641,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
             __syncwarp();
             rc = rc0 + nch;
             if (gin) xc = xc0 + nxc;
-            if (pub_global) pc = pc0 + nxc;
+            if (pub_remote || pub_global) pc = pc0 + nxc;
         }
         cluster_sync();  // the task is done in every CTA of the cluster
     }
