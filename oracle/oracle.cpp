@@ -2608,6 +2608,63 @@ int orc_fex_var(const scfd_chem* ch, const double* n, double* p, double* m) {
     return 0;
 }
 
+// DVODE (dvode.h) on test problems with known solutions, through the
+// reference's driver loop (restart on ISTATE = -1): problem 0 is the linear
+// system y' = A y (A row-major n x n), problem 1 Robertson's kinetics
+// (n = 3).  y: the state at t0 on entry, at tout on return.  Returns the
+// final ISTATE; *nst the accepted steps over all restarts.
+int orc_dvode_test(int problem, int n, const double* A, double* y, double t0, double tout, double rtol,
+                   double atol, int64_t* nst) {
+    if (n < 1 || n > SCFD_MAX_SPECIES + 1 || (problem == 1 && n != 3) || (problem == 0 && !A)) return -99;
+    struct Sys {
+        int problem, n;
+        const double* A;
+        void f(double, const double* yy, double* dy) {
+            if (problem == 0) {
+                for (int i = 0; i < n; ++i) {
+                    double a = 0.0;
+                    for (int j = 0; j < n; ++j) a += A[i * n + j] * yy[j + 1];
+                    dy[i + 1] = a;
+                }
+            } else {
+                dy[1] = -0.04 * yy[1] + 1.0e4 * yy[2] * yy[3];
+                dy[3] = 3.0e7 * yy[2] * yy[2];
+                dy[2] = -dy[1] - dy[3];
+            }
+        }
+        void jac(double, const double* yy, dvode::State& s) {
+            if (problem == 0) {
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j < n; ++j) s.A(i + 1, j + 1) = A[i * n + j];
+            } else {
+                s.A(1, 1) = -0.04;
+                s.A(1, 2) = 1.0e4 * yy[3];
+                s.A(1, 3) = 1.0e4 * yy[2];
+                s.A(3, 1) = 0.0;
+                s.A(3, 2) = 6.0e7 * yy[2];
+                s.A(3, 3) = 0.0;
+                s.A(2, 1) = -s.A(1, 1) - s.A(3, 1);
+                s.A(2, 2) = -s.A(1, 2) - s.A(3, 2);
+                s.A(2, 3) = -s.A(1, 3) - s.A(3, 3);
+            }
+        }
+    } sys{problem, n, A};
+    dvode::State st;
+    double y1[SCFD_MAX_SPECIES + 2];
+    for (int i = 0; i < n; ++i) y1[i + 1] = y[i];
+    double t = t0;
+    int64_t steps = 0;
+    int istate = 0;
+    for (int recalc = 0; recalc <= 1000; ++recalc) {
+        istate = dvode::solve(st, sys, n, y1, t, tout, rtol, atol, [](double, const double*) {});
+        steps += st.nst;
+        if (istate != -1) break;
+    }
+    for (int i = 0; i < n; ++i) y[i] = y1[i + 1];
+    if (nst) *nst = steps;
+    return istate;
+}
+
 int orc_chemeq2(const scfd_chem* ch, double* y, double tout, int64_t* attempts, int* fell_back) {
     long long a = 0;
     bool fb = false;

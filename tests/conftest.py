@@ -22,7 +22,7 @@ def pytest_configure(config):
 
 
 def build_oracle():
-    srcs = [os.path.join(ROOT, "oracle", f) for f in ("oracle.cpp", "cea.cpp", "Makefile")]
+    srcs = [os.path.join(ROOT, "oracle", f) for f in ("oracle.cpp", "cea.cpp", "dvode.h", "Makefile")]
     srcs.append(os.path.join(ROOT, "include", "scfd_b200.h"))
     if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < max(os.path.getmtime(s) for s in srcs):
         subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
