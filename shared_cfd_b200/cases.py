@@ -273,7 +273,7 @@ def moving_state(st, u, v, D):
 
 
 def reacting_step(scale=1.0, seed=20240607, precision=abi.PREC_FP64, inner=20, dt=1e-7, mech_kw=None, trace=0.0,
-                  omega_max=0.1, checks="relaxed"):
+                  omega_max=0.1, checks="relaxed", wake="air"):
     """Axisymmetric backward-facing step with a central H2 jet.
 
     Blocks (x axial, r radial, axis r=0; at scale 1 the cell counts are exact):
@@ -293,7 +293,10 @@ def reacting_step(scale=1.0, seed=20240607, precision=abi.PREC_FP64, inner=20, d
     falls below 1e-3 or whose inner residual does not drop three orders stops
     with E_OMEGA / E_RESRATE as the reference stops; "relaxed" lowers Omega Min
     to 1e-8 and turns ResRateErr off (the impulsive start from the uniform
-    initial state needs both)."""
+    initial state needs both).
+    wake: "air" fills block 4 with air at rest; "premixed" with a
+    stoichiometric H2 / air mixture at rest at 1500 K, which ignites, so the
+    chemistry's intervals there run out of CHEMEQ2 attempts and go to DVODE."""
     n = lambda k: max(4, int(round(k * scale)))
     n512, n256 = n(512), n(256)
     h1, h, H, Lu, Lx = 0.005, 0.010, 0.020, 0.02, 0.04
@@ -332,7 +335,16 @@ def reacting_step(scale=1.0, seed=20240607, precision=abi.PREC_FP64, inner=20, d
     fill_all(case, 0, q_air, w_air, ox["vhi"])
     fill_all(case, 1, q_air, w_air, ox["vhi"])
     fill_all(case, 2, q_h2, w_h2, fu["vhi"])
-    fill_all(case, 3, q_rest, w_rest, ox["vhi"])
+    if wake == "premixed":
+        comp = CH.parse_control_chem(control_chem_text(1e5, 1500.0, {"H2": 2, "O2": 1, "N2": 3.76}, 1e5, 300.0,
+                                                       {"H2": 1}), m)
+        pre = CH.fuel_oxidizer(m, comp, ns)["o"]
+        q_pre, w_pre = moving_state(pre, 0.0, 0.0, D)
+        fill_all(case, 3, q_pre, w_pre, pre["vhi"])
+    elif wake == "air":
+        fill_all(case, 3, q_rest, w_rest, ox["vhi"])
+    else:
+        raise ValueError("wake must be 'air' or 'premixed'")
     air = list(w_air) + list(ox["vhi"])
     h2 = list(w_h2) + list(fu["vhi"])
     case.bcs = [

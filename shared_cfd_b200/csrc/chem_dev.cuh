@@ -1,8 +1,8 @@
 // chem_dev.cuh -- device restatement of the UV source terms Fex_var, Fex and
 // their exact Jacobian Jex (store/therm_lib/chemkin/uvhp/uv/FJ.f90:152-709) and
 // of one CHEMEQ2 attempt (store/therm_lib/chemkin/core/sub_chem.f90:1714-1819),
-// with the implicit substeps that take over where the reference calls DVODE;
-// shared by the flow chemistry kernel and the batched 0-D reactors.
+// one thread each; shared by the flow chemistry kernel and the batched 0-D
+// reactors (whose one-warp versions and DVODE are in chem_warp.cuh).
 #pragma once
 
 #include "scfd_internal.h"
@@ -393,131 +393,21 @@ struct Ceq {
     double y[kMaxSpecies + 1], y0[kMaxSpecies + 1];
     double tt, tout, dt, ratio, counter;
     int countersum, substeps;
-    bool fell_back;   // the implicit fallback took over (the reference calls DVODE here)
-    int rejects;      // consecutive rejected implicit substeps
+    bool fell_back;   // the interval went to DVODE (sub_chem.f90:1755-1775)
     long long evals;  // source-term evaluations
-    double h_carry;   // step proposed by the last accepted implicit substep (0: none), kept
-                      // across the reaction_chemeq2 calls of one 0-D reactor
 };
 
-// Weight of component i in the error norm: the CHEMEQ2 tolerance
-// y*rtol + rtol*1e-5 for the species (sub_chem.f90:1801), rtol*T for T.
-__device__ inline double be_weight(int i, int ns, double yi, double rtol) {
-    return i < ns ? fabs(yi) * rtol + rtol * 1e-5 : fabs(yi) * rtol;
-}
-
-// Dense LU with partial pivoting of the N x N row-major M; false if singular.
-__device__ inline bool lu_factor(double* M, int* piv, int N) {
-    for (int k = 0; k < N; ++k) {
-        int pk = k;
-        double best = fabs(M[k * N + k]);
-        for (int i = k + 1; i < N; ++i)
-            if (fabs(M[i * N + k]) > best) {
-                best = fabs(M[i * N + k]);
-                pk = i;
-            }
-        piv[k] = pk;
-        if (!(best > 0.0)) return false;
-        if (pk != k)
-            for (int j = 0; j < N; ++j) {
-                const double t = M[k * N + j];
-                M[k * N + j] = M[pk * N + j];
-                M[pk * N + j] = t;
-            }
-        const double inv = 1.0 / M[k * N + k];
-        for (int i = k + 1; i < N; ++i) {
-            const double l = M[i * N + k] * inv;
-            M[i * N + k] = l;
-            for (int j = k + 1; j < N; ++j) M[i * N + j] = M[i * N + j] - l * M[k * N + j];
-        }
-    }
-    return true;
-}
-
-// Solves L U x = P b in place (factors and row swaps of lu_factor).
-__device__ inline void lu_solve(const double* M, const int* piv, int N, double* b) {
-    for (int k = 0; k < N; ++k) {
-        const int pk = piv[k];
-        if (pk != k) {
-            const double t = b[k];
-            b[k] = b[pk];
-            b[pk] = t;
-        }
-    }
-    for (int i = 1; i < N; ++i)
-        for (int j = 0; j < i; ++j) b[i] = b[i] - M[i * N + j] * b[j];
-    for (int i = N - 1; i >= 0; --i) {
-        for (int j = i + 1; j < N; ++j) b[i] = b[i] - M[i * N + j] * b[j];
-        b[i] = b[i] / M[i * N + i];
-    }
-}
-
-// Implicit fallback substep: the two-stage Rosenbrock method ROS2 of Verwer,
-// Spee, Blom and Hundsdorfer (SIAM J. Sci. Comput. 20, 1999), L-stable, order
-// 2, with gamma = 1 + 1/sqrt(2):
-//     (I - gamma h J) k1 = f(y0),   (I - gamma h J) k2 = f(y0 + h k1) - 2 k1,
-//     y = y0 + 3/2 h k1 + 1/2 h k2,  error estimate |h/2 (k1 + k2)| (vs. y0 + h k1),
-// f = Fex and J = Jex at y0 (the pair the reference hands DVODE, mf = 21),
-// step factor 0.8/sqrt(err) in [0.2, 2].  Used for the rest of an interval once CHEMEQ2
-// has made 10 attempts (where sub_chem.f90:1755-1775 calls DVODE).
-// Returns 1 when the interval is done, 0 to continue, <0 error.
-__device__ inline int be_attempt(const DevChem& ch, Ceq& s, double rtol, int max_substeps, long long& attempts) {
-    const int ns = ch.ns, N = ns + 1;
-    const double gam = 1.7071067811865475;  // 1 + 1/sqrt(2)
-    double f0[kMaxSpecies + 1], f[kMaxSpecies + 1], k1[kMaxSpecies + 1], k2[kMaxSpecies + 1];
-    double M[(kMaxSpecies + 1) * (kMaxSpecies + 1)];
-    int piv[kMaxSpecies + 1];
-    ++attempts;
-    double h = s.dt;
-    if (s.tout - s.tt < h) h = s.tout - s.tt;
-    // M = I - gamma h J with Jex's exact Jacobian at y0; f0 = Fex(y0) (Jex's dndt)
-    dev_jex(ch, s.y0, f0, M);
-    for (int i = 0; i < N; ++i)
-        for (int j = 0; j < N; ++j) M[i * N + j] = (i == j ? 1.0 : 0.0) - gam * h * M[i * N + j];
-    double err = 1e300;
-    if (lu_factor(M, piv, N)) {
-        for (int i = 0; i < N; ++i) k1[i] = f0[i];
-        lu_solve(M, piv, N, k1);
-        for (int i = 0; i < N; ++i) s.y[i] = s.y0[i] + h * k1[i];
-        dev_fex(ch, s.y, f);
-        for (int i = 0; i < N; ++i) k2[i] = f[i] - 2.0 * k1[i];
-        lu_solve(M, piv, N, k2);
-        err = 0.0;
-        for (int i = 0; i < N; ++i) {
-            s.y[i] = s.y0[i] + 1.5 * h * k1[i] + 0.5 * h * k2[i];
-            const double e = fabs(0.5 * h * (k1[i] + k2[i])) / be_weight(i, ns, s.y[i], rtol);
-            err = (e > err || e != e) ? e : err;
-        }
-    }
-    s.evals += 2;
-    if (!(err <= 1.0)) {
-        s.dt = h * (err == err && err < 1e300 ? fmax(0.2, 0.8 / sqrt(err)) : 0.25);
-        if (++s.rejects > 30) return -SCFD_E_CHEM;
-        return 0;
-    }
-    s.rejects = 0;
-    s.tt = s.tt + h;
-    for (int i = 0; i < N; ++i) s.y0[i] = s.y[i];
-    s.dt = h * fmin(2.0, fmax(0.2, 0.8 / sqrt(fmax(err, 1e-10))));
-    s.h_carry = s.dt;
-    if (s.tout <= s.tt) return 1;
-    if (++s.substeps > max_substeps) return -SCFD_E_CHEM;
-    return 0;
-}
-
-// One attempt; returns 1 when the interval is done, 0 to continue, <0 error.
-// After 10 CHEMEQ2 attempts in an interval the rest of it goes to be_attempt.
+// One attempt; returns 1 when the interval is done, 0 to continue, <0 error,
+// 2 when 10 attempts are used up and the rest of the interval, from (tt, y0),
+// goes to DVODE (sub_chem.f90:1755-1775).
 __device__ inline int ceq_attempt(const DevChem& ch, Ceq& s, double rtol, int max_substeps, long long& attempts) {
-    if (s.fell_back) return be_attempt(ch, s, rtol, max_substeps, attempts);
     const int ns = ch.ns;
     double yp[kMaxSpecies + 1], p[kMaxSpecies + 1], q[kMaxSpecies + 1], p0[kMaxSpecies + 1], q0[kMaxSpecies + 1];
     for (int i = 0; i <= ns; ++i) s.y[i] = s.y0[i];
     s.countersum += 1;
     if (s.countersum > 10) {
         s.fell_back = true;
-        s.rejects = 0;
-        if (s.h_carry > 0.0) s.dt = s.h_carry;
-        return be_attempt(ch, s, rtol, max_substeps, attempts);
+        return 2;
     }
     ++attempts;
     s.evals += 2;

@@ -3,23 +3,24 @@
 // Each reactor is advanced by successive reaction_chemeq2 calls
 // (store/therm_lib/chemkin/core/sub_chem.f90:1684-1713) over dt_call up to
 // t_end, with the ignition delay of reaction_one_steps (sub_chem.f90:1467-1472)
-// taken after every accepted substep (CHEMEQ2, or the Rosenbrock substeps of
-// chem_dev.cuh after the fallback):
+// taken after every accepted substep (of CHEMEQ2, or of DVODE where an
+// interval goes to it after 10 CHEMEQ2 attempts, sub_chem.f90:1755-1775):
 //     if not ignited and T >= T0 + dT:  t_ign = t - (T - (T0 + dT)) / (T - T_old) * (t - t_old)
 // where (t_old, T_old) is the previous accepted substep (initially t = 0, T0).
 //
-// One warp integrates one reactor: every source-term evaluation spreads the
-// species thermo and the reaction rates over the lanes (the rates are summed
-// per species in Fex_var's order), the Rosenbrock substep's Jex spreads the
-// reactions' derivative rows over the lanes and sums them per species in
-// Jex's order, its LU works on rows across lanes, and the serial-order sums
-// and the triangular solves run on lane 0, so each step does the arithmetic of
-// the one-thread code (chem_dev.cuh) in the same order.
+// One warp integrates one reactor with the one-warp source terms and DVODE of
+// chem_warp.cuh.
 //
 // Work distribution (SCFD_REACTOR_QUEUE): reactors need very different numbers
 // of substeps, so one persistent launch has every warp pull reactors from a
-// device counter until none is left.  The launch (status and counter reset +
-// kernel) is captured in a CUDA graph at the first run and replayed afterwards.
+// device counter until none is left.  The batch lasts as long as its stiffest
+// reactors, so the queue hands them out first (longest job first): a key
+// kernel evaluates Fex at every reactor's initial state, a bitonic sort orders
+// the reactors by decreasing |dT/dt| there (the initial heat release, which
+// ranks the reactors' source-evaluation counts closely), and warps take
+// reactors in that order.  The order changes no result.  The launch (resets,
+// keys, sort, kernel) is captured in a CUDA graph at the first run and
+// replayed afterwards.
 // SCFD_REACTOR_PER_LAUNCH runs the same kernel once per reactor, as a loop
 // over single-reactor calls would.
 #include <cuda_runtime.h>
@@ -28,33 +29,11 @@
 #include <string>
 #include <vector>
 
-#include "chem_dev.cuh"
 #include "chem_tables.h"
+#include "chem_warp.cuh"
 #include "scfd_internal.h"
 
 namespace scfd {
-
-// Per-species contribution lists of the reaction rates, in the order in which
-// Fex_var (FJ.f90:301-453) accumulates them: entry 2*i + kind adds the forward
-// (kind 0) or reverse (kind 1) rate of reaction i; p lists the production
-// terms, m the destruction terms; mref[i] is the reaction whose third-body
-// term reaction i uses (-1: none yet).
-//
-// For Fex / Jex (FJ.f90:152-709), the net list of species j, n_ptr[j] ..
-// n_ptr[j+1], holds 2*i + 1 for every reactant slot of j in reaction i and
-// 2*i for every product slot, reactions in order and reactants first, as the
-// reference subtracts and adds Dr; dref[i] is the last reaction up to i that
-// sets dlnkdlnM (third-body or fall-off rate; -1: none yet).
-struct RateLists {
-    const int* p_ptr;  // [ns+1]
-    const int* p_ent;
-    const int* m_ptr;  // [ns+1]
-    const int* m_ent;
-    const int* mref;   // [nr]
-    const int* n_ptr;  // [ns+1]
-    const int* n_ent;
-    const int* dref;   // [nr]
-};
 
 struct ReactorArgs {
     int n, first, queue, max_substeps;
@@ -68,294 +47,32 @@ struct ReactorArgs {
     int* flags;
     unsigned long long* counter;
     int* status;
-    RateLists rl;
+    const int* order;     // queue position -> reactor
     int wstride;          // doubles of shared memory per warp
 };
 
-// Shared-memory arrays of one warp (one reactor); N = ns + 1.
-struct WarpMem {
-    double *y0, *y, *yp, *q0, *p0, *q, *p, *f0, *k1, *k2, *M;
-    double *mu, *e, *cv, *lm, *rf, *rr;
-    double *dmu, *dcv, *vm, *dl, *dr, *drdn;  // Jex: per-species T-derivatives, per-reaction terms
-    int* piv;
-    __device__ WarpMem(double* b, int N, int ns, int nr) {
-        y0 = b; y = y0 + N; yp = y + N; q0 = yp + N; p0 = q0 + N; q = p0 + N; p = q + N;
-        f0 = p + N; k1 = f0 + N; k2 = k1 + N; M = k2 + N;
-        mu = M + N * N; e = mu + ns; cv = e + ns; lm = cv + ns; rf = lm + nr; rr = rf + nr;
-        dmu = rr + nr; dcv = dmu + ns; vm = dcv + ns; dl = vm + nr; dr = dl + nr; drdn = dr + nr;
-        piv = reinterpret_cast<int*>(drdn + nr * N);
-    }
-};
-
-__host__ __device__ inline int warp_mem_doubles(int ns, int nr) {
-    const int N = ns + 1;
-    return 10 * N + N * N + 5 * ns + 6 * nr + nr * N + (N + 1) / 2 + 1;
-}
-
-// Fex_var of the state n (shared memory) by one warp: species thermo and
-// reaction rates across lanes, per-species sums in the serial order.
-__device__ __noinline__ void warp_fex(const DevChem& ch, const RateLists& rl, const double* n, double* dndtp, double* dndtm,
-                         WarpMem& w, int lane) {
-    const int ns = ch.ns, nr = ch.nr;
-    double sn = 0.0;
-    if (lane == 0)
-        for (int j = 0; j < ns; ++j) sn += n[j];
-    sn = __shfl_sync(0xffffffffu, sn, 0);
-    FexPre f;
-    fex_pre(f, n[ns], sn);
-    for (int j = lane; j < ns; j += 32) species_thermo(ch, j, f, w.mu[j], w.e[j], w.cv[j]);
-    for (int i = lane; i < nr; i += 32)
-        if (ch.exist_m[i]) w.lm[i] = third_body_logM(ch, i, n, f);
-    __syncwarp();
-    for (int i = lane; i < nr; i += 32) {
-        const int r = rl.mref[i];
-        reaction_rates(ch, i, n, f, r >= 0 ? w.lm[r] : 0.0, w.mu, w.rf[i], w.rr[i]);
-    }
-    __syncwarp();
-    for (int j = lane; j < ns; j += 32) {
-        double a = 0.0;
-        for (int k = rl.p_ptr[j]; k < rl.p_ptr[j + 1]; ++k) {
-            const int en = rl.p_ent[k];
-            a = a + ((en & 1) ? w.rr[en >> 1] : w.rf[en >> 1]);
-        }
-        dndtp[j] = a;
-        a = 0.0;
-        for (int k = rl.m_ptr[j]; k < rl.m_ptr[j + 1]; ++k) {
-            const int en = rl.m_ent[k];
-            a = a - ((en & 1) ? w.rr[en >> 1] : w.rf[en >> 1]);
-        }
-        dndtm[j] = a;
-    }
-    __syncwarp();
-    if (lane == 0) {
-        double de = 0.0, cv = 0.0;
-        for (int j = 0; j < ns; ++j) {
-            de = de + w.e[j] * (dndtp[j] + dndtm[j]);
-            cv = cv + w.cv[j] * n[j];
-        }
-        dndtp[ns] = fmax(-de * f.T / cv, 0.0);
-        dndtm[ns] = fmin(-de * f.T / cv, 0.0);
-    }
-    __syncwarp();
-}
-
-// Fex (J == nullptr) or Jex (FJ.f90:152-709) of the state n (shared memory)
-// by one warp: species thermo and reactions across lanes, the per-species
-// sums in the reference's serial order (net lists), the T row on lane j.
-// dndt[0..ns] and, for Jex, J (row-major N x N) are written to shared memory.
-__device__ __noinline__ void warp_jex(const DevChem& ch, const RateLists& rl, const double* n, double* dndt, double* J,
-                         WarpMem& w, int lane) {
-    const int ns = ch.ns, nr = ch.nr, N = ns + 1;
-    const bool jac = J != nullptr;
-    double sn = 0.0;
-    if (lane == 0)
-        for (int j = 0; j < ns; ++j) sn += n[j];
-    sn = __shfl_sync(0xffffffffu, sn, 0);
-    if (jac) sn = fmax(sn, 1e-300);
-    FexPre f;
-    fex_pre(f, n[ns], sn);
-    double cdmurt[7], cdcpr[7];
-    jex_pre(f.T, cdmurt, cdcpr);
-    for (int j = lane; j < ns; j += 32) species_thermo_d(ch, j, f, cdmurt, cdcpr, w.mu[j], w.dmu[j], w.e[j], w.cv[j], w.dcv[j]);
-    for (int i = lane; i < nr; i += 32)
-        if (ch.exist_m[i]) {
-            double tmp = f.sn;
-            const int nm = ch.numm[i];
-            for (int j = 0; j < nm; ++j) tmp = tmp + ch.men[i * ns + j] * n[ch.indm[i * ns + j]];
-            w.vm[i] = tmp;
-            w.lm[i] = (tmp == f.sn) ? f.logsn : log(tmp);
-        }
-    __syncwarp();
-    for (int i = lane; i < nr; i += 32) {
-        const int r = rl.mref[i];
-        double dl = 0.0;  // read only where this reaction sets it (dref)
-        reaction_jac(ch, i, n, f, r >= 0 ? w.lm[r] : 0.0, w.mu, w.dmu, dl, w.dr[i], w.drdn + i * N);
-        w.dl[i] = dl;
-    }
-    __syncwarp();
-    if (jac)
-        for (int i = lane; i < nr; i += 32)
-            if (ch.exist_m[i]) {
-                const int d = rl.dref[i];
-                reaction_jac_m(ch, i, w.dr[i], d >= 0 ? w.dl[d] : 0.0, w.vm[i], w.drdn + i * N);
-            }
-    __syncwarp();
-    for (int j = lane; j < ns; j += 32) {
-        double a = 0.0;
-        for (int k = rl.n_ptr[j]; k < rl.n_ptr[j + 1]; ++k) {
-            const int en = rl.n_ent[k];
-            a = (en & 1) ? a - w.dr[en >> 1] : a + w.dr[en >> 1];
-        }
-        dndt[j] = a;
-    }
-    if (jac)
-        for (int t = lane; t < ns * N; t += 32) {
-            const int j = t / N, c = t - j * N;
-            double a = 0.0;
-            for (int k = rl.n_ptr[j]; k < rl.n_ptr[j + 1]; ++k) {
-                const int en = rl.n_ent[k];
-                const double v = w.drdn[(en >> 1) * N + c];
-                a = (en & 1) ? a - v : a + v;
-            }
-            J[j * N + c] = a;
-        }
-    __syncwarp();
-    if (lane == 0) {
-        double de = 0.0, cv = 0.0, dcv = 0.0, t1 = 0.0, t2 = 0.0;
-        for (int j = 0; j < ns; ++j) {
-            if (jac) t1 = t1 + w.e[j] * J[j * N + ns];
-            de = de + w.e[j] * dndt[j];
-            dcv = dcv + w.cv[j] * dndt[j];
-            cv = cv + w.cv[j] * n[j];
-            t2 = t2 + w.dcv[j] * n[j];
-        }
-        dndt[ns] = -de * f.T / cv;
-        if (jac) J[ns * N + ns] = -(f.T * t1 + dcv + dndt[ns] * t2) / cv;
-    }
-    __syncwarp();
-    if (jac) {
-        double cv = 0.0;  // the same sum on every lane
-        for (int j = 0; j < ns; ++j) cv = cv + w.cv[j] * n[j];
-        for (int j = lane; j < ns; j += 32) {
-            double t = 0.0;
-            for (int k = 0; k < ns; ++k) t = t + w.e[k] * J[k * N + j];
-            J[ns * N + j] = -(f.T * t + dndt[ns] * w.cv[j]) / cv;
-        }
-    }
-    __syncwarp();
-}
-
-// NaN-propagating min / max over the warp (order-free: exact comparisons)
-__device__ inline double warp_min_nan(double v) {
-    for (int o = 16; o > 0; o >>= 1) {
-        const double u = __shfl_xor_sync(0xffffffffu, v, o);
-        v = (u < v || u != u) ? u : v;
-    }
-    return v;
-}
-__device__ inline double warp_max_nan(double v) {
-    for (int o = 16; o > 0; o >>= 1) {
-        const double u = __shfl_xor_sync(0xffffffffu, v, o);
-        v = (u > v || u != u) ? u : v;
-    }
-    return v;
-}
-
 // Scalars of one CHEMEQ2 call (uniform over the warp).
 struct CallState {
-    double tt, tout, dt, counter, h_carry;
-    int countersum, substeps, rejects;
+    double tt, tout, dt, counter;
+    int countersum, substeps;
     bool fell_back;
     long long evals;
 };
 
-// Rosenbrock substep (be_attempt of chem_dev.cuh) by one warp: Jex for the
-// matrix, Fex for the second stage.
-__device__ int warp_ros_attempt(const DevChem& ch, const RateLists& rl, WarpMem& w, CallState& s, double rtol,
-                                int max_substeps, int lane) {
-    const int ns = ch.ns, N = ns + 1;
-    const double gam = 1.7071067811865475;
-    double h = s.dt;
-    if (s.tout - s.tt < h) h = s.tout - s.tt;
-    // M = I - gamma h J with Jex's exact Jacobian at y0; f0 = Fex(y0) (Jex's dndt)
-    warp_jex(ch, rl, w.y0, w.f0, w.M, w, lane);
-    for (int t = lane; t < N * N; t += 32) {
-        const int i = t / N, j = t - i * N;
-        w.M[t] = (i == j ? 1.0 : 0.0) - gam * h * w.M[t];
-    }
-    __syncwarp();
-    // LU with partial pivoting: first largest pivot, rows eliminated across lanes
-    bool ok = true;
-    for (int k = 0; k < N && ok; ++k) {
-        int pk = k;
-        if (lane == 0) {
-            double best = fabs(w.M[k * N + k]);
-            for (int i = k + 1; i < N; ++i)
-                if (fabs(w.M[i * N + k]) > best) {
-                    best = fabs(w.M[i * N + k]);
-                    pk = i;
-                }
-            w.piv[k] = pk;
-            if (!(best > 0.0)) pk = -1;
-        }
-        pk = __shfl_sync(0xffffffffu, pk, 0);
-        if (pk < 0) {
-            ok = false;
-            break;
-        }
-        if (pk != k)
-            for (int j = lane; j < N; j += 32) {
-                const double t = w.M[k * N + j];
-                w.M[k * N + j] = w.M[pk * N + j];
-                w.M[pk * N + j] = t;
-            }
-        __syncwarp();
-        const double inv = 1.0 / w.M[k * N + k];
-        for (int i = k + 1 + lane; i < N; i += 32) {
-            const double l = w.M[i * N + k] * inv;
-            w.M[i * N + k] = l;
-            for (int j = k + 1; j < N; ++j) w.M[i * N + j] = w.M[i * N + j] - l * w.M[k * N + j];
-        }
-        __syncwarp();
-    }
-    double err = 1e300;
-    if (ok) {
-        if (lane == 0) {
-            for (int i = 0; i < N; ++i) w.k1[i] = w.f0[i];
-            lu_solve(w.M, w.piv, N, w.k1);
-        }
-        __syncwarp();
-        for (int i = lane; i < N; i += 32) w.y[i] = w.y0[i] + h * w.k1[i];
-        __syncwarp();
-        warp_jex(ch, rl, w.y, w.q, nullptr, w, lane);
-        if (lane == 0) {
-            for (int i = 0; i < N; ++i) w.k2[i] = w.q[i] - 2.0 * w.k1[i];
-            lu_solve(w.M, w.piv, N, w.k2);
-        }
-        __syncwarp();
-        double e = 0.0;
-        for (int i = lane; i < N; i += 32) {
-            w.y[i] = w.y0[i] + 1.5 * h * w.k1[i] + 0.5 * h * w.k2[i];
-            const double ei = fabs(0.5 * h * (w.k1[i] + w.k2[i])) / be_weight(i, ns, w.y[i], rtol);
-            e = (ei > e || ei != ei) ? ei : e;
-        }
-        err = warp_max_nan(e);
-    }
-    s.evals += 2;
-    __syncwarp();
-    if (!(err <= 1.0)) {
-        s.dt = h * (err == err && err < 1e300 ? fmax(0.2, 0.8 / sqrt(err)) : 0.25);
-        if (++s.rejects > 30) return -SCFD_E_CHEM;
-        return 0;
-    }
-    s.rejects = 0;
-    s.tt = s.tt + h;
-    for (int i = lane; i < N; i += 32) w.y0[i] = w.y[i];
-    __syncwarp();
-    s.dt = h * fmin(2.0, fmax(0.2, 0.8 / sqrt(fmax(err, 1e-10))));
-    s.h_carry = s.dt;
-    if (s.tout <= s.tt) return 1;
-    if (++s.substeps > max_substeps) return -SCFD_E_CHEM;
-    return 0;
-}
-
-// One attempt (ceq_attempt of chem_dev.cuh) by one warp.
-__device__ int warp_ceq_attempt(const DevChem& ch, const RateLists& rl, WarpMem& w, CallState& s, double rtol,
-                                int max_substeps, int lane) {
-    if (s.fell_back) return warp_ros_attempt(ch, rl, w, s, rtol, max_substeps, lane);
+// One attempt (ceq_attempt of chem_dev.cuh) by one warp; 2: the rest of the
+// interval goes to DVODE, from (tt, w.y).
+__device__ int warp_ceq_attempt(const DevChem& ch, WarpMem& w, CallState& s, double rtol, int max_substeps, int lane) {
     const int ns = ch.ns, N = ns + 1;
     for (int i = lane; i < N; i += 32) w.y[i] = w.y0[i];
     __syncwarp();
     s.countersum += 1;
     if (s.countersum > 10) {
         s.fell_back = true;
-        s.rejects = 0;
-        if (s.h_carry > 0.0) s.dt = s.h_carry;
-        return warp_ros_attempt(ch, rl, w, s, rtol, max_substeps, lane);
+        return 2;
     }
     s.evals += 2;
     const double dt = s.dt;
-    warp_fex(ch, rl, w.y, w.q0, w.p0, w, lane);
+    warp_fex(ch, w.y, w.q0, w.p0, w, lane);
     for (int i = lane; i < ns; i += 32) {
         const double p0 = -w.p0[i] / (w.y[i] + 1e-300);
         w.p0[i] = p0;
@@ -365,7 +82,7 @@ __device__ int warp_ceq_attempt(const DevChem& ch, const RateLists& rl, WarpMem&
     }
     if (lane == 0) w.yp[ns] = w.y0[ns] + dt * (w.q0[ns] + w.p0[ns]);
     __syncwarp();
-    warp_fex(ch, rl, w.yp, w.q, w.p, w, lane);
+    warp_fex(ch, w.yp, w.q, w.p, w, lane);
     double ratio = 1e300;
     for (int i = lane; i < ns; i += 32) {
         double p = -w.p[i] / (w.yp[i] + 1e-300);
@@ -417,7 +134,6 @@ __device__ void warp_call(const ReactorArgs& a, ReactorState& r, WarpMem& w, int
     r.s.substeps = 0;
     r.s.counter = 0.0;
     r.s.fell_back = false;
-    r.s.rejects = 0;
 }
 
 // Whole reactor k by one warp: successive reaction_chemeq2 calls over dt_call
@@ -430,7 +146,6 @@ __device__ void warp_reactor(const DevChem& ch, const ReactorArgs& a, WarpMem& w
     if (lane == 0) w.y[ns] = r.T0;
     __syncwarp();
     r.s.evals = 0;
-    r.s.h_carry = 0.0;
     r.tg = 0.0;
     r.t_old = 0.0;
     r.T_old = r.T0;
@@ -439,18 +154,26 @@ __device__ void warp_reactor(const DevChem& ch, const ReactorArgs& a, WarpMem& w
     r.fell_back = false;
     warp_call(a, r, w, N, lane);
     int rc = 0;
+    // the ignition test of an accepted substep ending at tt (of this call) with temperature T
+    auto track = [&](double tt, double T) {
+        const double t = r.tg + tt, Tig = r.T0 + a.dT;
+        if (!r.ignited && T >= Tig) {
+            r.t_ign = t - (T - Tig) / (T - r.T_old) * (t - r.t_old);
+            r.ignited = true;
+        }
+        r.T_old = T;
+        r.t_old = t;
+    };
+    auto on_dvode_step = [&](double tn) { track(tn, w.yh[ns]); };
     for (;;) {
         const double t_before = r.s.tt;
-        rc = warp_ceq_attempt(ch, a.rl, w, r.s, ch.rtol, a.max_substeps, lane);
+        rc = warp_ceq_attempt(ch, w, r.s, ch.rtol, a.max_substeps, lane);
         r.fell_back = r.fell_back || r.s.fell_back;
-        if (r.s.tt > t_before) {  // accepted substep
-            const double T = w.y[ns], t = r.tg + r.s.tt, Tig = r.T0 + a.dT;
-            if (!r.ignited && T >= Tig) {
-                r.t_ign = t - (T - Tig) / (T - r.T_old) * (t - r.t_old);
-                r.ignited = true;
-            }
-            r.T_old = T;
-            r.t_old = t;
+        if (rc == 2) {
+            // DVODE from (tt, w.y) to tout: the result in w.y
+            rc = warp_dvode_rest(ch, w, w.y, r.s.tt, r.s.tout, r.s.evals, lane, on_dvode_step) == 0 ? 1 : -SCFD_E_CHEM;
+        } else if (r.s.tt > t_before) {  // accepted substep
+            track(r.s.tt, w.y[ns]);
         }
         if (rc == 1) {
             r.tg = r.tg + r.s.tout;
@@ -507,7 +230,45 @@ __global__ void __launch_bounds__(128) k_reactors(DevChem ch, ReactorArgs a) {
         if (lane == 0) k = atomicAdd(a.counter, 1ull);
         k = __shfl_sync(0xffffffffu, k, 0);
         if (k >= (unsigned long long)a.n) break;
-        warp_reactor(ch, a, w, (int)k, lane);
+        warp_reactor(ch, a, w, a.order[k], lane);
+    }
+}
+
+// Queue keys: -|dT/dt| of Fex at the initial state (ascending key = stiffest
+// first); positions n .. npow2-1 pad the sort with +inf.
+__global__ void k_reactor_keys(DevChem ch, ReactorArgs a, int npow2, double* key, int* idx) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= npow2) return;
+    double kv = __longlong_as_double(0x7FF0000000000000ll);
+    if (k < a.n) {
+        const int ns = ch.ns;
+        double y[kMaxSpecies + 1], f[kMaxSpecies + 1];
+        for (int j = 0; j < ns; ++j) y[j] = fmax(a.vrho0[(long long)k * ns + j] * ch.inv_mw[j] * 1e-3, 1e-40);
+        y[ns] = a.T0[k];
+        dev_fex(ch, y, f);
+        kv = -fabs(f[ns]);
+        if (kv != kv) kv = 0.0;
+    }
+    key[k] = kv;
+    idx[k] = k;
+}
+
+// One compare-exchange stage (size kk, distance j) of a bitonic sort of
+// (key, idx) ascending, ties by index.
+__global__ void k_bitonic_stage(double* key, int* idx, int npow2, int kk, int j) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npow2) return;
+    const int l = i ^ j;
+    if (l <= i) return;
+    const double ki = key[i], kl = key[l];
+    const int ii = idx[i], il = idx[l];
+    const bool gt = ki > kl || (ki == kl && ii > il);
+    const bool up = (i & kk) == 0;
+    if (gt == up) {
+        key[i] = kl;
+        key[l] = ki;
+        idx[i] = il;
+        idx[l] = ii;
     }
 }
 
@@ -525,8 +286,11 @@ struct scfd_reactors {
     int* flags = nullptr;
     int* status = nullptr;
     unsigned long long* counter = nullptr;
-    RateLists rl{};
+    double* qkey = nullptr;  // queue order: sort keys and reactor indices, npow2 each
+    int* qidx = nullptr;
+    int npow2 = 1;
     int wstride = 0;  // doubles of shared memory per warp
+    int wpb = 4;      // warps per block of the queued launch
     // graph of the queued launch, valid for the descriptor values it was captured with
     cudaGraphExec_t graph = nullptr;
     int graph_n = -1, graph_max = -1;
@@ -569,8 +333,8 @@ int enqueue(scfd_reactors* r, const scfd_reactor_desc* d) {
     a.flags = r->flags;
     a.counter = r->counter;
     a.status = r->status;
-    a.rl = r->rl;
     a.wstride = r->wstride;
+    a.order = r->qidx;
     const size_t wbytes = (size_t)r->wstride * sizeof(double);
     if (d->mode == SCFD_REACTOR_PER_LAUNCH) {
         RCK(cudaMemsetAsync(r->status, 0, sizeof(int), r->stream));
@@ -587,7 +351,7 @@ int enqueue(scfd_reactors* r, const scfd_reactor_desc* d) {
     // one warp per reactor, up to 16 warps per SM; beyond that the queue hands
     // each warp several reactors
     const long long warps = std::min<long long>(d->n, (long long)r->nsm * 16);
-    const unsigned blocks = (unsigned)((warps + 3) / 4);
+    const unsigned blocks = (unsigned)((warps + r->wpb - 1) / r->wpb);
     const bool reuse = r->graph && r->graph_n == d->n && r->graph_t_end == d->t_end && r->graph_dT == d->dT_ign &&
                        r->graph_max == a.max_substeps && r->graph_dt_call == d->dt_call;
     if (!reuse) {
@@ -599,7 +363,14 @@ int enqueue(scfd_reactors* r, const scfd_reactor_desc* d) {
         RCK(cudaStreamBeginCapture(r->stream, cudaStreamCaptureModeThreadLocal));
         cudaMemsetAsync(r->status, 0, sizeof(int), r->stream);
         cudaMemsetAsync(r->counter, 0, sizeof(unsigned long long), r->stream);
-        k_reactors<<<blocks, 128, 4 * wbytes, r->stream>>>(r->ch, a);
+        // the queue order: stiffest reactors first
+        int np2 = 1;
+        while (np2 < d->n) np2 <<= 1;
+        const unsigned sb = (unsigned)((np2 + 255) / 256);
+        k_reactor_keys<<<sb, 256, 0, r->stream>>>(r->ch, a, np2, r->qkey, r->qidx);
+        for (int kk = 2; kk <= np2; kk <<= 1)
+            for (int j = kk >> 1; j > 0; j >>= 1) k_bitonic_stage<<<sb, 256, 0, r->stream>>>(r->qkey, r->qidx, np2, kk, j);
+        k_reactors<<<blocks, 32 * r->wpb, r->wpb * wbytes, r->stream>>>(r->ch, a);
         RCK(cudaStreamEndCapture(r->stream, &g));
         const cudaError_t e = cudaGraphInstantiate(&r->graph, g, 0);
         cudaGraphDestroy(g);
@@ -615,7 +386,12 @@ int enqueue(scfd_reactors* r, const scfd_reactor_desc* d) {
         r->graph_dt_call = d->dt_call;
     }
     RCK(cudaGraphLaunch(r->graph, r->stream));
-    r->launches = 1;
+    // kernels in the graph: the keys, the sort stages, the reactors
+    int np2 = 1, stages = 0;
+    while (np2 < d->n) np2 <<= 1;
+    for (int kk = 2; kk <= np2; kk <<= 1)
+        for (int j = kk >> 1; j > 0; j >>= 1) ++stages;
+    r->launches = 2 + stages;
     return 0;
 }
 
@@ -643,51 +419,26 @@ int scfd_reactors_create(const scfd_chem* chem, int n_max, scfd_reactors** out) 
     cudaError_t e = cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(e);
     const size_t nn = (size_t)n_max, nv = nn * r->ns;
-    // per-species rate lists in the accumulation order of Fex_var (FJ.f90:301-453)
     const int ns = chem->ns, nr = chem->nr;
-    std::vector<int> pp(ns + 1, 0), mp(ns + 1, 0), np_(ns + 1, 0), pe, me, ne_, mref(nr > 0 ? nr : 1, -1),
-        dref(nr > 0 ? nr : 1, -1);
-    {
-        std::vector<std::vector<int>> pl(ns), ml(ns), nl(ns);
-        int last = -1, lastd = -1;
-        for (int i = 0; i < nr; ++i) {
-            if (chem->exist_m[i]) last = i;
-            mref[i] = last;
-            const int rs0 = chem->rstate[i][0], rs1 = chem->rstate[i][1];
-            if (rs1 >= 4 || (rs0 == 0 && (rs1 == 2 || rs1 == 3))) lastd = i;
-            dref[i] = lastd;
-            for (int k = 0; k < chem->numnu[i][0]; ++k) nl[chem->indnu[i][0][k]].push_back(2 * i + 1);
-            for (int k = 0; k < chem->numnu[i][1]; ++k) nl[chem->indnu[i][1][k]].push_back(2 * i);
-            const int nreac = chem->numnu[i][0], nprod = chem->numnu[i][1];
-            for (int k = 0; k < nreac; ++k) ml[chem->indnu[i][0][k]].push_back(2 * i);
-            for (int k = 0; k < nprod; ++k) pl[chem->indnu[i][1][k]].push_back(2 * i);
-            if (chem->rstate[i][0] == 0) {
-                for (int k = 0; k < nreac; ++k) pl[chem->indnu[i][0][k]].push_back(2 * i + 1);
-                for (int k = 0; k < nprod; ++k) ml[chem->indnu[i][1][k]].push_back(2 * i + 1);
-            }
-        }
-        for (int j = 0; j < ns; ++j) {
-            pe.insert(pe.end(), pl[j].begin(), pl[j].end());
-            me.insert(me.end(), ml[j].begin(), ml[j].end());
-            ne_.insert(ne_.end(), nl[j].begin(), nl[j].end());
-            pp[j + 1] = (int)pe.size();
-            mp[j + 1] = (int)me.size();
-            np_[j + 1] = (int)ne_.size();
-        }
-        if (pe.empty()) pe.push_back(0);
-        if (me.empty()) me.push_back(0);
-        if (ne_.empty()) ne_.push_back(0);
-    }
     r->wstride = (warp_mem_doubles(ns, nr) + 1) & ~1;
-    const int blk_smem = 4 * r->wstride * (int)sizeof(double);
-    if (blk_smem > 48 * 1024) {
-        e = cudaFuncSetAttribute(k_reactors, cudaFuncAttributeMaxDynamicSharedMemorySize, blk_smem);
+    // up to 4 warps per block, as many as the shared memory per block allows
+    int smem_max = 0;
+    cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int wbytes = r->wstride * (int)sizeof(double);
+    r->wpb = std::min(4, smem_max / wbytes);
+    if (r->wpb < 1) {
+        r->err = "mechanism too large for one warp's shared memory";
+        scfd_reactors_destroy(r);
+        return SCFD_E_ARG;
+    }
+    if (r->wpb * wbytes > 48 * 1024) {
+        e = cudaFuncSetAttribute(k_reactors, cudaFuncAttributeMaxDynamicSharedMemorySize, r->wpb * wbytes);
         if (e != cudaSuccess) return fail(e);
     }
     auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    while (r->npow2 < n_max) r->npow2 <<= 1;
     const size_t bytes = tabs.bytes() + 3 * al(nn * 8) + 2 * al(nv * 8) + al(nn * 8) + al(nn * 4) + 2 * 256 +
-                         2 * al(pp.size() * 4) + al(pe.size() * 4) + al(me.size() * 4) + al(mref.size() * 4) +
-                         al(np_.size() * 4) + al(ne_.size() * 4) + al(dref.size() * 4);
+                         al((size_t)r->npow2 * 8) + al((size_t)r->npow2 * 4);
     e = cudaMalloc(&r->arena, bytes);
     if (e != cudaSuccess) return fail(e);
     char* p = r->arena;
@@ -702,22 +453,8 @@ int scfd_reactors_create(const scfd_chem* chem, int n_max, scfd_reactors** out) 
     r->flags = carve_r<int>(p, nn);
     r->status = carve_r<int>(p, 1);
     r->counter = carve_r<unsigned long long>(p, 1);
-    int* dpp = carve_r<int>(p, pp.size());
-    int* dpe = carve_r<int>(p, pe.size());
-    int* dmp = carve_r<int>(p, mp.size());
-    int* dme = carve_r<int>(p, me.size());
-    int* dmr = carve_r<int>(p, mref.size());
-    int* dnp = carve_r<int>(p, np_.size());
-    int* dne = carve_r<int>(p, ne_.size());
-    int* ddr = carve_r<int>(p, dref.size());
-    for (auto cp : {std::make_pair(dpp, &pp), std::make_pair(dpe, &pe), std::make_pair(dmp, &mp),
-                    std::make_pair(dme, &me), std::make_pair(dmr, &mref), std::make_pair(dnp, &np_),
-                    std::make_pair(dne, &ne_), std::make_pair(ddr, &dref)}) {
-        e = cudaMemcpyAsync(cp.first, cp.second->data(), cp.second->size() * sizeof(int), cudaMemcpyHostToDevice,
-                            r->stream);
-        if (e != cudaSuccess) return fail(e);
-    }
-    r->rl = RateLists{dpp, dpe, dmp, dme, dmr, dnp, dne, ddr};
+    r->qkey = carve_r<double>(p, r->npow2);
+    r->qidx = carve_r<int>(p, r->npow2);
     if (p > r->arena + bytes) {
         r->err = "arena overflow";
         scfd_reactors_destroy(r);

@@ -56,6 +56,7 @@ struct scfd_ctx {
     Wave sw3{};
     // chemistry
     unsigned long long* d_counter = nullptr;
+    ChemQueue dq{};  // cells whose chemistry interval goes to DVODE
     // rms
     double* d_rms_partial = nullptr;
     double* d_rms_out = nullptr;
@@ -432,7 +433,8 @@ struct Seq {
         if (v.precision == SCFD_PREC_MIXED) n += timed(c, SCFD_K_OTHER, [&] { return launch_to_f32(v, s); });
     }
     void chem() {
-        n += timed(c, SCFD_K_CHEM, [&] { return launch_chem_impl(v, s, c->d.chem_max_substeps, c->d_counter, c->nsm); });
+        n += timed(c, SCFD_K_CHEM,
+                   [&] { return launch_chem_impl(v, s, c->d.chem_max_substeps, c->d_counter, c->nsm, c->dq); });
     }
     void setdt() { n += timed(c, SCFD_K_DT, [&] { return launch_set_dt(v, s); }); }
     void copyq(double* dst, const double* src) {
@@ -813,6 +815,11 @@ int scfd_commit(scfd_ctx* c) {
              need<double>(std::max<long long>(1, c->seg * c->nranks)) + need<double>(8);
     bytes += need<unsigned long long>(1) + need<double>(nrec) + need<double>(1);
     bytes += tabs.bytes();
+    long long dq_cap = 0;  // interior cells of the updated planes
+    for (int a = 0; a < c->P.nact; ++a) dq_cap += (long long)c->P.ni[c->P.act[a]] * c->P.nj[c->P.act[a]];
+    if (c->have_chem)
+        bytes += need<long long>(dq_cap) + need<double>(dq_cap) + need<double>((size_t)dq_cap * (c->chem.ns + 1)) +
+                 need<unsigned long long>(2);
     const size_t nref = (size_t)(c->nimax + 4) * (c->njmax + 4) * c->np;
     bytes += need<double>((size_t)std::max(std::max(W, D), nY) * nref);
     if (c->use_sw3)
@@ -866,6 +873,16 @@ int scfd_commit(scfd_ctx* c) {
     c->d_red = carve<double>(p, 8);
     c->d_bcval = carve<double>(p, std::max<size_t>(1, c->bcs.size()) * c->valstride);
     c->d_counter = carve<unsigned long long>(p, 1);
+    if (c->have_chem) {
+        c->dq.cell = carve<long long>(p, dq_cap);
+        c->dq.tt = carve<double>(p, dq_cap);
+        c->dq.y = carve<double>(p, (size_t)dq_cap * (c->chem.ns + 1));
+        c->dq.count = carve<unsigned long long>(p, 2);
+        c->dq.capacity = dq_cap;
+        c->dq.warp_doubles = (int)chem_dvode_warp_doubles(c->chem.ns, c->chem.nr);
+        const int e = chem_dvode_setup(c->chem.ns, c->chem.nr, &c->dq.warps_per_block);
+        if (e) return c->fail(SCFD_E_CUDA, std::string("DVODE kernel setup: ") + cudaGetErrorString((cudaError_t)e));
+    }
     c->d_rms_partial = carve<double>(p, nrec);
     c->d_rms_out = carve<double>(p, 1);
     c->d_ref = carve<double>(p, (size_t)std::max(std::max(W, D), nY) * nref);
@@ -1218,7 +1235,11 @@ int scfd_run(scfd_ctx* c, int step, int nsteps, scfd_stats* stats) {
     }
     if ((st = sync_scalars(c))) return st;
     collect_events(c);
-    return fill_stats(c, stats, att0, fb0);
+    // the chemistry counts of the last step (a run of no step reports none)
+    const DevScalars& h = *c->h_sc;
+    const bool any = nsteps > 0 && (h.chem_attempts != att0 || h.chem_fallback != fb0);
+    return fill_stats(c, stats, any ? h.chem_attempts - h.chem_attempts_last : h.chem_attempts,
+                      any ? h.chem_fallback - h.chem_fallback_last : h.chem_fallback);
 }
 
 int scfd_set_partition(scfd_ctx* c, const int32_t* owner, int nranks, int rank) {

@@ -39,6 +39,27 @@ __host__ __device__ inline long long cidx(const Planes& P, int p, int i, int j) 
     return P.base[p] + (long long)(j + 1) * P.pitch[p] + (i + 1);
 }
 
+// Per-species contribution lists of the reaction rates, in the order in which
+// the reference accumulates them.  For Fex_var (FJ.f90:301-453) entry 2*i + kind
+// adds the forward (kind 0) or reverse (kind 1) rate of reaction i; p lists the
+// production terms, m the destruction terms; mref[i] is the reaction whose
+// third-body term reaction i uses (-1: none yet).  For Fex / Jex
+// (FJ.f90:152-709), the net list of species j, n_ptr[j] .. n_ptr[j+1], holds
+// 2*i + 1 for every reactant slot of j in reaction i and 2*i for every product
+// slot, reactions in order and reactants first, as the reference subtracts and
+// adds Dr; dref[i] is the last reaction up to i that sets dlnkdlnM (third-body
+// or fall-off rate; -1: none yet).
+struct RateLists {
+    const int* p_ptr;  // [ns+1]
+    const int* p_ent;
+    const int* m_ptr;  // [ns+1]
+    const int* m_ent;
+    const int* mref;   // [nr]
+    const int* n_ptr;  // [ns+1]
+    const int* n_ent;
+    const int* dref;   // [nr]
+};
+
 // Compact chemistry tables on the device (0-based species).
 struct DevChem {
     int ns, nr, nt;
@@ -63,7 +84,8 @@ struct DevChem {
     const double* trans;      // [nt][5][4]
     const double* wc1;        // [nt][nt] (MW(jt)/MW(it))**0.25
     const double* wc2;        // [nt][nt] sqrt(2 MW(jt)/(MW(it)+MW(jt)))
-    double rtol;
+    RateLists rl;             // the per-species rate lists of the one-warp evaluations
+    double rtol, atol;        // control_chem.inp tolerances (atol: DVODE only)
 };
 
 // Scalars that live on the device between kernels of one step.
@@ -78,6 +100,8 @@ struct DevScalars {
     int first_dual;
     long long chem_attempts;
     long long chem_fallback;
+    long long chem_attempts_last;  // the same counts for the last chemistry launch only
+    long long chem_fallback_last;
     unsigned long long spin_abort;  // non-zero once a bounded wait gave up
     // per inner iteration of the last step (internal_res.dat of
     // time_NR_viscous.f90:87-95): omega from the Dqrate limiter before the
@@ -171,7 +195,21 @@ int wave_handoff_chunk();                  // hand-off columns per chunk
 int wave_max_clusters(int ny, bool mixed); // co-resident clusters of the sweep kernel (0: none)
 int launch_wave(const View& v, cudaStream_t s, const Wave& w, int what, int inner);
 int launch_nr_update(const View& v, cudaStream_t s, const double* partials, int nstrips, int inner);
-int launch_chem_impl(const View& v, cudaStream_t s, int max_substeps, unsigned long long* counter, int nsm);
+// Cells whose CHEMEQ2 interval went to DVODE: k_chem queues them (the cell, the
+// time reached and the moles and T there) and k_chem_dvode finishes them.
+struct ChemQueue {
+    long long* cell;             // [capacity]
+    double* tt;                  // [capacity]
+    double* y;                   // [capacity][ns + 1]
+    unsigned long long* count;   // 2: queued, taken
+    long long capacity;          // interior cells of the updated planes
+    int warp_doubles;            // shared memory per warp of k_chem_dvode
+    int warps_per_block;
+};
+size_t chem_dvode_warp_doubles(int ns, int nr);
+int chem_dvode_setup(int ns, int nr, int* warps_per_block);  // kernel attribute; 0 or a cudaError_t
+int launch_chem_impl(const View& v, cudaStream_t s, int max_substeps, unsigned long long* counter, int nsm,
+                     const ChemQueue& dq);
 int launch_step_end(const View& v, cudaStream_t s, double warn, double err);
 int launch_rms(const View& v, cudaStream_t s, double* partial, double* out);
 int launch_copy(double* dst, const double* src, long long n, cudaStream_t s);

@@ -70,3 +70,28 @@ def test_excess_work_restarts_continue_the_integration(orc_raw):
     st, y, nst = _run(orc_raw, 1, [1.0, 0.0, 0.0], 0.0, 4.0e5, 1e-8, 1e-14)
     assert st == 2 and nst > 500
     assert abs(y.sum() - 1.0) < 1e-8 and y[0] < 0.01
+
+
+def test_reactor_flags_under_one_ulp():
+    """The envelope the GPU reactor test allows: the oracle's own reactors,
+    with T0 moved by one ulp, keep their ignited / failed flags and ignition
+    delays (to 1e-4) but flip the DVODE flag of a few tenths of a percent
+    (whether an interval uses up its 10 CHEMEQ2 attempts turns on rounding)."""
+    import ctypes as C
+
+    from conftest import build_oracle
+    from shared_cfd_b200 import abi, cases
+    from shared_cfd_b200.reactors import Reactors
+
+    orc = abi.Bound(C.CDLL(build_oracle()), "orc_")
+    n = 2048
+    _, ch, T0, v, _ = cases.reactor_batch(n)
+    with Reactors(ch, n, lib=orc) as r:
+        a = r.run(T0, v, 2e-3)
+        b = r.run(np.nextafter(T0, np.inf), v, 2e-3)
+    hard = abi.REACTOR_IGNITED | abi.REACTOR_FAILED
+    assert np.array_equal(a["flags"] & hard, b["flags"] & hard)
+    flips = np.count_nonzero((a["flags"] ^ b["flags"]) & abi.REACTOR_FELL_BACK)
+    assert 0 < flips <= 0.005 * n, flips
+    ign = (a["flags"] & abi.REACTOR_IGNITED) > 0
+    assert np.allclose(a["t_ign"][ign], b["t_ign"][ign], rtol=1e-4, atol=0.0)

@@ -76,6 +76,23 @@ def test_reacting_step_small(gpu, orc):
     _parity(case, gpu, orc, 2)
 
 
+def test_reacting_step_chemistry_goes_to_dvode(gpu, orc):
+    """A premixed wake at 1500 K and dt = 1e-4 s: every wake cell's interval
+    uses up its 10 CHEMEQ2 attempts, and k_chem_dvode finishes it with DVODE
+    (sub_chem.f90:1755-1775) as the restatement does."""
+    case = cases.reacting_step(scale=1.0 / 32.0, inner=4, dt=1e-4, wake="premixed")
+    a = run_case(case, gpu, 2)
+    b = run_case(case, orc, 2)
+    sa, sb = a["stats"], b["stats"]
+    assert sa.status == 0 and sb.status == 0
+    wake = case.ni[3] * case.nj[3]
+    assert sb.chem_fallback_cells >= wake
+    assert sa.chem_fallback_cells == sb.chem_fallback_cells
+    assert np.isfinite(a["q"]).all()
+    err = rel_l2(case, a["q"], b["q"])
+    assert err <= 1e-8, "rel L2 %g" % err
+
+
 def test_halo_indexing_bit_exact(gpu, orc):
     """Ghost cells written by the halo copy and the boundary descriptors hold
     bit-identical values on both paths: q carries a unique density per cell

@@ -2,12 +2,18 @@
 restatement, through the C ABI.
 
 Tolerances.  The device and the host evaluate exp / log with different
-libraries; the adaptive substep sequence of a reactor can then branch
-differently (CHEMEQ2 and the Rosenbrock fallback choose their steps from error
-ratios), so results are compared reactor by reactor with tolerances at the
-integration error, not bit by bit: the flags must agree, the ignition delays
-to 1e-3, most final temperatures exactly and all to 1e-2.  Runs of the same
-batch on the GPU (graph replay, one launch per reactor) must agree bit by bit.
+libraries and the device contracts multiply-adds, so the two runs differ in
+the last bits.  The reactors are sensitive to that: whether an interval uses
+up its 10 CHEMEQ2 attempts and goes to DVODE flips on rounding, and the two
+integrators then take different steps.  The oracle itself shows the envelope
+(tests/test_dvode.py::test_reactor_flags_under_one_ulp): moving T0 or the
+partial densities by one ulp flips the DVODE flag of 0.2-0.25 % of the
+reactors and moves T_end by up to ~1e-2 and t_ign by up to ~3e-5 (relative).
+So, reactor by reactor: the ignited and failed flags must agree, the DVODE
+flag may differ in at most 0.5 % of the reactors, the ignition delays agree to
+1e-4, the final temperatures to 2e-2, and at least half of them exactly.
+Runs of the same batch on the GPU (graph replay, one launch per reactor) must
+agree bit by bit.
 """
 import numpy as np
 import pytest
@@ -22,8 +28,8 @@ KEYS = ("T_end", "vrho_end", "t_ign", "evals", "flags")
 
 @pytest.fixture(scope="module")
 def batch():
-    # 192 reactors of the benchmark distribution and 32 hot ones that ignite
-    _, ch, T0, v, _ = cases.reactor_batch(192)
+    # 2048 reactors of the benchmark distribution and 32 hot ones that ignite
+    _, ch, T0, v, _ = cases.reactor_batch(2048)
     _, _, T1, v1, _ = cases.reactor_batch(32, seed=7, T_range=(1540.0, 1600.0), phi_range=(0.8, 1.5))
     return ch, np.concatenate([T0, T1]), np.concatenate([v, v1])
 
@@ -40,14 +46,18 @@ def test_reactors_match_restatement(gpu, batch, reference):
     with Reactors(ch, len(T0)) as r:
         out = r.run(T0, v, 2e-3)
     ref = reference
-    assert out["status"] == 0
-    assert np.array_equal(out["flags"], ref["flags"])
+    assert out["status"] == 0 and ref["status"] == 0
+    hard = abi.REACTOR_IGNITED | abi.REACTOR_FAILED
+    assert np.array_equal(out["flags"] & hard, ref["flags"] & hard)
+    fb = (out["flags"] ^ ref["flags"]) & abi.REACTOR_FELL_BACK
+    assert np.count_nonzero(fb) <= 0.005 * len(T0), np.count_nonzero(fb)
+    assert np.count_nonzero(ref["flags"] & abi.REACTOR_FELL_BACK) >= 0.1 * len(T0)  # DVODE is exercised
     ign = (ref["flags"] & abi.REACTOR_IGNITED) > 0
-    assert ign.sum() >= 5
-    assert np.allclose(out["t_ign"][ign], ref["t_ign"][ign], rtol=1e-3, atol=0.0)
+    assert ign.sum() >= 32
+    assert np.allclose(out["t_ign"][ign], ref["t_ign"][ign], rtol=1e-4, atol=0.0)
     assert (out["t_ign"][~ign] == -1.0).all()
     rel = np.abs(out["T_end"] - ref["T_end"]) / ref["T_end"]
-    assert (rel <= 1e-2).all(), rel.max()
+    assert (rel <= 2e-2).all(), rel.max()
     assert np.mean(rel == 0.0) >= 0.5
     mass = out["vrho_end"].sum(axis=1) / ref["vrho_end"].sum(axis=1)
     assert np.allclose(mass, 1.0, rtol=1e-3)
@@ -58,7 +68,9 @@ def test_graph_replay_and_per_launch_are_bit_identical(gpu, batch):
     with Reactors(ch, len(T0)) as r:
         a = r.run(T0, v, 2e-3)           # captures the CUDA graph
         b = r.run(T0, v, 2e-3)           # replays it
-        assert r.launch_count() == 1
+        np2 = 1 << (len(T0) - 1).bit_length()
+        lg = np2.bit_length() - 1
+        assert r.launch_count() == 2 + lg * (lg + 1) // 2  # queue keys, bitonic stages, reactors
         for k in KEYS:
             assert np.array_equal(a[k], b[k]), k
         n = 24
