@@ -14,10 +14,10 @@
 //
 // A task is up to 8 consecutive strips of one plane, run by one thread-block
 // cluster of 8 CTAs (CTA rank r on the task's strip r).  Strip r's lane 31
-// stages its row in its own shared memory; every HK columns the helper warp
-// moves the chunk with one bulk copy into CTA r + 1's hand-off ring
-// (distributed shared memory), completing a transaction count on an mbarrier
-// of the receiving CTA; the receiver releases each chunk with a remote arrive.  A task with a successor
+// stages its row in its own shared memory; every HK columns it moves the chunk
+// with one bulk copy into CTA r + 1's hand-off ring (distributed shared
+// memory), completing a transaction count on an mbarrier of the receiving
+// CTA; the receiver releases each chunk with a remote arrive.  A task with a successor
 // holds 8 strips, so only rank 7 ever publishes to global memory and ranks
 // 0-6 only to the next CTA.  Between tasks of one plane the
 // top row travels through global memory: the last CTA's helper warp copies it
@@ -51,10 +51,14 @@ namespace {
 
 constexpr int CL = 8;    // CTAs per cluster = strips per task
 constexpr int HK = 4;    // hand-off columns per chunk
-constexpr int HS = 16;   // hand-off ring chunks
+constexpr int HS = 32;   // hand-off ring chunks
 constexpr int PFB = 4;   // record ring slots
 constexpr int kPadSteps = 8;  // zero step blocks before and after each strip's records
 constexpr long long kSpin = 1ll << 22;
+
+// hand-off chunks of a strip's top row for a plane of ni columns: chunk j
+// holds the columns 4j-3 .. 4j (HK = 4), j = 0 .. (ni + 2) / 4
+__host__ __device__ constexpr int chunks_of(int ni) { return (ni + 2) / 4 + 1; }
 
 // sum of a[B..E) as a balanced pairwise tree (short dependency chain)
 template <int B, int E, typename T>
@@ -265,11 +269,11 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
     using F = CF<NY>;
     using L = WL<RT, NY>;
     using V = typename Vec16<RT>::type;
-    constexpr int D = NY + 3, G = L::G, NGX = L::NGX, NGC = L::NGC, XS = L::XS, CSZ = L::CS, D4 = L::D4,
+    constexpr int D = NY + 3, G4 = L::G, NGX = L::NGX, NGC = L::NGC, XS = L::XS, CSZ = L::CS, D4 = L::D4,
                   SPB = L::SPB;
     constexpr unsigned CHUNK_BYTES = HK * D4 * sizeof(RT);
     static_assert(SPB <= kPadSteps, "a record chunk may reach into the padding by at most one chunk");
-    static_assert(D4 % G == 0 && (CHUNK_BYTES % 16) == 0, "hand-off chunks are whole 16-byte vectors");
+    static_assert(D4 % G4 == 0 && (CHUNK_BYTES % 16) == 0, "hand-off chunks are whole 16-byte vectors");
     extern __shared__ __align__(128) unsigned char sm[];
     RT* ringX = reinterpret_cast<RT*>(sm);   // [PFB][SPB][XS]
     RT* ringC = ringX + PFB * SPB * XS;      // [PFB][SPB][CS]
@@ -330,7 +334,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
         const bool pub_global = active && (int)rank + 1 == ns && succ_task;
         const int nsteps = ni + 31;
         const int nch = (nsteps + SPB - 1) / SPB;
-        const int nxc = (ni + HK - 1) / HK;
+        const int nxc = chunks_of(ni);
         const long long sbase = active ? a.step_off[fs] + kPadSteps : 0;
         // first record step (memory order) of chunk n
         auto chunk_step = [&](int n) -> long long {
@@ -343,6 +347,9 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
             const int lf = DIR == 0 ? lane : 31 - lane;  // this lane's slot in a step block
             // consumed chunks are released to the producer: the CTA below (remote) or this CTA's helper
             const unsigned rel = rank > 0 ? mapa(pempty, rank - 1) : mapa(hempty, rank);
+            // the next CTA's hand-off ring and its barriers (pub_remote)
+            const unsigned dring = pub_remote ? mapa(xin, rank + 1) : 0u;
+            const unsigned dfull = pub_remote ? mapa(xfull, rank + 1) : 0u;
             RT outA[D], outB[D];
 #pragma unroll
             for (int k = 0; k < D; ++k) {
@@ -356,6 +363,26 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
             // an FP32 cross product.
             constexpr bool f32 = sizeof(RT) == 4;
             RT on = RT(__longlong_as_double(0x7FF0000000000000ll)), od = RT(1);
+            // The hand-off.  Chunk j of the strip below holds the columns 4j-3 .. 4j
+            // (HK = 4) of its top row: its lane 31 computes column c at its step c + 31,
+            // so its group of steps G (4G .. 4G+3) yields exactly chunk G - 7.  Lane 0
+            // here uses column t at step t: chunk G's last column at step 4G (u = 0 of
+            // group G), chunk G+1's first three at u = 1..3, so chunk G is released and
+            // chunk G+1 awaited between u = 0 and u = 1.
+            static_assert(HK == 4 && SPB % HK == 0, "groups of 4 steps, whole groups per record slot");
+            const int lastc = nxc - 1;
+            const unsigned xc0 = xc;
+            unsigned xw = xc;  // chunks awaited (running, like xc)
+            auto await_chunk = [&]() -> bool {
+                bool ok = true;
+                if (lane == 0) ok = wait_phase(&xfull[xw % HS], (xw / HS) & 1u, v, s_bail);
+                ++xw;
+                return __all_sync(0xffffffffu, ok);
+            };
+            if (has_prev && !await_chunk()) {
+                if (lane == 0) give_up(v, s_bail);
+                bail = true;
+            }
             for (int n = 0; n < nch && !bail; ++n) {
                 const unsigned slot = rc % PFB, par = (rc / PFB) & 1u;
                 if (!__all_sync(0xffffffffu, wait_phase(&rfull[slot], par, v, s_bail))) {
@@ -365,144 +392,154 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                 }
                 RT* sx = ringX + slot * SPB * XS;
                 const RT* scf = ringC + slot * SPB * CSZ;
-#pragma unroll 2
-                for (int u = 0; u < SPB; ++u) {
-                    const int t = n * SPB + u;
-                    const int pos = DIR == 0 ? u : SPB - 1 - u;
-                    // column t from the strip below (lane 0)
-                    const bool in_col = has_prev && t < ni;
-                    const unsigned hs = xc % HS;
-                    bool ok = true;
-                    if (in_col && (t % HK) == 0 && lane == 0) ok = wait_phase(&xfull[hs], (xc / HS) & 1u, v, s_bail);
-                    if (!__all_sync(0xffffffffu, ok)) {
-                        if (lane == 0) give_up(v, s_bail);
-                        bail = true;
-                        break;
-                    }
-                    RT inB[D];
-                    const RT* xi = xin + (hs * HK + (t % HK)) * D4;
 #pragma unroll
-                    for (int k = 0; k < D; ++k) {
-                        const RT sh = __shfl_up_sync(0xffffffffu, outB[k], 1);
-                        inB[k] = lane == 0 ? (in_col ? xi[k] : RT(0)) : sh;
-                    }
-                    if (in_col && ((t % HK) == HK - 1 || t == ni - 1)) {
-                        // the chunk is refilled 16 chunks later, long after lane 0's reads
-                        // of it completed: no release fence needed
-                        if (lane == 0) mbar_arrive_cluster_relaxed(rel + hs * 8u);
-                        ++xc;
-                    }
-                    // this lane's cell
-                    RT fx[NGX * G], f[NGC * G];
-                    const V* srcx = reinterpret_cast<const V*>(sx + pos * XS) + lf;
-                    const V* srcc = reinterpret_cast<const V*>(scf + pos * CSZ) + lf;
-#pragma unroll
-                    for (int g = 0; g < NGX; ++g) *reinterpret_cast<V*>(&fx[g * G]) = srcx[g * 32];
-#pragma unroll
-                    for (int g = 0; g < NGC; ++g) *reinterpret_cast<V*>(&f[g * G]) = srcc[g * 32];
-                    const RT al = f[F::AL];
-                    RT x[D];
-#pragma unroll
-                    for (int k = 0; k < D; ++k)
-                        x[k] = DIR == 0 ? al * (fx[k] + (outA[k] + inB[k])) : fx[k] - al * (outA[k] + inB[k]);
-                    // dpdq (sch_NR.raw.f90:143-144): species hvs + DHi, then -g1 u, -g1 v, g1
-                    const RT g1 = f[F::G1], uu = f[F::U], vv = f[F::V];
-                    RT dp[D];
-#pragma unroll
-                    for (int k = 0; k < NY; ++k) dp[k] = f[F::HVS] + f[F::DH + k];
-                    dp[NY] = -g1 * uu;
-                    dp[NY + 1] = -g1 * vv;
-                    dp[NY + 2] = g1;
-                    // P = dpdq.x; forward q2d: semi-implicit pressure source
-                    // (q2d time_lusgs_viscous.f90:38-44).  Both sums are pairwise trees.
-                    RT pr[D - 1];
-#pragma unroll
-                    for (int k = 0; k < D - 1; ++k) {
-                        const int kk = k < NY + 1 ? k : k + 1;  // every component but rho v
-                        pr[k] = dp[kk] * x[kk];
-                    }
-                    RT P = tree_sum<0, D - 1>(pr);
-                    const RT S = tree_sum<0, NY>(x);
-                    if (DIR == 0 && q2d) x[NY + 1] = (x[NY + 1] + f[F::AA] * P) * f[F::RQ];
-                    P += dp[NY + 1] * x[NY + 1];
-#pragma unroll
-                    for (int dn = 0; dn < 2; ++dn) {
-                        const int b0 = dn == 0 ? F::FA : F::FB;
-                        const RT fa = f[b0], n1 = f[b0 + 1], n2 = f[b0 + 2];
-                        const RT un = n1 * uu + n2 * vv;
-                        const RT nu = (un < RT(0) ? -un : un) + f[F::CS];
-                        // ds/2 folded into the coefficients: o = cv (fa base) + (fa lam) x [+ (fa P) n]
-                        const RT fb = fa * (n1 * x[NY] + n2 * x[NY + 1] - un * S);
-                        const RT fl = fa * (DIR == 0 ? un + nu : un - nu);
-                        const RT fp = fa * P;
-                        RT* o = dn == 0 ? outA : outB;
-#pragma unroll
-                        for (int k = 0; k < NY; ++k) o[k] = f[F::Y + k] * fb + fl * x[k];
-                        o[NY] = uu * fb + fl * x[NY] + n1 * fp;
-                        o[NY + 1] = vv * fb + fl * x[NY + 1] + n2 * fp;
-                        o[NY + 2] = f[F::H] * fb + fl * x[NY + 2] + un * fp;
-                    }
-                    // results back into the slot (16-byte stores); the helper writes them out
-#pragma unroll
-                    for (int k = 0; k < D; ++k) fx[k] = x[k];
-                    V* dstx = reinterpret_cast<V*>(sx + pos * XS) + lf;
-#pragma unroll
-                    for (int g = 0; g < NGX; ++g) dstx[g * 32] = *reinterpret_cast<V*>(&fx[g * G]);
-                    if (DIR == 1 && nr) {
-                        const double dE = double(x[NY + 2]);
-                        res = res + dE * dE;
-                        const RT rho = f[F::RHO];
-#pragma unroll
-                        for (int k = 0; k < NY; ++k) {
-                            // smallest q_k/(-Dq_k) over Dq_k < 0
-                            const RT dk = x[k];
-                            const RT qn = rho * f[F::Y + k], qd = -dk;
-                            if constexpr (f32) {
-                                if (dk < RT(0)) on = fminf(on, __fdividef(qn, qd));
-                            } else {
-                                if (dk < RT(0) && qn * od < on * qd) {
-                                    on = qn;
-                                    od = qd;
-                                }
-                            }
-                        }
-                    }
-                    // publish column cc of the top row (lane 31) to the strip above: into
-                    // this CTA's xout ring; a whole chunk then goes by one bulk copy into
-                    // the next CTA's xin (or to the helper, for the next task)
-                    const int cc = t - 31;
-                    if ((pub_remote || pub_global) && cc >= 0 && cc < ni) {
-                        const unsigned ps = pc % HS;
-                        const int col = cc % HK;
-                        const bool last = col == HK - 1 || cc == ni - 1;
+                for (int h = 0; h < SPB / HK && !bail; ++h) {
+                    const int G = n * (SPB / HK) + h;
+                    // this group's top-row outputs form chunk J of the strip above
+                    const int J = G - 7;
+                    const bool pub = (pub_remote || pub_global) && J >= 0 && J <= lastc;
+                    const unsigned ps = pc % HS;
+                    if (pub && pc >= HS) {
                         bool okp = true;
-                        if (lane == 31) {
-                            if (col == 0 && pc >= HS)
-                                okp = wait_phase(pub_remote ? &pempty[ps] : &oemp[ps], ((pc / HS) - 1u) & 1u, v, s_bail);
-                            if (okp) {
-                                RT vals[D4];
-#pragma unroll
-                                for (int k = 0; k < D4; ++k) vals[k] = k < D ? outB[k] : RT(0);
-                                RT* dst = xout + (ps * HK + col) * D4;
-#pragma unroll
-                                for (int g = 0; g < D4 / G; ++g)
-                                    reinterpret_cast<V*>(dst)[g] = *reinterpret_cast<V*>(&vals[g * G]);
-                                // a whole chunk goes on to the helper, which moves it to the
-                                // next CTA (bulk copy) or to global memory
-                                if (last) {
-                                    fence_proxy_async_smem();
-                                    mbar_arrive(&oful[ps]);
-                                }
-                            }
-                        }
+                        if (lane == 31)
+                            okp = wait_phase(pub_remote ? &pempty[ps] : &oemp[ps], ((pc / HS) - 1u) & 1u, v, s_bail);
                         if (!__all_sync(0xffffffffu, okp)) {
                             if (lane == 31) give_up(v, s_bail);
                             bail = true;
                             break;
                         }
-                        if (last) ++pc;
+                    }
+#pragma unroll
+                    for (int u = 0; u < HK; ++u) {
+                        const int t = G * HK + u;
+                        const int pos = DIR == 0 ? h * HK + u : SPB - 1 - (h * HK + u);
+                        if (u == 1 && has_prev) {
+                            // chunk G is used up; chunk G+1 holds the next three columns.  A
+                            // chunk is refilled HS chunks later, long after these reads.
+                            if (G <= lastc) {
+                                if (lane == 0) mbar_arrive_cluster_relaxed(rel + (xc % HS) * 8u);
+                                ++xc;
+                            }
+                            if (G + 1 <= lastc && !await_chunk()) {
+                                if (lane == 0) give_up(v, s_bail);
+                                bail = true;
+                                break;
+                            }
+                        }
+                        // column t from the strip below (lane 0)
+                        const bool in_col = has_prev && t < ni;
+                        const RT* xi = xin + (((xc0 + (unsigned)((t + 3) >> 2)) % HS) * HK + ((t + 3) & 3)) * D4;
+                        RT inB[D];
+#pragma unroll
+                        for (int k = 0; k < D; ++k) {
+                            const RT sh = __shfl_up_sync(0xffffffffu, outB[k], 1);
+                            inB[k] = lane == 0 ? (in_col ? xi[k] : RT(0)) : sh;
+                        }
+                        // this lane's cell
+                        RT fx[NGX * G4], f[NGC * G4];
+                        const V* srcx = reinterpret_cast<const V*>(sx + pos * XS) + lf;
+                        const V* srcc = reinterpret_cast<const V*>(scf + pos * CSZ) + lf;
+#pragma unroll
+                        for (int g = 0; g < NGX; ++g) *reinterpret_cast<V*>(&fx[g * G4]) = srcx[g * 32];
+#pragma unroll
+                        for (int g = 0; g < NGC; ++g) *reinterpret_cast<V*>(&f[g * G4]) = srcc[g * 32];
+                        const RT al = f[F::AL];
+                        RT x[D];
+#pragma unroll
+                        for (int k = 0; k < D; ++k)
+                            x[k] = DIR == 0 ? al * (fx[k] + (outA[k] + inB[k])) : fx[k] - al * (outA[k] + inB[k]);
+                        // dpdq (sch_NR.raw.f90:143-144): species hvs + DHi, then -g1 u, -g1 v, g1
+                        const RT g1 = f[F::G1], uu = f[F::U], vv = f[F::V];
+                        RT dp[D];
+#pragma unroll
+                        for (int k = 0; k < NY; ++k) dp[k] = f[F::HVS] + f[F::DH + k];
+                        dp[NY] = -g1 * uu;
+                        dp[NY + 1] = -g1 * vv;
+                        dp[NY + 2] = g1;
+                        // P = dpdq.x; forward q2d: semi-implicit pressure source
+                        // (q2d time_lusgs_viscous.f90:38-44).  Both sums are pairwise trees.
+                        RT pr[D - 1];
+#pragma unroll
+                        for (int k = 0; k < D - 1; ++k) {
+                            const int kk = k < NY + 1 ? k : k + 1;  // every component but rho v
+                            pr[k] = dp[kk] * x[kk];
+                        }
+                        RT P = tree_sum<0, D - 1>(pr);
+                        const RT S = tree_sum<0, NY>(x);
+                        if (DIR == 0 && q2d) x[NY + 1] = (x[NY + 1] + f[F::AA] * P) * f[F::RQ];
+                        P += dp[NY + 1] * x[NY + 1];
+#pragma unroll
+                        for (int dn = 0; dn < 2; ++dn) {
+                            const int b0 = dn == 0 ? F::FA : F::FB;
+                            const RT fa = f[b0], n1 = f[b0 + 1], n2 = f[b0 + 2];
+                            const RT un = n1 * uu + n2 * vv;
+                            const RT nu = (un < RT(0) ? -un : un) + f[F::CS];
+                            // ds/2 folded into the coefficients: o = cv (fa base) + (fa lam) x [+ (fa P) n]
+                            const RT fb = fa * (n1 * x[NY] + n2 * x[NY + 1] - un * S);
+                            const RT fl = fa * (DIR == 0 ? un + nu : un - nu);
+                            const RT fp = fa * P;
+                            RT* o = dn == 0 ? outA : outB;
+#pragma unroll
+                            for (int k = 0; k < NY; ++k) o[k] = f[F::Y + k] * fb + fl * x[k];
+                            o[NY] = uu * fb + fl * x[NY] + n1 * fp;
+                            o[NY + 1] = vv * fb + fl * x[NY + 1] + n2 * fp;
+                            o[NY + 2] = f[F::H] * fb + fl * x[NY + 2] + un * fp;
+                        }
+                        // results back into the slot (16-byte stores); the helper writes them out
+#pragma unroll
+                        for (int k = 0; k < D; ++k) fx[k] = x[k];
+                        V* dstx = reinterpret_cast<V*>(sx + pos * XS) + lf;
+#pragma unroll
+                        for (int g = 0; g < NGX; ++g) dstx[g * 32] = *reinterpret_cast<V*>(&fx[g * G4]);
+                        if (DIR == 1 && nr) {
+                            const double dE = double(x[NY + 2]);
+                            res = res + dE * dE;
+                            const RT rho = f[F::RHO];
+#pragma unroll
+                            for (int k = 0; k < NY; ++k) {
+                                // smallest q_k/(-Dq_k) over Dq_k < 0
+                                const RT dk = x[k];
+                                const RT qn = rho * f[F::Y + k], qd = -dk;
+                                if constexpr (f32) {
+                                    if (dk < RT(0)) on = fminf(on, __fdividef(qn, qd));
+                                } else {
+                                    if (dk < RT(0) && qn * od < on * qd) {
+                                        on = qn;
+                                        od = qd;
+                                    }
+                                }
+                            }
+                        }
+                        // lane 31: entry u of chunk J in this CTA's xout ring
+                        if (pub && lane == 31) {
+                            RT vals[D4];
+#pragma unroll
+                            for (int k = 0; k < D4; ++k) vals[k] = k < D ? outB[k] : RT(0);
+                            RT* dst = xout + (ps * HK + u) * D4;
+#pragma unroll
+                            for (int g = 0; g < D4 / G4; ++g)
+                                reinterpret_cast<V*>(dst)[g] = *reinterpret_cast<V*>(&vals[g * G4]);
+                        }
+                    }
+                    if (bail) break;
+                    // chunk J complete: one bulk copy into the next CTA's ring, completing the
+                    // receiver's barrier phase with this arrival and the copy's bytes (in
+                    // either order), or on to the helper, which publishes it in global
+                    // memory.  Columns outside 0 .. ni-1 travel as they are.
+                    if (pub) {
+                        if (lane == 31) {
+                            fence_proxy_async_smem();
+                            if (pub_remote) {
+                                mbar_arrive_expect_tx_cluster_relaxed(dfull + ps * 8u, CHUNK_BYTES);
+                                bulk_s2dsmem(dring + ps * CHUNK_BYTES, xout + ps * HK * D4, CHUNK_BYTES, dfull + ps * 8u);
+                            } else {
+                                mbar_arrive(&oful[ps]);
+                            }
+                        }
+                        ++pc;
                     }
                 }
+                if (bail) break;
                 // the slot's results are visible to the helper's bulk store
                 fence_proxy_async_smem();
                 __syncwarp();
@@ -538,9 +575,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
             int nl = 0, nst = 0, hin = 0, hout = 0;
             long long idle = 0;
             bool bail = false;
-            const unsigned dring = pub_remote ? mapa(xin, rank + 1) : 0u;
-            const unsigned dfull = pub_remote ? mapa(xfull, rank + 1) : 0u;
-            while (!bail && (nst < nch || (gin && hin < nxc) || ((pub_remote || pub_global) && hout < nxc))) {
+            while (!bail && (nst < nch || (gin && hin < nxc) || (pub_global && hout < nxc))) {
                 bool prog = false;
                 // record loads: the slot of chunk nl is free once chunk nl - PFB is stored
                 if (nl < nch && nl - PFB < nst) {
@@ -584,23 +619,6 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                     }
                     if (__shfl_sync(0xffffffffu, go, 0)) {
                         ++hin;
-                        prog = true;
-                    }
-                }
-                // this CTA's top row into the next CTA's xin: the chunk's phase of the
-                // receiver's barrier completes with this arrival and the copy's bytes, in
-                // either order; columns past ni of a partial last chunk travel as they are
-                if (pub_remote && hout < nxc) {
-                    const unsigned g = pc0 + hout, hs = g % HS;
-                    int rd = 0;
-                    if (lane == 0) rd = mbar_test_wait(&oful[hs], (g / HS) & 1u) ? 1 : 0;
-                    if (__shfl_sync(0xffffffffu, rd, 0)) {
-                        if (lane == 0) {
-                            fence_proxy_async_smem();
-                            mbar_arrive_expect_tx_cluster_relaxed(dfull + hs * 8u, CHUNK_BYTES);
-                            bulk_s2dsmem(dring + hs * CHUNK_BYTES, xout + hs * HK * D4, CHUNK_BYTES, dfull + hs * 8u);
-                        }
-                        ++hout;
                         prog = true;
                     }
                 }
@@ -721,6 +739,7 @@ __global__ void __launch_bounds__(1024) k_unpack(View v, const int2* blk, const 
 int wave_pad_steps() { return kPadSteps; }
 int wave_strips_per_task() { return CL; }
 int wave_handoff_chunk() { return HK; }
+int wave_chunks(int ni) { return chunks_of(ni); }
 
 namespace {
 template <typename RT, int NY>

@@ -796,7 +796,7 @@ int scfd_commit(scfd_ctx* c) {
     }
     const int ntasks = (int)tasksf.size() / 4;
     const int hk = wave_handoff_chunk();
-    const long long xstride3 = (long long)((c->nimax + hk - 1) / hk) * hk * std::max(1, wz.d4);
+    const long long xstride3 = (long long)wave_chunks(c->nimax) * hk * std::max(1, wz.d4);
     // arena size
     size_t bytes = 0;
     bytes += 3 * need<double>(D * N);                         // q, qp, qpp

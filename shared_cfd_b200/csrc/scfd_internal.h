@@ -192,6 +192,7 @@ WaveSizes wave_sizes(int ny, bool mixed);  // xs = 0 if the species count has no
 int wave_pad_steps();                      // zero step blocks before and after each strip
 int wave_strips_per_task();
 int wave_handoff_chunk();                  // hand-off columns per chunk
+int wave_chunks(int ni);                   // hand-off chunks of a top row of ni columns
 int wave_max_clusters(int ny, bool mixed); // co-resident clusters of the sweep kernel (0: none)
 int launch_wave(const View& v, cudaStream_t s, const Wave& w, int what, int inner);
 int launch_nr_update(const View& v, cudaStream_t s, const double* partials, int nstrips, int inner);
