@@ -65,14 +65,13 @@ __global__ void k_dt_import(View v, const double* red) {
 
 // the per-strip partials of the backward sweep, reduced in strip order
 __global__ void k_res_export(View v, const double* partials, int nstrips, double* red) {
-    double res = 0.0, om = 1e300;
-    for (int k = 0; k < nstrips; ++k) {
-        res += partials[2 * k];
-        om = fmin(om, partials[2 * k + 1]);
+    double res, om;
+    reduce_partials(partials, nstrips, res, om);
+    if (threadIdx.x == 0) {
+        red[0] = res;
+        red[1] = om;
+        red[2] = -(double)v.sc->status;
     }
-    red[0] = res;
-    red[1] = om;
-    red[2] = -(double)v.sc->status;
 }
 
 // The global omega candidate decides the omega test on every rank alike
@@ -122,7 +121,7 @@ int launch_dt_import(const View& v, cudaStream_t s, const double* red) {
 }
 
 int launch_res_export(const View& v, cudaStream_t s, const double* partials, int nstrips, double* red) {
-    k_res_export<<<1, 1, 0, s>>>(v, partials, nstrips, red);
+    k_res_export<<<1, 1024, 0, s>>>(v, partials, nstrips, red);
     return 1;
 }
 

@@ -28,7 +28,7 @@
 //
 // Each CTA has one compute warp and one helper warp.  The compute warp does
 // the wavefront only: no global loads, stores or fences in its step loop.  The
-// helper streams the strip's records through a ring of PFB slots (bulk copies
+// helper streams the strip's records through a ring of slots (bulk copies
 // completing on mbarriers), writes the results back with bulk stores, and moves
 // the hand-off chunks on (to the next CTA, or through global memory).  Every wait is bounded; a wait that gives up sets
 // SCFD_E_SPIN and the kernel winds down instead of hanging.
@@ -52,7 +52,6 @@ namespace {
 constexpr int CL = 8;    // CTAs per cluster = strips per task
 constexpr int HK = 4;    // hand-off columns per chunk
 constexpr int HS = 32;   // hand-off ring chunks
-constexpr int PFB = 4;   // record ring slots
 constexpr int kPadSteps = 8;  // zero step blocks before and after each strip's records
 constexpr long long kSpin = 1ll << 22;
 
@@ -109,7 +108,8 @@ struct WL {
     static constexpr int XS = NGX * 32 * G;  // elements of one step block of X
     static constexpr int CS = NGC * 32 * G;  // and of C
     static constexpr int D4 = NGX * G;       // hand-off column (D values, padded)
-    static constexpr int SPB = sizeof(RT) == 4 ? 8 : 4;  // steps per record bulk copy
+    static constexpr int SPB = 4;                          // steps per record bulk copy (one group)
+    static constexpr int PFB = sizeof(RT) == 4 ? 8 : 4;    // record ring slots
     static constexpr size_t SMEM = sizeof(RT) * ((size_t)PFB * SPB * (XS + CS) + 2 * HS * HK * D4) +
                                    8 * (2 * PFB + 5 * HS) + 16;
 };
@@ -236,7 +236,6 @@ struct WaveArgs {
     long long xstride;          // elements per task
     int* progress;              // per task: hand-off chunks published
     int* ticket;
-    double* partials;           // per forward strip: (res, omega candidate)
 };
 
 namespace {
@@ -270,7 +269,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
     using L = WL<RT, NY>;
     using V = typename Vec16<RT>::type;
     constexpr int D = NY + 3, G4 = L::G, NGX = L::NGX, NGC = L::NGC, XS = L::XS, CSZ = L::CS, D4 = L::D4,
-                  SPB = L::SPB;
+                  SPB = L::SPB, PFB = L::PFB;
     constexpr unsigned CHUNK_BYTES = HK * D4 * sizeof(RT);
     static_assert(SPB <= kPadSteps, "a record chunk may reach into the padding by at most one chunk");
     static_assert(D4 % G4 == 0 && (CHUNK_BYTES % 16) == 0, "hand-off chunks are whole 16-byte vectors");
@@ -301,7 +300,6 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
     __syncthreads();
     cluster_sync();
 
-    const bool nr = v.scheme == SCFD_SCHEME_NR;
     const bool q2d = v.dim == SCFD_DIM_Q2D;
     // running uses (over all tasks of this cluster) of this CTA's rings
     unsigned rc = 0;  // record chunks
@@ -356,13 +354,6 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                 outA[k] = RT(0);
                 outB[k] = RT(0);
             }
-            double res = 0.0;
-            // smallest omega candidate q / (-Dq) of the lane.  FP64 keeps it as the
-            // pair (q, -Dq), compared by cross-multiplication; FP32 keeps the ratio
-            // (fast divide), since species held at the density floor would underflow
-            // an FP32 cross product.
-            constexpr bool f32 = sizeof(RT) == 4;
-            RT on = RT(__longlong_as_double(0x7FF0000000000000ll)), od = RT(1);
             // The hand-off.  Chunk j of the strip below holds the columns 4j-3 .. 4j
             // (HK = 4) of its top row: its lane 31 computes column c at its step c + 31,
             // so its group of steps G (4G .. 4G+3) yields exactly chunk G - 7.  Lane 0
@@ -491,25 +482,6 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                         V* dstx = reinterpret_cast<V*>(sx + pos * XS) + lf;
 #pragma unroll
                         for (int g = 0; g < NGX; ++g) dstx[g * 32] = *reinterpret_cast<V*>(&fx[g * G4]);
-                        if (DIR == 1 && nr) {
-                            const double dE = double(x[NY + 2]);
-                            res = res + dE * dE;
-                            const RT rho = f[F::RHO];
-#pragma unroll
-                            for (int k = 0; k < NY; ++k) {
-                                // smallest q_k/(-Dq_k) over Dq_k < 0
-                                const RT dk = x[k];
-                                const RT qn = rho * f[F::Y + k], qd = -dk;
-                                if constexpr (f32) {
-                                    if (dk < RT(0)) on = fminf(on, __fdividef(qn, qd));
-                                } else {
-                                    if (dk < RT(0) && qn * od < on * qd) {
-                                        on = qn;
-                                        od = qd;
-                                    }
-                                }
-                            }
-                        }
                         // lane 31: entry u of chunk J in this CTA's xout ring
                         if (pub && lane == 31) {
                             RT vals[D4];
@@ -545,22 +517,6 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&rdone[slot]);
                 ++rc;
-            }
-            if (DIR == 1 && nr && !bail) {
-                for (int o = 16; o > 0; o >>= 1) {
-                    res += __shfl_xor_sync(0xffffffffu, res, o);
-                    const RT on2 = __shfl_xor_sync(0xffffffffu, on, o), od2 = __shfl_xor_sync(0xffffffffu, od, o);
-                    if (on2 * od < on * od2) {  // FP32: od = 1, a plain minimum of the ratios
-                        on = on2;
-                        od = od2;
-                    }
-                }
-                if (lane == 0) {
-                    const double om = double(on) / double(od) * v.dq_max;  // -q/Dq*Dqmax of the limiting cell
-                    a.partials[2 * fs] = res;
-                    a.partials[2 * fs + 1] = om;
-                    if (om < v.omega_min) atomicMax(&v.sc->status, SCFD_E_OMEGA);
-                }
             }
         } else if (warp == 1 && active) {
             // ------------------------------------------------------------ helper warp
@@ -669,8 +625,77 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
 }
 
 // ---------------------------------------------------------------------------
+// k_omega: the NR relaxation's candidates from the backward sweep's result
+// (time_NR_viscous.f90:56-78): per block of 32 steps x 32 lanes of a strip,
+// res = sum of Dq(E)^2 and omega = min over Dq_k < 0 of -q_k / Dq_k * Dqmax,
+// into partials[2 b], partials[2 b + 1].  Records are read coalesced (step y,
+// lane x) and turned to cells (step x, lane y) through shared memory, so that
+// q is read along rows.
+// ---------------------------------------------------------------------------
+template <typename T, int NY>
+__global__ void __launch_bounds__(1024) k_omega(View v, const int2* blk, const int4* strips, const long long* step_off,
+                                                const T* X, double* partials) {
+    using L = WL<T, NY>;
+    constexpr int G = L::G;
+    __shared__ double tile[32][33];
+    const int2 b = blk[blockIdx.x];
+    const int4 st = strips[b.x];
+    const int p = st.x, s = st.y;
+    const int ni = v.P.ni[p], nj = v.P.nj[p];
+    const T* in = X + (step_off[b.x] + kPadSteps + b.y) * L::XS;
+    const int nt = min(32, ni + 31 - b.y);
+    const long long N = v.ncell;
+    const bool rd = (int)threadIdx.y < nt;
+    const long long rbase = (long long)threadIdx.y * L::XS + threadIdx.x * G;
+    const int tt = threadIdx.x, l = threadIdx.y;
+    const int t = b.y + tt, cc = t - l, j = 32 * s + 1 + l;
+    const bool wr = tt < nt && cc >= 0 && cc < ni && j <= nj;
+    const long long c = wr ? cidx(v.P, p, cc + 1, j) : 0;
+    double res = 0.0, om = 1e300;
+    for (int m = 0; m <= NY; ++m) {
+        const int k = m < NY ? m : NY + 2;  // the species, then the energy
+        const double cur = rd ? double(in[rbase + (long long)(k / G) * 32 * G + k % G]) : 0.0;
+        const double qk = (wr && m < NY) ? v.q[k * N + c] : 0.0;
+        tile[threadIdx.y][threadIdx.x] = cur;
+        __syncthreads();
+        if (wr) {
+            const double dq = tile[tt][l];
+            if (m < NY) {
+                if (dq < 0.0) om = fmin(om, -qk / dq * v.dq_max);
+            } else {
+                res = dq * dq;
+            }
+        }
+        __syncthreads();
+    }
+    double* out = partials + 2 * blockIdx.x;
+    // the block's cells in a fixed order: warps, then lanes
+    for (int d = 16; d > 0; d >>= 1) {
+        res += __shfl_down_sync(0xffffffffu, res, d);
+        om = fmin(om, __shfl_down_sync(0xffffffffu, om, d));
+    }
+    if (threadIdx.x == 0) {
+        tile[0][threadIdx.y] = res;
+        tile[1][threadIdx.y] = om;
+    }
+    __syncthreads();
+    if (threadIdx.y == 0) {
+        res = tile[0][threadIdx.x];
+        om = tile[1][threadIdx.x];
+        for (int d = 16; d > 0; d >>= 1) {
+            res += __shfl_down_sync(0xffffffffu, res, d);
+            om = fmin(om, __shfl_down_sync(0xffffffffu, om, d));
+        }
+        if (threadIdx.x == 0) {
+            out[0] = res;
+            out[1] = om;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // k_unpack: q += omega * Dq from the records (LU-SGS: omega = 1; NR: the
-// positivity-limited omega reduced from the per-strip partials in fixed order,
+// positivity-limited omega reduced from k_omega's per-block partials in fixed order,
 // time_NR_viscous.f90:86-108).
 // ---------------------------------------------------------------------------
 template <typename T, int NY>
@@ -680,28 +705,22 @@ __global__ void __launch_bounds__(1024) k_unpack(View v, const int2* blk, const 
     using L = WL<T, NY>;
     constexpr int D = NY + 3, G = L::G;
     __shared__ double tile[32][33];
-    __shared__ double s_om;
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        double om = 1.0;
-        if (nr_mode) {
-            double res = 0.0, o = 1e300;
-            for (int k = 0; k < nstrips; ++k) {
-                res += partials[2 * k];
-                o = fmin(o, partials[2 * k + 1]);
-            }
-            om = fmin(v.omega_max, o);
-            if (blockIdx.x == 0) {
-                if (inner == 1) v.sc->res1 = res;
-                v.sc->res = res;
-                v.sc->omega = om;
-                log_inner(v.sc, inner, o, res);
-            }
+    double om = 1.0;
+    if (nr_mode) {
+        // every block reduces the partials alike (fixed order)
+        double res, o;
+        reduce_partials(partials, nstrips, res, o);
+        if (blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+            if (o < v.omega_min) atomicMax(&v.sc->status, SCFD_E_OMEGA);
+            if (inner == 1) v.sc->res1 = res;
+            v.sc->res = res;
+            v.sc->omega = fmin(v.omega_max, o);
+            log_inner(v.sc, inner, o, res);
         }
-        s_om = om;
+        // time_NR_viscous.f90:75-78: below omega_min the step stops without the update
+        if (o < v.omega_min || v.sc->status == SCFD_E_OMEGA) return;
+        om = fmin(v.omega_max, o);
     }
-    __syncthreads();
-    if (nr_mode && v.sc->status == SCFD_E_OMEGA) return;
-    const double om = s_om;
     const int2 b = blk[blockIdx.x];
     const int4 st = strips[b.x];
     const int p = st.x, s = st.y;
@@ -814,7 +833,7 @@ template <typename RT, int NY, int DIR>
 void sweep_launch(const View& v, cudaStream_t s, const Wave& w) {
     using L = WL<RT, NY>;
     WaveArgs a{DIR == 0 ? w.tasks_f : w.tasks_b, w.ntasks,    w.step_off, w.X, w.C, w.xfer, w.xstride,
-               w.progress + (DIR == 0 ? 0 : w.ntasks), w.tickets + (DIR == 0 ? 0 : 1), w.partials};
+               w.progress + (DIR == 0 ? 0 : w.ntasks), w.tickets + (DIR == 0 ? 0 : 1)};
     const int ncl = w.nclusters < w.ntasks ? w.nclusters : w.ntasks;
     k_wave<RT, NY, DIR><<<ncl * CL, 64, L::SMEM, s>>>(v, a);
 }
@@ -829,6 +848,9 @@ void run_t(const View& v, cudaStream_t s, const Wave& w, int what, int inner) {
         k_unpack<RT, NY><<<w.nblk, dim3(32, 32), 0, s>>>(v, w.blk, w.strips, w.step_off,
                                                          reinterpret_cast<const RT*>(w.X), w.partials, w.nstrips,
                                                          nr ? 1 : 0, inner);
+    } else if (what == 4) {
+        k_omega<RT, NY><<<w.nblk, dim3(32, 32), 0, s>>>(v, w.blk, w.strips, w.step_off,
+                                                        reinterpret_cast<const RT*>(w.X), w.partials);
     } else if (what == 1) {
         sweep_launch<RT, NY, 0>(v, s, w);
     } else {
@@ -838,7 +860,8 @@ void run_t(const View& v, cudaStream_t s, const Wave& w, int what, int inner) {
 
 }  // namespace
 
-// what: 0 pack, 1 forward sweep, 2 backward sweep, 3 unpack/update
+// what: 0 pack, 1 forward sweep, 2 backward sweep, 3 unpack/update, 4 the NR
+// partials (res, omega) of the backward sweep's result
 int launch_wave(const View& v, cudaStream_t s, const Wave& w, int what, int inner) {
     const bool mixed = v.precision == SCFD_PREC_MIXED;
     switch (v.nY) {

@@ -455,6 +455,7 @@ struct Seq {
             n += timed(c, SCFD_K_PACK, [&] { return launch_wave(v, s, c->sw3, 0, 0); });
             n += timed(c, SCFD_K_SWEEP_FWD, [&] { return launch_wave(v, s, c->sw3, 1, 0); });
             n += timed(c, SCFD_K_SWEEP_BWD, [&] { return launch_wave(v, s, c->sw3, 2, 0); });
+            if (c->d.scheme == SCFD_SCHEME_NR) n += timed(c, SCFD_K_UPDATE, [&] { return launch_wave(v, s, c->sw3, 4, 0); });
             return;
         }
         n += timed(c, SCFD_K_SWEEP_FWD, [&] {
@@ -466,7 +467,8 @@ struct Seq {
                                 c->d_strips_f, c->d_strips_b);
         });
     }
-    // the per-strip (res, omega) partials of the last backward sweep
+    // the (res, omega) partials of the last backward sweep: per pack block
+    // (k_omega) on the wavefront path, per strip on the one-warp-per-strip path
     const double* partials() const { return c->use_sw3 ? c->sw3.partials : c->d_partials; }
     int nstrips() const { return c->use_sw3 ? c->sw3.nstrips : c->nsb; }
     // q update after the sweeps: NR relaxes with the omega reduced from
@@ -809,7 +811,7 @@ int scfd_commit(scfd_ctx* c) {
     bytes += need<DevScalars>(1);
     bytes += 2 * need<int>(2 * c->nsf);
     bytes += need<double>((size_t)c->nsf * (c->nimax + 8) * D);
-    bytes += need<int>(c->nsf + c->nsb) + need<int>(2) + need<double>(2 * c->nsb);
+    bytes += need<int>(c->nsf + c->nsb) + need<int>(2) + need<double>(2 * std::max<size_t>(c->nsb, blks3.size() / 2));
     bytes += need<GhostOp>(std::max(1, c->nops)) + need<double>(std::max<size_t>(1, c->bcs.size()) * c->valstride);
     bytes += need<long long>(std::max(1, c->nexp)) + need<HaloImport>(std::max(1, c->nimp)) +
              need<double>(std::max<long long>(1, c->seg * c->nranks)) + need<double>(8);
@@ -865,7 +867,7 @@ int scfd_commit(scfd_ctx* c) {
     c->d_xfer = carve<double>(p, (size_t)c->nsf * (c->nimax + 8) * D);
     c->d_progress = carve<int>(p, c->nsf + c->nsb);
     c->d_tickets = carve<int>(p, 2);
-    c->d_partials = carve<double>(p, 2 * c->nsb);
+    c->d_partials = carve<double>(p, 2 * std::max<size_t>(c->nsb, blks3.size() / 2));
     c->d_ops = carve<GhostOp>(p, std::max(1, c->nops));
     c->d_exp = carve<long long>(p, std::max(1, c->nexp));
     c->d_imp = carve<HaloImport>(p, std::max(1, c->nimp));
@@ -909,7 +911,7 @@ int scfd_commit(scfd_ctx* c) {
         w3.blk = reinterpret_cast<const int2*>(bk);
         w3.nblk = (int)blks3.size() / 2;
         w3.strips = reinterpret_cast<const int4*>(sp);
-        w3.nstrips = c->nsf;
+        w3.nstrips = w3.nblk;  // k_omega's partials: one per pack block
         w3.tasks_f = reinterpret_cast<const int4*>(tf);
         w3.tasks_b = reinterpret_cast<const int4*>(tb);
         w3.ntasks = ntasks;

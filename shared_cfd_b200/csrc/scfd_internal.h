@@ -117,6 +117,46 @@ __device__ __forceinline__ void log_inner(DevScalars* sc, int inner, double omeg
     }
 }
 
+// (res, omega) of n partials (pairs), reduced by every thread of a block of
+// up to 1024 threads in a fixed order (the same value in every block and every
+// run): res summed, omega the minimum.  Every thread of the block must call it.
+__device__ __forceinline__ void reduce_partials(const double* part, int n, double& res, double& om) {
+    __shared__ double s_r[32], s_o[32];
+    const int tid = (threadIdx.z * blockDim.y + threadIdx.y) * blockDim.x + threadIdx.x;
+    const int nth = blockDim.x * blockDim.y * blockDim.z;
+    const int lane = tid & 31, wid = tid >> 5, nw = (nth + 31) >> 5;
+    double r = 0.0, o = 1e300;
+    for (int k = tid; k < n; k += nth) {
+        r += part[2 * k];
+        o = fmin(o, part[2 * k + 1]);
+    }
+    for (int d = 16; d > 0; d >>= 1) {
+        r += __shfl_down_sync(0xffffffffu, r, d);
+        o = fmin(o, __shfl_down_sync(0xffffffffu, o, d));
+    }
+    __syncthreads();  // s_r / s_o may still be read by a previous call
+    if (lane == 0) {
+        s_r[wid] = r;
+        s_o[wid] = o;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        r = lane < nw ? s_r[lane] : 0.0;
+        o = lane < nw ? s_o[lane] : 1e300;
+        for (int d = 16; d > 0; d >>= 1) {
+            r += __shfl_down_sync(0xffffffffu, r, d);
+            o = fmin(o, __shfl_down_sync(0xffffffffu, o, d));
+        }
+        if (lane == 0) {
+            s_r[0] = r;
+            s_o[0] = o;
+        }
+    }
+    __syncthreads();
+    res = s_r[0];
+    om = s_o[0];
+}
+
 // All device pointers of a context; passed by value to the kernels.
 struct View {
     Planes P;
@@ -182,7 +222,7 @@ struct Wave {
     long long xstride;          // elements per task
     int* progress;              // 2*ntasks
     int* tickets;               // 2
-    double* partials;           // 2*nstrips
+    double* partials;           // (res, omega) per pack block: 2*nstrips, nstrips = nblk
 };
 struct WaveSizes {
     int xs, cs, d4;  // elements of an X / C step block; padded hand-off column

@@ -34,12 +34,8 @@ def _sharded(case, lib, owner, nsteps):
         for s in ranks:
             s.upload()
             s.prepare(1)
-        attempts = [0] * nr
         for n in range(nsteps):
-            stats = lockstep(ranks, 1 + n)
-            attempts = [a + st.chem_attempts for a, st in zip(attempts, stats)]
-        for st, a in zip(stats, attempts):
-            st.chem_attempts = a  # over all steps, as scfd_run reports
+            stats = lockstep(ranks, 1 + n)  # the last step's, as scfd_run reports
         outs = []
         for s in ranks:
             q, w, vhi, tt = s.download()
