@@ -764,6 +764,7 @@ def main():
     unit = unit_of(args.config)
     res = {}
     solvers = {}
+    q_after = {}
     pieces = shard_pieces(args.config, world)
     for prec, tag in ((abi.PREC_FP64, "fp64"), (abi.PREC_MIXED, "mixed")):
         case = make_case(args.config, args.scale, prec)
@@ -777,6 +778,8 @@ def main():
         s.prepare(1)
         ms, st, nl, clk = time_resident(s, args.steps, args.warmup, torch, dev, dev, barrier)
         ms = max_over_ranks(ms)
+        # the state after the warm-up and timed steps, for the mixed-vs-FP64 error
+        q_after[tag] = s.gather()[0] if sharded else s.download()[0]
         # strong scaling under sharding: the ranks share one workload
         units = case.ncells * iters_per_step(case) * args.steps * (1 if sharded else world)
         om, rr = s.inner_log() if case.desc.scheme == abi.SCHEME_NR else (np.zeros(0), np.zeros(0))
@@ -817,12 +820,11 @@ def main():
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": unit, "cores": cores, "kind": "port", "sample": "failed: %s" % e}
 
-    # the mixed path against the FP64 path after the timed steps
+    # the mixed path against the FP64 path after the same warm-up + timed steps
+    # from the same initial state
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from helpers import rel_l2
-    qm = solvers["mixed"][0].gather()[0] if sharded else solvers["mixed"][0].download()[0]
-    qd = solvers["fp64"][0].gather()[0] if sharded else solvers["fp64"][0].download()[0]
-    l2_mixed_fp64 = rel_l2(solvers["fp64"][1], qm, qd)
+    l2_mixed_fp64 = rel_l2(solvers["fp64"][1], q_after["mixed"], q_after["fp64"])
 
     if rank == 0:
         d, m = res["fp64"], res["mixed"]
@@ -846,7 +848,8 @@ def main():
                        "last_step_inner_omega": d["inner_omega"], "last_step_inner_res_ratio": d["inner_res_ratio"]},
             "mixed": {"value": m["value"], "unit": unit, "ms_per_step": m["ms"] / args.steps,
                       "over_fp64": m["value"] / d["value"], "e2e": e2e["mixed"], "gpu_launches": m["launches"],
-                      "clocks": m["clocks"], "roofline": roof["mixed"], "l2_vs_fp64_gpu": l2_mixed_fp64,
+                      "clocks": m["clocks"], "roofline": roof["mixed"],
+                      "l2_vs_fp64_gpu": {"value": l2_mixed_fp64, "steps": args.warmup + args.steps},
                       "dtype": "f32 reconstruction, fluxes and sweeps; f64 thermo, chemistry, sums, updates",
                       "status": {"code": m["status"], "omega": m["omega"],
                                  "last_step_inner_omega": m["inner_omega"]}},

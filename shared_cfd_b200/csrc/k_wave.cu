@@ -365,8 +365,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
             const unsigned xc0 = xc;
             unsigned xw = xc;  // chunks awaited (running, like xc)
             auto await_chunk = [&]() -> bool {
-                bool ok = true;
-                if (lane == 0) ok = wait_phase(&xfull[xw % HS], (xw / HS) & 1u, v, s_bail);
+                const bool ok = wait_phase(&xfull[xw % HS], (xw / HS) & 1u, v, s_bail);
                 ++xw;
                 return __all_sync(0xffffffffu, ok);
             };
@@ -391,9 +390,8 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                     const bool pub = (pub_remote || pub_global) && J >= 0 && J <= lastc;
                     const unsigned ps = pc % HS;
                     if (pub && pc >= HS) {
-                        bool okp = true;
-                        if (lane == 31)
-                            okp = wait_phase(pub_remote ? &pempty[ps] : &oemp[ps], ((pc / HS) - 1u) & 1u, v, s_bail);
+                        const bool okp =
+                            wait_phase(pub_remote ? &pempty[ps] : &oemp[ps], ((pc / HS) - 1u) & 1u, v, s_bail);
                         if (!__all_sync(0xffffffffu, okp)) {
                             if (lane == 31) give_up(v, s_bail);
                             bail = true;
@@ -420,11 +418,16 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                         // column t from the strip below (lane 0)
                         const bool in_col = has_prev && t < ni;
                         const RT* xi = xin + (((xc0 + (unsigned)((t + 3) >> 2)) % HS) * HK + ((t + 3) & 3)) * D4;
+                        // every lane reads the column (16-byte shared-memory broadcasts); lane 0 uses it
+                        RT xv[D4];
+#pragma unroll
+                        for (int g = 0; g < D4 / G4; ++g)
+                            *reinterpret_cast<V*>(&xv[g * G4]) = reinterpret_cast<const V*>(xi)[g];
                         RT inB[D];
 #pragma unroll
                         for (int k = 0; k < D; ++k) {
                             const RT sh = __shfl_up_sync(0xffffffffu, outB[k], 1);
-                            inB[k] = lane == 0 ? (in_col ? xi[k] : RT(0)) : sh;
+                            inB[k] = lane == 0 ? (in_col ? xv[k] : RT(0)) : sh;
                         }
                         // this lane's cell
                         RT fx[NGX * G4], f[NGC * G4];
