@@ -89,18 +89,18 @@ def workload_name(config, scale):
         ("" if scale == 1.0 else " (scale %g)" % scale)
 
 
-# algorithmic HBM bytes per interior cell and launch, FP64 storage
-# DRAM bytes (read + write) per interior cell and launch, from an ncu capture of
-# the reacting step at scale 0.5 (196 608 cells; ncu flushes the caches before each
-# launch, so these are cold-cache figures), residual tile pinned to 16x16:
-#   SCFD_RES_TILE=1 ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
-#       --clock-control none -k regex:"k_residual2|k_thermo|k_pack|k_unpack|k_sweep3" -c 80 --csv
-#       python bench.py --scale 0.5 --steps 1 --warmup 1 --no-cpu-baseline
-# None of these kernels reuses data across launches, so the traffic of a launch
-# grows with the cell count and is scaled to the workload by cells.
+# DRAM bytes (read + write) per interior cell and launch of this build, from ncu
+# captures of the reacting step at scale 0.5 (196 608 cells; ncu flushes the caches
+# before each launch, so reads are cold, and writes still in L2 at a launch's end are
+# not counted); commands in profiles/traffic_reacting_step_196k.md.  None of these
+# kernels reuses data across launches, so the traffic of a launch grows with the cell
+# count and is scaled to the workload by cells.  K_UPDATE averages its two launches
+# per inner iteration (k_omega and k_unpack).
 NCU_DRAM_BYTES_PER_CELL = {
-    ("reacting_step", True): {abi.K_THERMO: 494.2, abi.K_RESIDUAL: 549.5, abi.K_PACK: 540.2,
-                              abi.K_SWEEP_FWD: 285.2, abi.K_SWEEP_BWD: 285.3, abi.K_UPDATE: 155.9},
+    ("reacting_step", False): {abi.K_THERMO: 159.3, abi.K_RESIDUAL: 644.8, abi.K_PACK: 542.1,
+                               abi.K_SWEEP_FWD: 417.0, abi.K_SWEEP_BWD: 418.0, abi.K_UPDATE: 197.0},
+    ("reacting_step", True): {abi.K_THERMO: 159.3, abi.K_RESIDUAL: 553.9, abi.K_PACK: 404.7,
+                              abi.K_SWEEP_FWD: 216.2, abi.K_SWEEP_BWD: 216.2, abi.K_UPDATE: 143.2},
 }
 NCU_TRAFFIC_NOTE = "ncu dram__bytes_read+write per cell at scale 0.5 (cold cache), scaled by cells"
 
@@ -120,9 +120,11 @@ def algo_bytes(kind, case, mixed):
         geo = 28 if case.desc.viscous else 14
         return wb * (W + nY) + 8 * ((3 * D if nr else 2 * D) + geo + D + 3)
     if kind in (abi.K_SWEEP_FWD, abi.K_SWEEP_BWD):
-        return 8 * (D + 1 + 4 + 2 * nY + 2 + 4 + 2 + 1 + D + (nY if kind == abi.K_SWEEP_BWD else 0))
+        return 8 * (D + 1 + 4 + 2 * nY + 2 + 4 + 2 + 1 + D)
     if kind == abi.K_UPDATE:
-        return 8 * 3 * D
+        # NR: k_omega (Dq of the species and energy, q of the species) and k_unpack
+        # (q += omega Dq), averaged over the two launches
+        return (8 * (2 * nY + 1) + 8 * 3 * D) // 2 if nr else 8 * 3 * D
     if kind == abi.K_BC:
         return 0
     if kind == abi.K_CHEM:
