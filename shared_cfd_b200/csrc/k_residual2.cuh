@@ -59,7 +59,11 @@ struct Smem {
 
 // the MUSCL limiters get their own phase (FP64 only, see the file comment)
 template <typename RT>
-constexpr bool kSlopePhase = sizeof(RT) == 8;
+constexpr bool kSlopePhase = false;
+// vhi staged in shared memory (FP32); the FP64 faces read it through L1 instead,
+// which keeps the FP64 tile at three CTAs per SM
+template <typename RT>
+constexpr bool kStageVh = sizeof(RT) == 4;
 
 // limiter cells of a direction: i: rows 2 .. TY+1, columns 1 .. TX+2 of the
 // staged tile; j: rows 1 .. TY+2, columns 2 .. TX+1
@@ -179,7 +183,13 @@ __device__ __forceinline__ void face2(const View& v, const Smem<RT>& S, int p, i
         const RT dC = (W_(kw, p1) + W_(kw, p2) - W_(kw, m1) - W_(kw, m2)) * q4;
         const RT dxi = iface ? dN : dC, deta = iface ? dC : dN;
         const RT dwdx = dxi * g11 + deta * g21, dwdr = dxi * g12 + deta * g22;
-        const RT lhi = (S.vh[k * HS + c0] + S.vh[k * HS + cb]) * half;
+        RT lhi;
+        if constexpr (kStageVh<RT>) {
+            lhi = (S.vh[k * HS + c0] + S.vh[k * HS + cb]) * half;
+        } else {
+            const long long cgb = cg + (iface ? 1 : v.P.pitch[p]);
+            lhi = (RT(__ldg(v.vhi + k * N + cg)) + RT(__ldg(v.vhi + k * N + cgb))) * half;
+        }
         hidwdx = hidwdx + dwdx * lhi;
         hidwdr = hidwdr + dwdr * lhi;
         tv[k] = rhoD * dwdx * n1 + rhoD * dwdr * n2;
@@ -205,8 +215,9 @@ __global__ void __launch_bounds__(TL::NTH) k_residual2(View v) {
     extern __shared__ __align__(16) unsigned char smraw[];
     Smem<RT> S;
     S.w = reinterpret_cast<RT*>(smraw);
+    constexpr int NVH = kStageVh<RT> ? NY : 0;  // staged vhi components
     S.vh = S.w + W * HS;
-    S.T = S.vh + NY * HS;
+    S.T = S.vh + NVH * HS;
     S.FI = S.T + HS;
     S.FJ = S.FI + NFI * D;
     S.SL = S.FJ + NFJ * D;
@@ -220,7 +231,7 @@ __global__ void __launch_bounds__(TL::NTH) k_residual2(View v) {
     // stage w, vhi: rows j0-2 .. j0+TY+1, columns i0-2 .. i0+TX+1 (coalesced along i)
     const long long base0 = cidx(v.P, p, i0 - 2, j0 - 2);
     const int pitch = v.P.pitch[p];
-    for (int e = tid; e < (W + NY) * HS; e += NTH) {
+    for (int e = tid; e < (W + NVH) * HS; e += NTH) {
         const int comp = e / HS, rem = e - comp * HS;
         const int jy = rem / HX, ix = rem - jy * HX;
         const int i = i0 - 2 + ix, j = j0 - 2 + jy;
@@ -362,7 +373,7 @@ inline void launch2(const View& v, cudaStream_t s) {
     }
     if (v.P.nact == 0) return;
     dim3 grid((nimax + TX - 1) / TX, (njmax + TY - 1) / TY, v.P.nact);
-    const size_t smem = ((size_t)(W + NY + 1) * TL::HY * TL::HX + (size_t)(TL::NFI + TL::NFJ) * D +
+    const size_t smem = ((size_t)(W + (kStageVh<RT> ? NY : 0) + 1) * TL::HY * TL::HX + (size_t)(TL::NFI + TL::NFJ) * D +
                          (kSlopePhase<RT> ? (size_t)(NY + 6) * SlopeGrid<TL>::NMAX : 0)) * sizeof(RT);
     // the attribute is per device: set it before every launch (host only, cheap)
     cudaFuncSetAttribute(k_residual2<RT, NY, MODE, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
