@@ -9,12 +9,9 @@
 // tile plus a 2-cell halo into shared memory with coalesced loads, then
 // computes the TY(TX+1) i-faces and (TY+1)TX j-faces of the tile from shared
 // memory (about two faces per thread), then sums faces and sources per cell.
-// FP64: per direction, every cell's MUSCL limiter s is formed once (one divide
-// per component and cell) into shared memory before that direction's faces,
-// which read the limiters of their two cells; forming them per face divides
-// twice as often.  FP32 divides are cheap enough that the extra phase costs
-// more than it saves, so the FP32 faces form their limiters themselves.  The
-// limiter's value is the same either way.
+// The FP64 kernel stages w and T only and reads vhi through L1: its 16x8 tile
+// then takes 61 KB of shared memory and three CTAs fit on an SM (with vhi
+// staged, two), which its latency-bound faces need more than the loads.
 // The LU-SGS coefficients are formed later by the record packer, so this
 // kernel writes only the D values of the right-hand side (or the explicit
 // update).  The tile shape is one of residual2_tiles(), picked per context by
@@ -54,24 +51,12 @@ struct Smem {
     RT* T;   // [HY][HX]
     RT* FI;  // [NFI][D]
     RT* FJ;  // [NFJ][D]
-    RT* SL;  // [NY+6][TY][TX+2] (i) or [NY+6][TY+2][TX] (j): MUSCL limiters of one direction
 };
 
-// the MUSCL limiters get their own phase (FP64 only, see the file comment)
-template <typename RT>
-constexpr bool kSlopePhase = false;
 // vhi staged in shared memory (FP32); the FP64 faces read it through L1 instead,
 // which keeps the FP64 tile at three CTAs per SM
 template <typename RT>
 constexpr bool kStageVh = sizeof(RT) == 4;
-
-// limiter cells of a direction: i: rows 2 .. TY+1, columns 1 .. TX+2 of the
-// staged tile; j: rows 1 .. TY+2, columns 2 .. TX+1
-template <typename TL>
-struct SlopeGrid {
-    static constexpr int NI = TL::TY * (TL::TX + 2), NJ = (TL::TY + 2) * TL::TX;
-    static constexpr int NMAX = NI > NJ ? NI : NJ;
-};
 
 }  // namespace
 
@@ -85,23 +70,18 @@ __device__ __forceinline__ void face2(const View& v, const Smem<RT>& S, int p, i
     // smem cell offsets along the face normal: m1, 0 (left), 1 (right), 2
     const int st = iface ? 1 : HX;
     const int c0 = jy * HX + ix;
-    // the limiters of the left and right cells (slopes phase)
-    constexpr int TX = TL::TX, TY = TL::TY;
-    const RT* sA = S.SL + (iface ? (jy - 2) * (TX + 2) + (ix - 1) : (jy - 1) * TX + (ix - 2));
-    const int sB = iface ? 1 : TX;
-    const int sM = iface ? SlopeGrid<TL>::NI : SlopeGrid<TL>::NJ;
     RT wl[NY + 6], wr[NY + 6];
 #pragma unroll
     for (int m = 0; m < NY + 6; ++m) {
         const RT* a = S.w + m * HS + c0;
         const RT wm1 = a[-st], w0 = a[0], w1 = a[st], w2 = a[2 * st];
         RT Du = w1 - w0, Dl = w0 - wm1;
-        RT s = kSlopePhase<RT> ? sA[m * sM] : (two * Du * Dl) / (Du * Du + Dl * Dl + eps_of<RT>());
+        RT s = (two * Du * Dl) / (Du * Du + Dl * Dl + eps_of<RT>());
         const RT du = half * s * ((one + km * s) * Du + (one - km * s) * Dl);
         wl[m] = w0 + phi * half * du;
         Du = w2 - w1;
         Dl = w1 - w0;
-        s = kSlopePhase<RT> ? sA[m * sM + sB] : (two * Du * Dl) / (Du * Du + Dl * Dl + eps_of<RT>());
+        s = (two * Du * Dl) / (Du * Du + Dl * Dl + eps_of<RT>());
         const RT dl = half * s * ((one + km * s) * Dl + (one - km * s) * Du);
         wr[m] = w1 - phi * half * dl;
     }
@@ -220,7 +200,6 @@ __global__ void __launch_bounds__(TL::NTH) k_residual2(View v) {
     S.T = S.vh + NVH * HS;
     S.FI = S.T + HS;
     S.FJ = S.FI + NFI * D;
-    S.SL = S.FJ + NFJ * D;
     const int p = v.P.act[blockIdx.z];
     const int ni = v.P.ni[p], nj = v.P.nj[p];
     const int i0 = blockIdx.x * TX + 1, j0 = blockIdx.y * TY + 1;
@@ -251,58 +230,17 @@ __global__ void __launch_bounds__(TL::NTH) k_residual2(View v) {
         S.T[e] = rr != RT(0) ? S.w[3 * HS + e] / rr / S.w[(D + 3) * HS + e] : RT(0);
     }
     __syncthreads();
-    // MUSCL limiter s = 2 Du Dl / (Du^2 + Dl^2 + eps) (muscl.f90:7-73) of every
-    // cell a face of direction `idir` reconstructs from, component by component
-    auto slopes = [&](bool idir) {
-        constexpr int NI = SlopeGrid<TL>::NI, NJ = SlopeGrid<TL>::NJ;
-        const int ncell = idir ? NI : NJ;
-        const int st = idir ? 1 : HX;
-        const RT two = RT(2);
-        for (int e = tid; e < (NY + 6) * ncell; e += NTH) {
-            const int m = e / ncell, r = e - m * ncell;
-            int ix, jy;
-            if (idir) {
-                jy = r / (TX + 2) + 2;
-                ix = r - (jy - 2) * (TX + 2) + 1;
-            } else {
-                jy = r / TX + 1;
-                ix = r - (jy - 1) * TX + 2;
-            }
-            const RT* a = S.w + m * HS + jy * HX + ix;
-            const RT Du = a[st] - a[0], Dl = a[0] - a[-st];
-            S.SL[e] = (two * Du * Dl) / (Du * Du + Dl * Dl + eps_of<RT>());
-        }
-    };
-    if constexpr (kSlopePhase<RT>) {
-        // i-faces, then j-faces, each after its direction's limiters
-        slopes(true);
-        __syncthreads();
-        for (int f = tid; f < NFI; f += NTH) {
+    // faces: i-faces f < NFI, j-faces after
+    for (int f = tid; f < NFI + NFJ; f += NTH) {
+        if (f < NFI) {
             const int fy = f / (TX + 1), fx = f - fy * (TX + 1);
             const int i = i0 - 1 + fx, j = j0 + fy;
             if (i <= ni && j <= nj) face2<RT, NY, TL>(v, S, p, i, j, fx + 1, fy + 2, true, S.FI + f * D);
-        }
-        __syncthreads();
-        slopes(false);
-        __syncthreads();
-        for (int g = tid; g < NFJ; g += NTH) {
+        } else {
+            const int g = f - NFI;
             const int fy = g / TX, fx = g - fy * TX;
             const int i = i0 + fx, j = j0 - 1 + fy;
             if (i <= ni && j <= nj) face2<RT, NY, TL>(v, S, p, i, j, fx + 2, fy + 1, false, S.FJ + g * D);
-        }
-    } else {
-        // i-faces f < NFI, j-faces after, in one loop
-        for (int f = tid; f < NFI + NFJ; f += NTH) {
-            if (f < NFI) {
-                const int fy = f / (TX + 1), fx = f - fy * (TX + 1);
-                const int i = i0 - 1 + fx, j = j0 + fy;
-                if (i <= ni && j <= nj) face2<RT, NY, TL>(v, S, p, i, j, fx + 1, fy + 2, true, S.FI + f * D);
-            } else {
-                const int g = f - NFI;
-                const int fy = g / TX, fx = g - fy * TX;
-                const int i = i0 + fx, j = j0 - 1 + fy;
-                if (i <= ni && j <= nj) face2<RT, NY, TL>(v, S, p, i, j, fx + 2, fy + 1, false, S.FJ + g * D);
-            }
         }
     }
     __syncthreads();
@@ -373,8 +311,8 @@ inline void launch2(const View& v, cudaStream_t s) {
     }
     if (v.P.nact == 0) return;
     dim3 grid((nimax + TX - 1) / TX, (njmax + TY - 1) / TY, v.P.nact);
-    const size_t smem = ((size_t)(W + (kStageVh<RT> ? NY : 0) + 1) * TL::HY * TL::HX + (size_t)(TL::NFI + TL::NFJ) * D +
-                         (kSlopePhase<RT> ? (size_t)(NY + 6) * SlopeGrid<TL>::NMAX : 0)) * sizeof(RT);
+    const size_t smem =
+        ((size_t)(W + (kStageVh<RT> ? NY : 0) + 1) * TL::HY * TL::HX + (size_t)(TL::NFI + TL::NFJ) * D) * sizeof(RT);
     // the attribute is per device: set it before every launch (host only, cheap)
     cudaFuncSetAttribute(k_residual2<RT, NY, MODE, TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     k_residual2<RT, NY, MODE, TL><<<grid, TL::NTH, smem, s>>>(v);
