@@ -206,7 +206,6 @@ __global__ void __launch_bounds__(TL::NTH) k_residual2(View v) {
     if (i0 > ni || j0 > nj) return;
     const int tid = threadIdx.x;
     const long long N = v.ncell;
-    const bool mixed = sizeof(RT) == 4;
     // stage w, vhi: rows j0-2 .. j0+TY+1, columns i0-2 .. i0+TX+1 (coalesced along i)
     const long long base0 = cidx(v.P, p, i0 - 2, j0 - 2);
     const int pitch = v.P.pitch[p];
@@ -217,10 +216,9 @@ __global__ void __launch_bounds__(TL::NTH) k_residual2(View v) {
         RT val = RT(0);
         if (i <= ni + 2 && j <= nj + 2) {
             const long long c = base0 + (long long)jy * pitch + ix;
-            if (comp < W)
-                val = mixed ? RT(__ldg(v.w32 + comp * N + c)) : RT(__ldg(v.w + comp * N + c));
-            else
-                val = mixed ? RT(__ldg(v.vhi32 + (comp - W) * N + c)) : RT(__ldg(v.vhi + (comp - W) * N + c));
+            // the FP32 tile is rounded from the FP64 state here (the values the
+            // generic kernel's FP32 copies hold)
+            val = comp < W ? RT(__ldg(v.w + comp * N + c)) : RT(__ldg(v.vhi + (comp - W) * N + c));
         }
         S.w[e] = val;  // S.vh follows S.w contiguously
     }

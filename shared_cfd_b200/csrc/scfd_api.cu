@@ -419,6 +419,15 @@ void collect_events(scfd_ctx* c) {
     c->ev_used = 0;
 }
 
+// Whether the residual runs the fused kernel (k_residual2.cuh) rather than the
+// generic one (the conditions of launch_residual and launch_residual2).
+bool fused_residual(const scfd_ctx* c) {
+    const int sch = c->d.scheme;
+    if (sch == SCFD_SCHEME_DUAL || precon_scheme(sch)) return false;
+    if (sch != SCFD_SCHEME_EULER && !c->use_sw3) return false;
+    return c->nY == 1 || c->nY == 8 || c->nY == 9;
+}
+
 // The kernels of one physical step, stage by stage; n counts the launches.
 struct Seq {
     scfd_ctx* c;
@@ -430,7 +439,10 @@ struct Seq {
     void primitive() { n += timed(c, SCFD_K_THERMO, [&] { return launch_thermo(v, s, c->cells_max); }); }
     void bc() {
         n += timed(c, SCFD_K_BC, [&] { return launch_ghosts(v, s, c->d_ops, c->nops, c->d_bcval, c->valstride); });
-        if (v.precision == SCFD_PREC_MIXED) n += timed(c, SCFD_K_OTHER, [&] { return launch_to_f32(v, s); });
+        // FP32 copies of w and vhi for the generic residual kernel (the fused one
+        // rounds its tile from the FP64 state itself)
+        if (v.precision == SCFD_PREC_MIXED && !fused_residual(c))
+            n += timed(c, SCFD_K_OTHER, [&] { return launch_to_f32(v, s); });
     }
     void chem() {
         n += timed(c, SCFD_K_CHEM,
