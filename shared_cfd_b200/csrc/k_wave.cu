@@ -84,20 +84,21 @@ struct Vec16<double> {
 }  // namespace
 
 // Coefficient fields of one cell (set_ABpm's quantities, sch_lusgs.raw.f90:27-50,134-136;
-// NR/q2d/sch_NR.raw.f90:43-50,143-144):
+// NR/q2d/sch_NR.raw.f90:43-50,143-144), formed in FP64 by k_pack:
 //   AL            alpha = 1/(Vol/dt + dsci nuA + dscj nuB)   (NR: 3 Vol/(2 dt))
 //   AA, RQ        alpha*Area and 1/(1 - alpha*Area*dpdq_my)  (q2d pressure source)
-//   G1, HVS       gamma - 1 and 0.5 g1 |u|^2; dpdq = (HVS + DHi, -g1 u, -g1 v, g1)
-//   DH(1:nY)      DHi
+//   G1            gamma - 1
+//   DP(1:nY)      dpdq of the species: 0.5 g1 |u|^2 + DHi
 //   Y(1:nY), U, V, H    the primitive vector (Y, u, v, H) of the split Jacobians
-//   CS            sound speed; nu = |n.u| + CS per direction
-//   FA, N1A, N2A  dsci/2 and vnci;  FB, N1B, N2B  dscj/2 and vncj
-//   RHO           density (q_k = RHO * Y_k for the positivity limiter)
+//   per direction d (A: i, ds = dsci, n = vnci; B: j, ds = dscj, n = vncj), with
+//   fa = ds/2, un = n.u and nu = |un| + sound speed:
+//   P1 = fa n1, P2 = fa n2, PU = fa un, LP = fa (un + nu), LM = fa (un - nu)
 template <int NY>
 struct CF {
-    static constexpr int AL = 0, AA = 1, RQ = 2, G1 = 3, HVS = 4, DH = 5, Y = DH + NY, U = Y + NY, V = U + 1,
-                         H = U + 2, CS = U + 3, FA = U + 4, N1A = FA + 1, N2A = FA + 2, FB = FA + 3, N1B = FA + 4,
-                         N2B = FA + 5, RHO = FA + 6, NC = RHO + 1;
+    static constexpr int AL = 0, AA = 1, RQ = 2, G1 = 3, DP = 4, Y = DP + NY, U = Y + NY, V = U + 1, H = U + 2,
+                         PA = U + 3, PB = PA + 5, NC = PB + 5;
+    // offsets within a direction's block
+    static constexpr int P1 = 0, P2 = 1, PU = 2, LP = 3, LM = 4;
 };
 template <typename RT, int NY>
 struct WL {
@@ -137,10 +138,11 @@ __global__ void __launch_bounds__(1024) k_pack(View v, const int2* blk, const in
     const bool ok = cc >= 0 && cc < ni && j <= nj && t < ni + 31;
     const long long N = v.ncell;
     const long long c = ok ? cidx(v.P, p, i, j) : 0;
-    double al = 0.0, u = 0.0, vv = 0.0, g1 = 0.0, hvs = 0.0, aA = 0.0, rq = 1.0, cs = 0.0, rho = 0.0;
+    double al = 0.0, u = 0.0, vv = 0.0, g1 = 0.0, hvs = 0.0, aA = 0.0, rq = 1.0, cs = 0.0;
+    double dir[2][5] = {};  // P1, P2, PU, LP, LM of directions A (i) and B (j)
     if (ok) {
         const double* w = v.w;
-        rho = w[c];
+        const double rho = w[c];
         const double pr = w[3 * N + c];
         u = w[N + c];
         vv = w[2 * N + c];
@@ -151,6 +153,16 @@ __global__ void __launch_bounds__(1024) k_pack(View v, const int2* blk, const in
         const double nuA = fabs(v.vnci[c] * u + v.vnci[N + c] * vv) + cs;
         const double nuB = fabs(v.vncj[c] * u + v.vncj[N + c] * vv) + cs;
         const double dsa = v.dsci[c], dsb = v.dscj[c], vol = v.Vol[c];
+        for (int d = 0; d < 2; ++d) {
+            const double fa = 0.5 * (d == 0 ? dsa : dsb);
+            const double n1 = d == 0 ? v.vnci[c] : v.vncj[c], n2 = d == 0 ? v.vnci[N + c] : v.vncj[N + c];
+            const double un = n1 * u + n2 * vv, nu = fabs(un) + cs;
+            dir[d][0] = fa * n1;
+            dir[d][1] = fa * n2;
+            dir[d][2] = fa * un;
+            dir[d][3] = fa * (un + nu);
+            dir[d][4] = fa * (un - nu);
+        }
         const double dtl = v.dt_mode == SCFD_DT_LOCAL ? v.dt_mat[c] : v.sc->dt_grbl;
         const double tmp = nr_mode ? 3.0 * vol / (2.0 * dtl) + dsa * nuA + dsb * nuB : vol / dtl + dsa * nuA + dsb * nuB;
         al = 1.0 / tmp;
@@ -168,20 +180,13 @@ __global__ void __launch_bounds__(1024) k_pack(View v, const int2* blk, const in
         if (m == F::AA) return aA;
         if (m == F::RQ) return rq;
         if (m == F::G1) return g1;
-        if (m == F::HVS) return hvs;
-        if (m < F::Y) return v.DHi[(m - F::DH) * N + c];
+        if (m < F::Y) return hvs + v.DHi[(m - F::DP) * N + c];
         if (m < F::U) return v.w[(4 + m - F::Y) * N + c];
         if (m == F::U) return u;
         if (m == F::V) return vv;
         if (m == F::H) return v.w[(D + 2) * N + c];
-        if (m == F::CS) return cs;
-        if (m == F::FA) return 0.5 * v.dsci[c];
-        if (m == F::N1A) return v.vnci[c];
-        if (m == F::N2A) return v.vnci[N + c];
-        if (m == F::FB) return 0.5 * v.dscj[c];
-        if (m == F::N1B) return v.vncj[c];
-        if (m == F::N2B) return v.vncj[N + c];
-        if (m == F::RHO) return rho;
+        if (m < F::PB) return dir[0][m - F::PA];
+        if (m < F::NC) return dir[1][m - F::PB];
         return 0.0;
     };
     const long long s0 = step_off[b.x] + kPadSteps + b.y;
@@ -442,11 +447,12 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
 #pragma unroll
                         for (int k = 0; k < D; ++k)
                             x[k] = DIR == 0 ? al * (fx[k] + (outA[k] + inB[k])) : fx[k] - al * (outA[k] + inB[k]);
-                        // dpdq (sch_NR.raw.f90:143-144): species hvs + DHi, then -g1 u, -g1 v, g1
+                        // dpdq (sch_NR.raw.f90:143-144): species hvs + DHi (from the record),
+                        // then -g1 u, -g1 v, g1
                         const RT g1 = f[F::G1], uu = f[F::U], vv = f[F::V];
                         RT dp[D];
 #pragma unroll
-                        for (int k = 0; k < NY; ++k) dp[k] = f[F::HVS] + f[F::DH + k];
+                        for (int k = 0; k < NY; ++k) dp[k] = f[F::DP + k];
                         dp[NY] = -g1 * uu;
                         dp[NY + 1] = -g1 * vv;
                         dp[NY + 2] = g1;
@@ -464,20 +470,18 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                         P += dp[NY + 1] * x[NY + 1];
 #pragma unroll
                         for (int dn = 0; dn < 2; ++dn) {
-                            const int b0 = dn == 0 ? F::FA : F::FB;
-                            const RT fa = f[b0], n1 = f[b0 + 1], n2 = f[b0 + 2];
-                            const RT un = n1 * uu + n2 * vv;
-                            const RT nu = (un < RT(0) ? -un : un) + f[F::CS];
-                            // ds/2 folded into the coefficients: o = cv (fa base) + (fa lam) x [+ (fa P) n]
-                            const RT fb = fa * (n1 * x[NY] + n2 * x[NY + 1] - un * S);
-                            const RT fl = fa * (DIR == 0 ? un + nu : un - nu);
-                            const RT fp = fa * P;
+                            // ds/2 folded into the direction's coefficients (k_pack):
+                            // o = (Y, u, v, H) fb + (fa lam) x + (fa n1, fa n2, fa un) P
+                            const int b0 = dn == 0 ? F::PA : F::PB;
+                            const RT p1 = f[b0 + F::P1], p2 = f[b0 + F::P2], pu = f[b0 + F::PU];
+                            const RT fl = f[b0 + (DIR == 0 ? F::LP : F::LM)];
+                            const RT fb = p1 * x[NY] + p2 * x[NY + 1] - pu * S;
                             RT* o = dn == 0 ? outA : outB;
 #pragma unroll
                             for (int k = 0; k < NY; ++k) o[k] = f[F::Y + k] * fb + fl * x[k];
-                            o[NY] = uu * fb + fl * x[NY] + n1 * fp;
-                            o[NY + 1] = vv * fb + fl * x[NY + 1] + n2 * fp;
-                            o[NY + 2] = f[F::H] * fb + fl * x[NY + 2] + un * fp;
+                            o[NY] = uu * fb + fl * x[NY] + p1 * P;
+                            o[NY + 1] = vv * fb + fl * x[NY + 1] + p2 * P;
+                            o[NY + 2] = f[F::H] * fb + fl * x[NY + 2] + pu * P;
                         }
                         // results back into the slot (16-byte stores); the helper writes them out
 #pragma unroll
