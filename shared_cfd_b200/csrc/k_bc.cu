@@ -14,78 +14,89 @@ namespace scfd {
 
 
 
+// One thread per (ghost op, component): component m < W of w, then vhi.
 __global__ void k_ghost(View v, const GhostOp* ops, int nops, const double* bcval, int valstride) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nops) return;
-    const GhostOp op = ops[t];
+    const int W = v.W, nY = v.nY, NC = W + nY;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)nops * NC) return;
+    const int m = (int)(t / nops), o = (int)(t - (long long)m * nops);
+    const GhostOp op = ops[o];
     const long long N = v.ncell;
-    const int W = v.W, nY = v.nY;
-    double* w = v.w;
-    double* vhi = v.vhi;
     const long long d = op.dst, s = op.src;
     const double* val = bcval + (long long)op.bc * valstride;
+    if (m >= W) {  // vhi
+        const int k = m - W;
+        v.vhi[k * N + d] = (op.kind == SCFD_BC_FIXED || op.kind == SCFD_BC_FIXED_PIN) ? val[W + k] : v.vhi[k * N + s];
+        return;
+    }
+    const double* w = v.w;
+    double r;
     switch (op.kind) {
         case SCFD_BC_FIXED:
-            for (int k = 0; k < W; ++k) w[k * N + d] = val[k];
-            for (int k = 0; k < nY; ++k) vhi[k * N + d] = val[W + k];
-            return;
+            r = val[m];
+            break;
         case SCFD_BC_FIXED_PIN: {
             const double pin = w[3 * N + s];
-            for (int k = 0; k < W; ++k) w[k * N + d] = val[k];
-            for (int k = 0; k < nY; ++k) vhi[k * N + d] = val[W + k];
-            w[d] = pin * val[W + nY] / val[W + nY + 1];
-            w[3 * N + d] = pin;
-            return;
+            r = m == 0 ? pin * val[W + nY] / val[W + nY + 1] : (m == 3 ? pin : val[m]);
+            break;
         }
+        case SCFD_BC_OUTFLOW_P:
+            r = m == 3 ? val[0] : w[m * N + s];
+            break;
+        case SCFD_BC_SLIP:
+            if (m == 1 || m == 2) {
+                const double u = w[N + s], vv = w[2 * N + s];
+                const double un = u * op.n1 + vv * op.n2;
+                r = m == 1 ? u - 2.0 * un * op.n1 : vv - 2.0 * un * op.n2;
+            } else {
+                r = w[m * N + s];
+            }
+            break;
+        case SCFD_BC_NOSLIP:
+            r = (m == 1 || m == 2) ? val[m - 1] * 2.0 - w[m * N + s] : w[m * N + s];
+            break;
         default:
+            r = w[m * N + s];
             break;
     }
-    for (int k = 0; k < W; ++k) w[k * N + d] = w[k * N + s];
-    for (int k = 0; k < nY; ++k) vhi[k * N + d] = vhi[k * N + s];
-    if (op.kind == SCFD_BC_OUTFLOW_P) {
-        w[3 * N + d] = val[0];
-    } else if (op.kind == SCFD_BC_SLIP) {
-        const double u = w[N + s], vv = w[2 * N + s];
-        const double un = u * op.n1 + vv * op.n2;
-        w[N + d] = u - 2.0 * un * op.n1;
-        w[2 * N + d] = vv - 2.0 * un * op.n2;
-    } else if (op.kind == SCFD_BC_NOSLIP) {
-        w[N + d] = val[0] * 2.0 - w[N + s];
-        w[2 * N + d] = val[1] * 2.0 - w[2 * N + s];
-    }
+    v.w[m * N + d] = r;
 }
 
+// set_corners (condition.tail.f90:331-356): one thread per (plane, corner, component)
 __global__ void k_corners(View v) {
-    const int t = threadIdx.x;
-    if ((t >> 2) >= v.P.nact) return;
-    const int p = v.P.act[t >> 2];
-    const int pi = (t & 1) ? 1 : -1, pj = (t & 2) ? 1 : -1;
+    const int NC = v.W + v.nY;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 4 * v.P.nact * NC) return;
+    const int m = t % NC, pc = t / NC;
+    const int p = v.P.act[pc >> 2];
+    const int pi = (pc & 1) ? 1 : -1, pj = (pc & 2) ? 1 : -1;
     const int i = pi < 0 ? 1 : v.P.ni[p];
     const int j = pj < 0 ? 1 : v.P.nj[p];
     const long long N = v.ncell;
     const long long a = cidx(v.P, p, i, j), b = cidx(v.P, p, i, j + pj), c = cidx(v.P, p, i + pi, j);
     const long long d = cidx(v.P, p, i + pi, j + pj);
-    for (int k = 0; k < v.W; ++k)
-        v.w[k * N + d] = 1.0 / 3.0 * (v.w[k * N + a] + v.w[k * N + b] + v.w[k * N + c]);
-    for (int k = 0; k < v.nY; ++k)
-        v.vhi[k * N + d] = 1.0 / 3.0 * (v.vhi[k * N + a] + v.vhi[k * N + b] + v.vhi[k * N + c]);
+    double* f = m < v.W ? v.w + m * N : v.vhi + (m - v.W) * N;
+    f[d] = 1.0 / 3.0 * (f[a] + f[b] + f[c]);
 }
 
 // the ghost-cell writes without set_corners (for stencils that never read corners)
 int launch_ghost_ops(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride) {
     if (nops <= 0) return 0;
-    k_ghost<<<(nops + 127) / 128, 128, 0, s>>>(v, ops, nops, bcval, valstride);
+    const long long nt = (long long)nops * (v.W + v.nY);
+    k_ghost<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(v, ops, nops, bcval, valstride);
     return 1;
 }
 
 int launch_ghosts(const View& v, cudaStream_t s, const GhostOp* ops, int nops, const double* bcval, int valstride) {
     int n = 0;
     if (nops > 0) {
-        k_ghost<<<(nops + 127) / 128, 128, 0, s>>>(v, ops, nops, bcval, valstride);
+        const long long nt = (long long)nops * (v.W + v.nY);
+        k_ghost<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(v, ops, nops, bcval, valstride);
         ++n;
     }
     if (v.P.nact == 0) return n;
-    k_corners<<<1, 4 * v.P.nact, 0, s>>>(v);
+    const int nc = 4 * v.P.nact * (v.W + v.nY);
+    k_corners<<<(nc + 127) / 128, 128, 0, s>>>(v);
     return n + 1;
 }
 
