@@ -58,6 +58,34 @@ struct Smem {
 template <typename RT>
 constexpr bool kStageVh = sizeof(RT) == 4;
 
+// a / b for a positive normal b, without branches, so that the 2 (NY + 6)
+// limiter quotients of a face and the SLAU and viscous ones overlap (the IEEE
+// division's out-of-line slow path keeps them apart; with this one the FP64
+// residual takes 0.42 ms instead of 0.59 at 786 k cells, FP32 0.36 instead of
+// 0.44).  Every denominator it takes is a sum of squares plus eps, a density,
+// a sound speed, gamma - 1 or a positive constant.  Newton-Raphson on the reciprocal from the hardware's
+// approximate reciprocal y0 (rcp.approx.ftz, about 23 bits): FP64 takes one
+// third-order step y1 = y0 (1 + e + e^2), e = 1 - b y0 (relative error about
+// e^3), FP32 one second-order step y1 = y0 (1 + e); then q0 = a y1 and
+// Markstein's remainder correction q = q0 + (a - b q0) y1.  The result is
+// within one unit in the last place of a / b (tests/test_division.py checks the
+// steps in exact arithmetic from seeds 2^-21 off).
+__device__ __forceinline__ double div_pos(double a, double b) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    const double e = fma(-b, y, 1.0);
+    y = fma(fma(e, e, e), y, y);
+    const double q = a * y;
+    return fma(fma(-b, q, a), y, q);
+}
+__device__ __forceinline__ float div_pos(float a, float b) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
+    y = fmaf(fmaf(-b, y, 1.0f), y, y);
+    const float q = a * y;
+    return fmaf(fmaf(-b, q, a), y, q);
+}
+
 }  // namespace
 
 template <typename RT, int NY, typename TL>
@@ -76,12 +104,12 @@ __device__ __forceinline__ void face2(const View& v, const Smem<RT>& S, int p, i
         const RT* a = S.w + m * HS + c0;
         const RT wm1 = a[-st], w0 = a[0], w1 = a[st], w2 = a[2 * st];
         RT Du = w1 - w0, Dl = w0 - wm1;
-        RT s = (two * Du * Dl) / (Du * Du + Dl * Dl + eps_of<RT>());
+        RT s = div_pos(two * Du * Dl, Du * Du + Dl * Dl + eps_of<RT>());
         const RT du = half * s * ((one + km * s) * Du + (one - km * s) * Dl);
         wl[m] = w0 + phi * half * du;
         Du = w2 - w1;
         Dl = w1 - w0;
-        s = (two * Du * Dl) / (Du * Du + Dl * Dl + eps_of<RT>());
+        s = div_pos(two * Du * Dl, Du * Du + Dl * Dl + eps_of<RT>());
         const RT dl = half * s * ((one + km * s) * Dl + (one - km * s) * Du);
         wr[m] = w1 - phi * half * dl;
     }
@@ -94,21 +122,22 @@ __device__ __forceinline__ void face2(const View& v, const Smem<RT>& S, int p, i
     {
         const RT rhol = wl[0], ul = wl[1], vl = wl[2], pl = wl[3], gl = wl[4 + NY];
         const RT rhor = wr[0], ur = wr[1], vr = wr[2], pr = wr[3], gr = wr[4 + NY];
-        const RT al = sqrt(gl * pl / rhol), ar = sqrt(gr * pr / rhor);
+        const RT al = sqrt(div_pos(gl * pl, rhol)), ar = sqrt(div_pos(gr * pr, rhor));
         const RT unl = n1 * ul + n2 * vl, unr = n1 * ur + n2 * vr;
         const RT dp = pr - pl;
         const RT a_bar = half * (ar + al);
         const RT p_bar = half * (pr + pl);
-        const RT ml = unl / a_bar, mr = unr / a_bar;
-        const RT m_tilde = fmin(one, one / a_bar * sqrt(half * (ul * ul + vl * vl + ur * ur + vr * vr)));
+        const RT ia = div_pos(one, a_bar);
+        const RT ml = unl * ia, mr = unr * ia;
+        const RT m_tilde = fmin(one, ia * sqrt(half * (ul * ul + vl * vl + ur * ur + vr * vr)));
         const RT chi = (one - m_tilde) * (one - m_tilde);
         const RT gp = -fmax(fmin(ml, RT(0)), -one);
         const RT gm = fmin(fmax(mr, RT(0)), one);
         const RT g = gp * gm;
-        const RT ub = (fabs(unr) * rhor + fabs(unl) * rhol) / (rhor + rhol);
+        const RT ub = div_pos(fabs(unr) * rhor + fabs(unl) * rhol, rhor + rhol);
         const RT ubp = (one - g) * ub + g * fabs(unl);
         const RT ubm = (one - g) * ub + g * fabs(unr);
-        const RT dm = half * (rhol * (unl + ubp) + rhor * (unr - ubm) - chi / a_bar * dp);
+        const RT dm = half * (rhol * (unl + ubp) + rhor * (unr - ubm) - chi * ia * dp);
         const RT betar = fabs(mr) < one ? RT(0.25) * (two + mr) * ((mr - one) * (mr - one)) : half * (one - copysign(one, mr));
         const RT betal = fabs(ml) < one ? RT(0.25) * (two - ml) * ((ml + one) * (ml + one)) : half * (one + copysign(one, ml));
         const RT pt = p_bar + half * (betal - betar) * (pl - pr) + (one - chi) * (betar + betal - one) * p_bar;
@@ -139,8 +168,8 @@ __device__ __forceinline__ void face2(const View& v, const Smem<RT>& S, int p, i
     const RT gamm = (W_(ig, c0) + W_(ig, cb)) * half;
     const RT Rgas = (W_(iR, c0) + W_(iR, cb)) * half;
     const RT mu = (W_(imu, c0) + W_(imu, cb)) * half;
-    const RT Dd = mu / rho / RT(v.schmidt);
-    const RT k_heat = mu * gamm / (gamm - one) * Rgas / RT(v.prandtl);
+    const RT Dd = div_pos(div_pos(mu, rho), RT(v.schmidt));
+    const RT k_heat = div_pos(div_pos(mu * gamm, gamm - one) * Rgas, RT(v.prandtl));
     const RT dN_u = W_(1, cb) - W_(1, c0), dN_v = W_(2, cb) - W_(2, c0), dN_T = S.T[cb] - S.T[c0];
     const RT dC_u = (W_(1, p1) + W_(1, p2) - W_(1, m1) - W_(1, m2)) * q4;
     const RT dC_v = (W_(2, p1) + W_(2, p2) - W_(2, m1) - W_(2, m2)) * q4;
