@@ -20,6 +20,7 @@
 // in k_residual2_f32.cu and k_residual2_f64.cu.
 #pragma once
 
+#include "div_pos.cuh"
 #include "scfd_internal.h"
 
 namespace scfd {
@@ -58,36 +59,13 @@ struct Smem {
 template <typename RT>
 constexpr bool kStageVh = sizeof(RT) == 4;
 
-// a / b for a positive normal b, without branches, so that the 2 (NY + 6)
-// limiter quotients of a face and the SLAU and viscous ones overlap (the IEEE
-// division's out-of-line slow path keeps them apart; with this one the FP64
-// residual takes 0.42 ms instead of 0.59 at 786 k cells, FP32 0.36 instead of
-// 0.44).  Every denominator it takes is a sum of squares plus eps, a density,
-// a sound speed, gamma - 1 or a positive constant.  Newton-Raphson on the reciprocal from the hardware's
-// approximate reciprocal y0 (rcp.approx.ftz, about 23 bits): FP64 takes one
-// third-order step y1 = y0 (1 + e + e^2), e = 1 - b y0 (relative error about
-// e^3), FP32 one second-order step y1 = y0 (1 + e); then q0 = a y1 and
-// Markstein's remainder correction q = q0 + (a - b q0) y1.  The result is
-// within one unit in the last place of a / b (tests/test_division.py checks the
-// steps in exact arithmetic from seeds 2^-21 off).
-__device__ __forceinline__ double div_pos(double a, double b) {
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
-    const double e = fma(-b, y, 1.0);
-    y = fma(fma(e, e, e), y, y);
-    const double q = a * y;
-    return fma(fma(-b, q, a), y, q);
-}
-__device__ __forceinline__ float div_pos(float a, float b) {
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(b));
-    y = fmaf(fmaf(-b, y, 1.0f), y, y);
-    const float q = a * y;
-    return fmaf(fmaf(-b, q, a), y, q);
-}
-
 }  // namespace
 
+// The face's quotients go through div_pos (a branch-free quotient): the 2 (NY + 6)
+// limiter quotients and the SLAU and viscous ones then overlap, and the FP64
+// residual takes 0.42 ms instead of 0.59 at 786 k cells (FP32 0.36 instead of
+// 0.44).  Their denominators are sums of squares plus eps, densities, a sound
+// speed, gamma - 1 and positive constants.
 template <typename RT, int NY, typename TL>
 __device__ __forceinline__ void face2(const View& v, const Smem<RT>& S, int p, int i, int j, int ix, int jy, bool iface,
                                       RT* out) {

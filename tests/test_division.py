@@ -1,5 +1,5 @@
 """The branch-free quotient of the residual kernel's MUSCL limiter
-(shared_cfd_b200/csrc/k_residual2.cuh, div_pos), restated step by step in exact
+(shared_cfd_b200/csrc/div_pos.cuh, used by the residual kernel), restated step by step in exact
 rational arithmetic, each operation (a fused multiply-add included) rounded once
 to nearest-even in the kernel's precision.  From reciprocal seeds up to 2^-21
 off (the hardware's approximate reciprocal is good to about 2^-23), the
