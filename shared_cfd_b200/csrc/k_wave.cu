@@ -667,16 +667,25 @@ __global__ void __launch_bounds__(1024) k_omega(View v, const int2* blk, const i
     const bool wr = tt < nt && cc >= 0 && cc < ni && j <= nj;
     const long long c = wr ? cidx(v.P, p, cc + 1, j) : 0;
     double res = 0.0, om = 1e300;
+    // every record value and q of the block's cells are loaded before the first
+    // barrier, so that the loads overlap one another instead of one component's
+    // barriers
+    double xr[NY + 1], qr[NY];
+#pragma unroll
     for (int m = 0; m <= NY; ++m) {
         const int k = m < NY ? m : NY + 2;  // the species, then the energy
-        const double cur = rd ? double(in[rbase + (long long)(k / G) * 32 * G + k % G]) : 0.0;
-        const double qk = (wr && m < NY) ? v.q[k * N + c] : 0.0;
-        tile[threadIdx.y][threadIdx.x] = cur;
+        xr[m] = rd ? double(in[rbase + (long long)(k / G) * 32 * G + k % G]) : 0.0;
+    }
+#pragma unroll
+    for (int m = 0; m < NY; ++m) qr[m] = wr ? v.q[m * N + c] : 0.0;
+#pragma unroll
+    for (int m = 0; m <= NY; ++m) {
+        tile[threadIdx.y][threadIdx.x] = xr[m];
         __syncthreads();
         if (wr) {
             const double dq = tile[tt][l];
             if (m < NY) {
-                if (dq < 0.0) om = fmin(om, -qk / dq * v.dq_max);
+                if (dq < 0.0) om = fmin(om, -qr[m] / dq * v.dq_max);
             } else {
                 res = dq * dq;
             }
@@ -743,26 +752,25 @@ __global__ void __launch_bounds__(1024) k_unpack(View v, const int2* blk, const 
     const T* in = X + (step_off[b.x] + kPadSteps + b.y) * L::XS;
     const int nt = min(32, ni + 31 - b.y);
     const long long N = v.ncell;
-    // read (step y, lane x) coalesced, write cells (step x, lane y); component
-    // k+1's record value and the cell's q are loaded before component k's
-    // barriers, so that the loads overlap them
+    // read (step y, lane x) coalesced, write cells (step x, lane y); every record
+    // value and q of the block's cells are loaded before the first barrier, so
+    // that the loads overlap one another
     const bool rd = (int)threadIdx.y < nt;
     const long long rbase = (long long)threadIdx.y * L::XS + threadIdx.x * G;
     const int tt = threadIdx.x, l = threadIdx.y;
     const int t = b.y + tt, cc = t - l, j = 32 * s + 1 + l;
     const bool wr = tt < nt && cc >= 0 && cc < ni && j <= nj;
     const long long c = wr ? cidx(v.P, p, cc + 1, j) : 0;
-    double nxt = rd ? double(in[rbase]) : 0.0;
-    double qn = wr ? v.q[c] : 0.0;
+    double xr[D], qr[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) xr[k] = rd ? double(in[rbase + (long long)(k / G) * 32 * G + k % G]) : 0.0;
+#pragma unroll
+    for (int k = 0; k < D; ++k) qr[k] = wr ? v.q[k * N + c] : 0.0;
+#pragma unroll
     for (int k = 0; k < D; ++k) {
-        const double cur = nxt, qk = qn;
-        if (k + 1 < D) {
-            nxt = rd ? double(in[rbase + (long long)((k + 1) / G) * 32 * G + (k + 1) % G]) : 0.0;
-            qn = wr ? v.q[(k + 1) * N + c] : 0.0;
-        }
-        if (rd) tile[threadIdx.y][threadIdx.x] = cur;
+        if (rd) tile[threadIdx.y][threadIdx.x] = xr[k];
         __syncthreads();
-        if (wr) v.q[k * N + c] = nr_mode ? qk + om * tile[tt][l] : qk + tile[tt][l];
+        if (wr) v.q[k * N + c] = nr_mode ? qr[k] + om * tile[tt][l] : qr[k] + tile[tt][l];
         __syncthreads();
     }
 }
