@@ -89,16 +89,17 @@ def workload_name(config, scale):
         ("" if scale == 1.0 else " (scale %g)" % scale)
 
 
-# DRAM bytes (read + write) per interior cell and launch of this build, from ncu
-# captures of the reacting step at scale 0.5 (196 608 cells; ncu flushes the caches
-# before each launch, so reads are cold, and writes still in L2 at a launch's end are
-# not counted); commands in profiles/traffic_reacting_step_196k.md.  None of these
-# kernels reuses data across launches, so the traffic of a launch grows with the cell
-# count and is scaled to the workload by cells.  K_UPDATE averages its two launches
-# per inner iteration (k_omega and k_unpack).
+# DRAM bytes (read + write) per interior cell and launch, from ncu captures of the
+# reacting step at scale 0.5 (196 608 cells; ncu flushes the caches before each
+# launch, so reads are cold, and writes still in L2 at a launch's end are not
+# counted); commands in profiles/traffic_reacting_step_196k.md, which also says which
+# build each figure was captured on (the sweeps and the FP64 residual on this one).
+# None of these kernels reuses data across launches, so the traffic of a launch grows
+# with the cell count and is scaled to the workload by cells.  K_UPDATE averages its
+# two launches per inner iteration (k_omega and k_unpack).
 NCU_DRAM_BYTES_PER_CELL = {
-    ("reacting_step", False): {abi.K_THERMO: 159.3, abi.K_RESIDUAL: 644.8, abi.K_PACK: 542.1,
-                               abi.K_SWEEP_FWD: 417.0, abi.K_SWEEP_BWD: 418.0, abi.K_UPDATE: 197.0},
+    ("reacting_step", False): {abi.K_THERMO: 159.3, abi.K_RESIDUAL: 656.0, abi.K_PACK: 542.1,
+                               abi.K_SWEEP_FWD: 447.3, abi.K_SWEEP_BWD: 437.7, abi.K_UPDATE: 197.0},
     ("reacting_step", True): {abi.K_THERMO: 159.3, abi.K_RESIDUAL: 553.9, abi.K_PACK: 404.7,
                               abi.K_SWEEP_FWD: 216.2, abi.K_SWEEP_BWD: 216.2, abi.K_UPDATE: 143.2},
 }
