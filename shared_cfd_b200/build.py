@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libscfd_b200.so")
-HEADERS = ["k_residual2.cuh", "adj_face.cuh", "scfd_internal.h", "async_ptx.h", "chem_tables.h", "chem_dev.cuh"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".h", ".cuh")))  # every header: a change rebuilds
 SOURCES = ["scfd_api.cu", "k_thermo.cu", "k_bc.cu", "k_residual.cu", "k_lusgs.cu", "k_chem.cu", "k_misc.cu", "k_sweep2.cu", "k_wave.cu", "k_residual2.cu", "k_residual2_f32.cu", "k_residual2_f64.cu", "noalloc.cu", "k_reactors.cu", "k_shard.cu", "k_adjoint.cu", "k_cea.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

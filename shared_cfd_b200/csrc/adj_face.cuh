@@ -15,6 +15,7 @@
 #include <math.h>
 
 #ifdef __CUDACC__
+#include "div_pos.cuh"
 #define SCFD_HD __host__ __device__ __forceinline__
 #else
 #define SCFD_HD inline
@@ -25,14 +26,27 @@ namespace adj {
 
 constexpr double kEps = 1e-300;  // muscl.f90 epsln
 
+// a / b for a positive normal b: on the device the branch-free quotient of
+// div_pos.cuh (within one unit in the last place; the adjoint run of 300 steps
+// at 196 k cells takes 62 ms with it, 68 without), on the host IEEE division.
+// Every b below is a sum of squares plus eps, a density, a sound speed or a
+// sum of them, or a positive square root.
+SCFD_HD double qdiv(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return div_pos(a, b);
+#else
+    return a / b;
+#endif
+}
+
 SCFD_HD void muscl_fwd(double wm1, double w0, double w1, double w2, double phi, double km, double& wl, double& wr) {
     double Du = w1 - w0, Dl = w0 - wm1;
-    double s = (2.0 * Du * Dl) / (Du * Du + Dl * Dl + kEps);
+    double s = qdiv(2.0 * Du * Dl, Du * Du + Dl * Dl + kEps);
     const double du = 0.5 * s * ((1.0 + km * s) * Du + (1.0 - km * s) * Dl);
     wl = w0 + phi * 0.5 * du;
     Du = w2 - w1;
     Dl = w1 - w0;
-    s = (2.0 * Du * Dl) / (Du * Du + Dl * Dl + kEps);
+    s = qdiv(2.0 * Du * Dl, Du * Du + Dl * Dl + kEps);
     const double dl = 0.5 * s * ((1.0 + km * s) * Dl + (1.0 - km * s) * Du);
     wr = w1 - phi * 0.5 * dl;
 }
@@ -47,7 +61,7 @@ SCFD_HD void limiter_grad(double a, double b, double iQ, double& sa, double& sb)
 // One-sided slope d(a, b) = s/2 ((1 + km s) a + (1 - km s) b), s = s(a, b): adds
 // its adjoint g times the partial derivatives to ab, bb.
 SCFD_HD void slope_rev(double a, double b, double km, double g, double& ab, double& bb) {
-    const double iQ = 1.0 / (a * a + b * b + kEps);
+    const double iQ = qdiv(1.0, a * a + b * b + kEps);
     const double s = 2.0 * a * b * iQ;
     const double A = (1.0 + km * s) * a + (1.0 - km * s) * b;
     const double dds = 0.5 * A + 0.5 * s * km * (a - b);
@@ -82,21 +96,22 @@ SCFD_HD double sgn(double x) { return x >= 0.0 ? 1.0 : -1.0; }
 SCFD_HD void slau_fwd(int nY, const double* wl, const double* wr, double n1, double n2, double* tg) {
     const double rhol = wl[0], ul = wl[1], vl = wl[2], pl = wl[3], gl = wl[4 + nY];
     const double rhor = wr[0], ur = wr[1], vr = wr[2], pr = wr[3], gr = wr[4 + nY];
-    const double al = sqrt(gl * pl / rhol), ar = sqrt(gr * pr / rhor);
+    const double al = sqrt(qdiv(gl * pl, rhol)), ar = sqrt(qdiv(gr * pr, rhor));
     const double unl = n1 * ul + n2 * vl, unr = n1 * ur + n2 * vr;
     const double dp = pr - pl;
     const double a_bar = 0.5 * (ar + al);
     const double p_bar = 0.5 * (pr + pl);
-    const double ml = unl / a_bar, mr = unr / a_bar;
-    const double m_tilde = fmin(1.0, 1.0 / a_bar * sqrt(0.5 * (ul * ul + vl * vl + ur * ur + vr * vr)));
+    const double ia = qdiv(1.0, a_bar);
+    const double ml = unl * ia, mr = unr * ia;
+    const double m_tilde = fmin(1.0, ia * sqrt(0.5 * (ul * ul + vl * vl + ur * ur + vr * vr)));
     const double chi = (1.0 - m_tilde) * (1.0 - m_tilde);
     const double gp = -fmax(fmin(ml, 0.0), -1.0);
     const double gm = fmin(fmax(mr, 0.0), 1.0);
     const double g = gp * gm;
-    const double ub = (fabs(unr) * rhor + fabs(unl) * rhol) / (rhor + rhol);
+    const double ub = qdiv(fabs(unr) * rhor + fabs(unl) * rhol, rhor + rhol);
     const double ubp = (1.0 - g) * ub + g * fabs(unl);
     const double ubm = (1.0 - g) * ub + g * fabs(unr);
-    const double dm = 0.5 * (rhol * (unl + ubp) + rhor * (unr - ubm) - chi / a_bar * dp);
+    const double dm = 0.5 * (rhol * (unl + ubp) + rhor * (unr - ubm) - chi * ia * dp);
     const double betar = fabs(mr) < 1.0 ? 0.25 * (2.0 + mr) * ((mr - 1.0) * (mr - 1.0)) : 0.5 * (1.0 - copysign(1.0, mr));
     const double betal = fabs(ml) < 1.0 ? 0.25 * (2.0 - ml) * ((ml + 1.0) * (ml + 1.0)) : 0.5 * (1.0 + copysign(1.0, ml));
     const double pt = p_bar + 0.5 * (betal - betar) * (pl - pr) + (1.0 - chi) * (betar + betal - 1.0) * p_bar;
@@ -113,26 +128,28 @@ SCFD_HD void slau_rev(int nY, const double* wl, const double* wr, double n1, dou
     // forward values
     const double rhol = wl[0], ul = wl[1], vl = wl[2], pl = wl[3], gl = wl[4 + nY];
     const double rhor = wr[0], ur = wr[1], vr = wr[2], pr = wr[3], gr = wr[4 + nY];
-    const double Al = gl * pl / rhol, Ar = gr * pr / rhor;
+    const double Al = qdiv(gl * pl, rhol), Ar = qdiv(gr * pr, rhor);
     const double al = sqrt(Al), ar = sqrt(Ar);
     const double unl = n1 * ul + n2 * vl, unr = n1 * ur + n2 * vr;
     const double dp = pr - pl;
     const double a_bar = 0.5 * (ar + al);
     const double p_bar = 0.5 * (pr + pl);
-    const double ml = unl / a_bar, mr = unr / a_bar;
+    const double ia = qdiv(1.0, a_bar), ia2 = ia * ia;
+    const double ml = unl * ia, mr = unr * ia;
     const double S = 0.5 * (ul * ul + vl * vl + ur * ur + vr * vr);
     const double sq = sqrt(S);
-    const double mraw = 1.0 / a_bar * sq;
+    const double mraw = ia * sq;
     const double m_tilde = fmin(1.0, mraw);
     const double chi = (1.0 - m_tilde) * (1.0 - m_tilde);
     const double gp = -fmax(fmin(ml, 0.0), -1.0);
     const double gm = fmin(fmax(mr, 0.0), 1.0);
     const double g = gp * gm;
     const double num = fabs(unr) * rhor + fabs(unl) * rhol, den = rhor + rhol;
-    const double ub = num / den;
+    const double iden = qdiv(1.0, den);
+    const double ub = num * iden;
     const double ubp = (1.0 - g) * ub + g * fabs(unl);
     const double ubm = (1.0 - g) * ub + g * fabs(unr);
-    const double dm = 0.5 * (rhol * (unl + ubp) + rhor * (unr - ubm) - chi / a_bar * dp);
+    const double dm = 0.5 * (rhol * (unl + ubp) + rhor * (unr - ubm) - chi * ia * dp);
     const bool rin = fabs(mr) < 1.0, lin = fabs(ml) < 1.0;
     const double betar = rin ? 0.25 * (2.0 + mr) * ((mr - 1.0) * (mr - 1.0)) : 0.5 * (1.0 - copysign(1.0, mr));
     const double betal = lin ? 0.25 * (2.0 - ml) * ((ml + 1.0) * (ml + 1.0)) : 0.5 * (1.0 + copysign(1.0, ml));
@@ -161,7 +178,6 @@ SCFD_HD void slau_rev(int nY, const double* wl, const double* wr, double n1, dou
     const double betarb = ptb * (-0.5 * (pl - pr) + (1.0 - chi) * p_bar);
     double plb = ptb * 0.5 * (betal - betar), prb = -ptb * 0.5 * (betal - betar);
     double chib = -ptb * (betar + betal - 1.0) * p_bar;
-    const double ia = 1.0 / a_bar, ia2 = ia * ia;
     double mrb = 0.0, mlb = 0.0;
     if (rin) mrb += betarb * 0.25 * ((mr - 1.0) * (mr - 1.0) + (2.0 + mr) * 2.0 * (mr - 1.0));
     if (lin) mlb += betalb * 0.25 * (-(ml + 1.0) * (ml + 1.0) + (2.0 - ml) * 2.0 * (ml + 1.0));
@@ -178,7 +194,6 @@ SCFD_HD void slau_rev(int nY, const double* wl, const double* wr, double n1, dou
     unlb += ubpb * g * sgn(unl);
     unrb += ubmb * g * sgn(unr);
     // ub = num / den
-    const double iden = 1.0 / den;
     const double numb = ubb * iden, denb = -ubb * num * iden * iden;
     unrb += numb * rhor * sgn(unr);
     rhorb += numb * fabs(unr) + denb;
@@ -194,7 +209,7 @@ SCFD_HD void slau_rev(int nY, const double* wl, const double* wr, double n1, dou
     const double sqb = mrawb * ia;
     a_barb += -mrawb * sq * ia2;
     if (sq > 0.0) {
-        const double Sb = sqb / (2.0 * sq);
+        const double Sb = qdiv(sqb, 2.0 * sq);
         ulb += Sb * ul;
         vlb += Sb * vl;
         urb += Sb * ur;
@@ -214,8 +229,8 @@ SCFD_HD void slau_rev(int nY, const double* wl, const double* wr, double n1, dou
     urb += n1 * unrb;
     vrb += n2 * unrb;
     // sound speeds a = sqrt(gamma p / rho)
-    const double irl = 1.0 / rhol, irr = 1.0 / rhor;
-    const double Alb = 0.5 * alb / al, Arb = 0.5 * arb / ar;
+    const double irl = qdiv(1.0, rhol), irr = qdiv(1.0, rhor);
+    const double Alb = qdiv(0.5 * alb, al), Arb = qdiv(0.5 * arb, ar);
     wlb[4 + nY] += Alb * pl * irl;
     plb += Alb * gl * irl;
     rholb += -Alb * Al * irl;
@@ -240,7 +255,7 @@ SCFD_HD void ideal_prim_rev(int nY, const double* q, double kappa, double rhob, 
                             const double* Yb, double htb, double* qb) {
     double rho = 0.0;
     for (int k = 0; k < nY; ++k) rho = rho + q[k];
-    const double ir = 1.0 / rho, ir2 = ir * ir;
+    const double ir = qdiv(1.0, rho), ir2 = ir * ir;
     const double u = q[nY] * ir, v = q[nY + 1] * ir, E = q[nY + 2];
     const double ei = E * ir - 0.5 * (u * u + v * v);
     const double p = rho * (kappa - 1.0) * ei;
