@@ -897,11 +897,17 @@ def roofline_of(prof, config, mixed, cells_here, peak, peak_kind):
 
 def e2e_run(s_e, case_e, steps, sharded, world, barrier, max_over_ranks, torch, dev):
     """The metric through scfd_upload / scfd_step / scfd_download with host
-    buffers every step (the reference-layout arrays cross PCIe)."""
-    q = np.ascontiguousarray(case_e.q)
-    w = np.ascontiguousarray(case_e.w)
-    vhi = np.ascontiguousarray(case_e.vhi)
-    qout = np.zeros_like(q)
+    buffers every step (the reference-layout arrays cross PCIe).  The host
+    arrays are page-locked, as a caller that keeps its fields in pinned memory
+    holds them; the library then moves them by DMA without a staging copy."""
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float64).pin_memory()
+        h = t.numpy()
+        h[...] = a
+        return t, h
+
+    keep = [pinned(np.ascontiguousarray(a)) for a in (case_e.q, case_e.w, case_e.vhi, np.zeros_like(case_e.q))]
+    q, w, vhi, qout = (h for _, h in keep)
     lib = s_e.lib
     ttc = C.c_double()
     barrier()

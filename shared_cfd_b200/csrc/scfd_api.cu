@@ -972,9 +972,24 @@ int scfd_commit(scfd_ctx* c) {
 }
 
 // reference layout f(k, -1:nimax+2, -1:njmax+2, plane) <-> SoA slots
-// Host <-> device copies of the caller's (pageable) arrays go through two
-// pinned chunks: the host threads copy one chunk while the DMA engine moves the
-// other.
+// Host <-> device copies of the caller's arrays.  Page-locked arrays (the
+// caller's cudaHostRegister or cudaMallocHost memory) are moved by the DMA
+// engine directly; pageable ones go through two pinned chunks: the host threads
+// copy one chunk while the DMA engine moves the other.
+
+// true when [p, p + bytes) starts and ends in page-locked host memory
+static bool page_locked(const void* p, size_t bytes) {
+    if (!p || bytes == 0) return false;
+    for (const char* q : {static_cast<const char*>(p), static_cast<const char*>(p) + bytes - 1}) {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+            cudaGetLastError();  // an unknown pointer is pageable memory, not an error
+            return false;
+        }
+        if (a.type != cudaMemoryTypeHost) return false;
+    }
+    return true;
+}
 
 static void par_copy(void* dst, const void* src, size_t bytes) {
     const size_t piece = 1ull << 20;
@@ -987,6 +1002,10 @@ static void par_copy(void* dst, const void* src, size_t bytes) {
 }
 
 static int h2d_pipelined(scfd_ctx* c, void* dev, const void* host, size_t bytes) {
+    if (page_locked(host, bytes)) {
+        CK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, c->stream));
+        return 0;
+    }
     size_t off = 0;
     for (int k = 0; off < bytes; ++k) {
         const int b = k & 1;
@@ -1001,6 +1020,11 @@ static int h2d_pipelined(scfd_ctx* c, void* dev, const void* host, size_t bytes)
 }
 
 static int d2h_pipelined(scfd_ctx* c, void* host, const void* dev, size_t bytes) {
+    if (page_locked(host, bytes)) {
+        CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        return 0;
+    }
     size_t off = 0, prev_off = 0, prev_len = 0;
     int k = 0;
     for (; off < bytes; ++k) {
