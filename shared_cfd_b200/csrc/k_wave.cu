@@ -402,9 +402,13 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                     const int J = G - 7;
                     const bool pub = (pub_remote || pub_global) && J >= 0 && J <= lastc;
                     const unsigned ps = pc % HS;
-                    if (pub && pc >= HS) {
+                    // back-pressure once per 8 chunks: chunk pc + k (k < 8) reuses the
+                    // slot of chunk pc + k - HS, and chunks are released in order, so
+                    // the release of chunk pc + 7 - HS covers the next 8
+                    if (pub && pc % 8u == 0u && pc + 7u >= HS) {
+                        const unsigned pw = pc + 7u, sw = pw % HS;
                         const bool okp =
-                            wait_phase(pub_remote ? &pempty[ps] : &oemp[ps], ((pc / HS) - 1u) & 1u, v, s_bail);
+                            wait_phase(pub_remote ? &pempty[sw] : &oemp[sw], ((pw / HS) - 1u) & 1u, v, s_bail);
                         if (!__all_sync(0xffffffffu, okp)) {
                             if (lane == 31) give_up(v, s_bail);
                             bail = true;
