@@ -302,8 +302,10 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
     int* s_task = reinterpret_cast<int*>(oemp + HS);
     int* s_bail = s_task + 1;
 
+    __shared__ __align__(16) RT s_zero[D4];  // the strip-below column where there is none
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned rank = cluster_rank();
+    if (sizeof(RT) == 8 && threadIdx.x < D4) s_zero[threadIdx.x] = RT(0);
     if (threadIdx.x == 0) {
         for (int k = 0; k < 2 * PFB + 5 * HS; ++k) mbar_init(&bars[k], 1);
         *s_bail = 0;
@@ -433,8 +435,14 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
                             }
                         }
                         // column t from the strip below (lane 0)
+                        // Where there is no strip below or the column is past the plane,
+                        // the FP64 step reads a zero column (one address select instead of a
+                        // value select per component: FP64 sweep pair 0.879 -> 0.850 ms); the
+                        // FP32 step keeps the value selects, which measured faster for it
+                        // (0.578 against 0.592 ms).
                         const bool in_col = has_prev && t < ni;
-                        const RT* xi = xin + (((xc0 + (unsigned)((t + 3) >> 2)) % HS) * HK + ((t + 3) & 3)) * D4;
+                        const RT* xring = xin + (((xc0 + (unsigned)((t + 3) >> 2)) % HS) * HK + ((t + 3) & 3)) * D4;
+                        const RT* xi = sizeof(RT) == 8 && !in_col ? s_zero : xring;
                         // every lane reads the column (16-byte shared-memory broadcasts); lane 0 uses it
                         RT xv[D4];
 #pragma unroll
@@ -444,7 +452,10 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(64) k_wave(View v, 
 #pragma unroll
                         for (int k = 0; k < D; ++k) {
                             const RT sh = __shfl_up_sync(0xffffffffu, outB[k], 1);
-                            inB[k] = lane == 0 ? (in_col ? xv[k] : RT(0)) : sh;
+                            if constexpr (sizeof(RT) == 8)
+                                inB[k] = lane == 0 ? xv[k] : sh;
+                            else
+                                inB[k] = lane == 0 ? (in_col ? xv[k] : RT(0)) : sh;
                         }
                         // this lane's cell
                         RT fx[NGX * G4], f[NGC * G4];
